@@ -1,0 +1,73 @@
+"""Build recipe for the oracle (test infrastructure only).
+
+Two artefacts:
+
+* ``oracle/libfdg_oracle.so`` -- the plain-C restatement (``fdg_oracle.c``).
+* ``oracle/_ref/fdg_ref<EXT_SUFFIX>`` -- the reference's own CPU implementation
+  of the path, ``src/convert/flexible_dual_grid.cpp`` compiled unmodified from
+  the reference source tree against the project's Eigen-API shim
+  (``oracle/eigen_shim``; Eigen is an un-vendored submodule of the reference),
+  plus ``ref_binding.cpp``.  Built only where the reference tree exists; the
+  built file travels with the repository snapshot to machines without it.
+
+Flags follow the reference's own build (``setup.py:65-67``: ``-O3 -std=c++17``,
+no ``-march``), with ``-ffp-contract=off`` stated explicitly.
+"""
+import os
+import subprocess
+import sys
+import sysconfig
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE_ROOT = os.environ.get("OVX_REFERENCE_ROOT", "/root/reference")
+ORACLE_SO = os.path.join(HERE, "libfdg_oracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+REF_SO = os.path.join(REF_DIR, "fdg_ref" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def _newer(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
+
+
+def build_oracle(force=False):
+    src = [os.path.join(HERE, "fdg_oracle.c"), os.path.join(HERE, "fdg_oracle_impl.h")]
+    if force or _newer(ORACLE_SO, src):
+        cmd = ["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fPIC", "-shared", src[0], "-o", ORACLE_SO, "-lm"]
+        subprocess.check_call(cmd)
+    return ORACLE_SO
+
+
+def build_ref(force=False):
+    """Compile the reference CPU path; returns the .so path or None if the source is absent."""
+    ref_cpp = os.path.join(REFERENCE_ROOT, "src", "convert", "flexible_dual_grid.cpp")
+    if not os.path.exists(ref_cpp):
+        return REF_SO if os.path.exists(REF_SO) else None
+    binding = os.path.join(HERE, "ref_binding.cpp")
+    shim = os.path.join(HERE, "eigen_shim")
+    if not (force or _newer(REF_SO, [ref_cpp, binding, os.path.join(shim, "Eigen", "Dense")])):
+        return REF_SO
+    import torch
+    from torch.utils import cpp_extension as ce
+
+    os.makedirs(REF_DIR, exist_ok=True)
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    cmd = ["g++", "-O3", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared",
+           "-w", "-fext-numeric-literals",
+           f"-D_GLIBCXX_USE_CXX11_ABI={abi}", "-DTORCH_EXTENSION_NAME=fdg_ref", "-DTORCH_API_INCLUDE_EXTENSION_H",
+           "-I", shim, "-I", os.path.dirname(ref_cpp), "-I", sysconfig.get_paths()["include"]]
+    for p in ce.include_paths():
+        cmd += ["-I", p]
+    cmd += [ref_cpp, binding, "-o", REF_SO]
+    for p in ce.library_paths():
+        cmd += ["-L", p, f"-Wl,-rpath,{p}"]
+    cmd += ["-lc10", "-ltorch", "-ltorch_cpu", "-ltorch_python"]
+    subprocess.check_call(cmd)
+    return REF_SO
+
+
+if __name__ == "__main__":
+    print(build_oracle(force="--force" in sys.argv))
+    print(build_ref(force="--force" in sys.argv))
