@@ -1,0 +1,114 @@
+/*
+ * ovx_fdg.h -- C ABI of the B200 mesh -> flexible dual grid library
+ * (libovx_fdg.so).  Plain pointers and sizes; device pointers are CUDA device
+ * memory on the context's device; `stream` is a cudaStream_t passed as void*
+ * (NULL = legacy default stream).
+ *
+ * The entry points replace the reference's CUDA operator for this path:
+ *
+ *   o_voxel._C.mesh_to_flexible_dual_grid_cuda(vertices, faces, voxel_size,
+ *       grid_range, face_weight, boundary_weight, regularization_weight)
+ *       -> (voxels int32[N,3], dual_vertices float32[N,3], intersected bool[N,3])
+ *     declared in src/convert/api.h:164-172, bound in src/ext.cpp:19,
+ *     implemented in src/convert/mesh_to_flexible_dual_grid_gpu/mesh_to_flexible_dual_grid.cu:797-895
+ *   -> ovx_fdg_begin + ovx_fdg_finish
+ *
+ *   o_voxel._C.intersect_occ_cuda(triangles, voxel_size, grid_range) -> int32[N,3]
+ *     declared in src/convert/api.h:63-66, bound in src/ext.cpp:21,
+ *     implemented in src/convert/mesh_to_flexible_dual_grid_gpu/intersect_qef.cu:896-920
+ *   -> ovx_fdg_occupancy_begin + ovx_fdg_occupancy_finish
+ *
+ * Semantics follow the reference CPU path (src/convert/flexible_dual_grid.cpp):
+ * occupancy, intersected flags and dual vertices are bit-identical to it for
+ * the floating-point evaluation order documented in the library.  Output rows
+ * are in a deterministic order: 8x8x8 bricks in x-fastest order, voxels inside
+ * a brick in x-fastest order (the reference GPU order is arbitrary; the
+ * reference CPU order is first-touch order).
+ *
+ * Two calls per conversion: `begin` runs the occupancy stage and returns the
+ * number of voxel rows N (one stream synchronisation); the caller then
+ * provides output buffers with N rows and `finish` runs the quadric and solve
+ * stages (one more stream synchronisation, for the quadric entry count).  A
+ * context holds its device workspace and the state between the two calls; it
+ * is not safe to use one context from two threads at once.
+ */
+#ifndef OVX_FDG_H
+#define OVX_FDG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum ovx_fdg_status
+{
+    OVX_FDG_OK = 0,
+    OVX_FDG_INVALID_ARGUMENT = 1, /* bad pointer, size, grid or call order (reference: TORCH_CHECK -> RuntimeError) */
+    OVX_FDG_BAD_FACE_INDEX = 2,   /* a face index outside [0, num_vertices) */
+    OVX_FDG_CUDA_ERROR = 3,       /* a CUDA runtime call or launch failed */
+    OVX_FDG_OUT_OF_MEMORY = 4,    /* workspace allocation failed */
+    OVX_FDG_CAPACITY = 5,         /* result larger than the 32-bit row / 64-bit entry indexing supports */
+    OVX_FDG_INTERNAL = 6          /* a device-side bound (walk length) was hit; results not produced */
+};
+
+/* Voxel grid: voxel i along axis a spans [i*voxel_size[a], (i+1)*voxel_size[a])
+ * in grid-local coordinates, for grid_min[a] <= i < grid_max[a]
+ * (reference grid_range = {grid_min..., grid_max...}, flexible_dual_grid.py:178). */
+typedef struct ovx_fdg_grid
+{
+    float voxel_size[3];
+    int32_t grid_min[3];
+    int32_t grid_max[3];
+} ovx_fdg_grid;
+
+typedef struct ovx_fdg_context ovx_fdg_context;
+
+/* Create a context bound to a CUDA device.  No device memory is allocated until the first call. */
+int ovx_fdg_context_create(int device, ovx_fdg_context **out);
+void ovx_fdg_context_destroy(ovx_fdg_context *ctx);
+/* Human-readable text for a status code, and the last error recorded on a context. */
+const char *ovx_fdg_status_string(int status);
+const char *ovx_fdg_last_error(const ovx_fdg_context *ctx);
+/* Bytes of device workspace the context currently holds. */
+int64_t ovx_fdg_workspace_bytes(const ovx_fdg_context *ctx);
+
+/*
+ * Occupancy stage of mesh -> flexible dual grid.
+ *   vertices: device float32 [num_vertices, 3], NOT shifted; origin (host
+ *             float[3], may be NULL for zero) is subtracted in float32 exactly
+ *             as the reference wrapper does (`vertices - aabb[0]`,
+ *             flexible_dual_grid.py:181).
+ *   faces:    device int32 or int64 [num_faces, 3] (face_index_bytes = 4 or 8).
+ *   grid, weights: as the reference operator (face_weight only gates the face
+ *             stage, as in the reference CPU path).
+ * On success *num_voxels receives N.  The inputs must stay valid and unchanged until finish returns.
+ */
+int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int64_t num_vertices,
+                  const void *faces, int32_t face_index_bytes, int64_t num_faces, const float *origin,
+                  const ovx_fdg_grid *grid, float face_weight, float boundary_weight,
+                  float regularization_weight, int64_t *num_voxels);
+
+/*
+ * Quadric + solve stages.  Output device buffers with room for N rows:
+ *   voxel_indices int32 [N,3], dual_vertices float32 [N,3] (grid-local frame,
+ *   like the reference), intersected uint8 [N,3] (0/1, torch.bool layout).
+ * Work is enqueued on `stream`; the function synchronises once on it.
+ */
+int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, float *dual_vertices,
+                   uint8_t *intersected);
+
+/*
+ * Occupancy only (reference intersect_occ).  triangles: device float32
+ * [num_triangles, 3, 3] in grid-local coordinates (already shifted), as the
+ * reference operator takes them.  begin returns N; finish writes int32 [N,3].
+ */
+int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *triangles, int64_t num_triangles,
+                            const ovx_fdg_grid *grid, int64_t *num_voxels);
+int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OVX_FDG_H */

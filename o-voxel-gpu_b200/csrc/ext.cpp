@@ -1,0 +1,157 @@
+// ext.cpp -- torch extension `o_voxel._C` for the B200 flexible-dual-grid
+// library.  Mirrors the reference binding (src/ext.cpp:18-21) for this path:
+//
+//   mesh_to_flexible_dual_grid_cuda(vertices, faces, voxel_size, grid_range,
+//       face_weight, boundary_weight, regularization_weight)
+//       -> (voxels int32[N,3], dual_vertices float32[N,3], intersected bool[N,3])
+//       reference: src/convert/api.h:164-172
+//   intersect_occ_cuda(triangles, voxel_size, grid_range) -> int32[N,3]
+//       reference: src/convert/api.h:63-66
+//
+// plus `mesh_to_flexible_dual_grid_cuda_ex`, which takes unshifted vertices,
+// the aabb origin and int32 or int64 faces so the wrapper does not need the
+// extra cast and shift passes over the inputs.
+//
+// All compute goes through the C ABI in include/ovx_fdg.h (libovx_fdg.so).
+// Outputs come from torch's caching allocator on the input's device, work runs
+// on torch's current stream, and the GIL is released during the call, as in
+// the reference.  Errors raise RuntimeError (TORCH_CHECK), as in the reference.
+#include <torch/extension.h>
+#include <ATen/cuda/CUDAContext.h>
+#include <c10/cuda/CUDAGuard.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "ovx_fdg.h"
+
+namespace
+{
+
+struct DeviceContext
+{
+    ovx_fdg_context *ctx = nullptr;
+    std::mutex mu;
+    ~DeviceContext()
+    {
+        if (ctx)
+            ovx_fdg_context_destroy(ctx);
+    }
+};
+
+DeviceContext &context_for(int device)
+{
+    static std::mutex map_mu;
+    static std::map<int, std::unique_ptr<DeviceContext>> contexts;
+    std::lock_guard<std::mutex> lock(map_mu);
+    auto &slot = contexts[device];
+    if (!slot)
+    {
+        slot = std::make_unique<DeviceContext>();
+        const int rc = ovx_fdg_context_create(device, &slot->ctx);
+        TORCH_CHECK(rc == OVX_FDG_OK, "ovx_fdg_context_create failed: ", ovx_fdg_status_string(rc));
+    }
+    return *slot;
+}
+
+void check(int rc, ovx_fdg_context *ctx, const char *what)
+{
+    TORCH_CHECK(rc == OVX_FDG_OK, what, " failed (", ovx_fdg_status_string(rc), "): ", ovx_fdg_last_error(ctx));
+}
+
+ovx_fdg_grid make_grid(const std::vector<float> &voxel_size, const std::vector<int64_t> &grid_range)
+{
+    TORCH_CHECK(voxel_size.size() == 3, "voxel_size must have 3 elements");
+    TORCH_CHECK(grid_range.size() == 6, "grid_range must have 6 elements");
+    ovx_fdg_grid g;
+    for (int a = 0; a < 3; ++a)
+    {
+        g.voxel_size[a] = voxel_size[a];
+        g.grid_min[a] = static_cast<int32_t>(grid_range[a]);
+        g.grid_max[a] = static_cast<int32_t>(grid_range[3 + a]);
+    }
+    return g;
+}
+
+std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Tensor &vertices, const torch::Tensor &faces,
+                                                                 const float *origin, const std::vector<float> &voxel_size,
+                                                                 const std::vector<int64_t> &grid_range, float face_weight,
+                                                                 float boundary_weight, float regularization_weight)
+{
+    TORCH_CHECK(vertices.is_cuda(), "vertices must be a CUDA tensor");
+    TORCH_CHECK(faces.is_cuda(), "faces must be a CUDA tensor");
+    TORCH_CHECK(vertices.device() == faces.device(), "vertices and faces must be on the same device");
+    TORCH_CHECK(vertices.scalar_type() == torch::kFloat32, "vertices must be float32");
+    TORCH_CHECK(faces.scalar_type() == torch::kInt32 || faces.scalar_type() == torch::kInt64, "faces must be int32 or int64");
+    TORCH_CHECK(vertices.dim() == 2 && vertices.size(1) == 3, "vertices must be [V,3]");
+    TORCH_CHECK(faces.dim() == 2 && faces.size(1) == 3, "faces must be [F,3]");
+    auto v = vertices.contiguous();
+    auto f = faces.contiguous();
+    const ovx_fdg_grid grid = make_grid(voxel_size, grid_range);
+    const c10::cuda::CUDAGuard guard(v.device());
+    const int device = v.get_device();
+    cudaStream_t stream = at::cuda::getCurrentCUDAStream(device).stream();
+    DeviceContext &dc = context_for(device);
+    std::lock_guard<std::mutex> lock(dc.mu);
+    int64_t n = 0;
+    check(ovx_fdg_begin(dc.ctx, stream, v.data_ptr<float>(), v.size(0), f.numel() ? f.data_ptr() : nullptr,
+                        f.scalar_type() == torch::kInt64 ? 8 : 4, f.size(0), origin, &grid, face_weight, boundary_weight,
+                        regularization_weight, &n),
+          dc.ctx, "mesh_to_flexible_dual_grid (occupancy)");
+    auto opts = torch::TensorOptions().device(v.device());
+    auto vox = torch::empty({n, 3}, opts.dtype(torch::kInt32));
+    auto dual = torch::empty({n, 3}, opts.dtype(torch::kFloat32));
+    auto inter = torch::empty({n, 3}, opts.dtype(torch::kBool));
+    check(ovx_fdg_finish(dc.ctx, stream, n ? vox.data_ptr<int32_t>() : nullptr, n ? dual.data_ptr<float>() : nullptr,
+                         n ? reinterpret_cast<uint8_t *>(inter.data_ptr<bool>()) : nullptr),
+          dc.ctx, "mesh_to_flexible_dual_grid (quadrics)");
+    return std::make_tuple(vox, dual, inter);
+}
+
+} // namespace
+
+std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> mesh_to_flexible_dual_grid_cuda(
+    const torch::Tensor &vertices, const torch::Tensor &faces, const std::vector<float> &voxel_size,
+    const std::vector<int64_t> &grid_range, float face_weight, float boundary_weight, float regularization_weight)
+{
+    return run_fdg(vertices, faces, nullptr, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight);
+}
+
+std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> mesh_to_flexible_dual_grid_cuda_ex(
+    const torch::Tensor &vertices, const torch::Tensor &faces, const std::vector<float> &origin,
+    const std::vector<float> &voxel_size, const std::vector<int64_t> &grid_range, float face_weight, float boundary_weight,
+    float regularization_weight)
+{
+    TORCH_CHECK(origin.size() == 3, "origin must have 3 elements");
+    const float o[3] = {origin[0], origin[1], origin[2]};
+    return run_fdg(vertices, faces, o, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight);
+}
+
+torch::Tensor intersect_occ_cuda(const torch::Tensor &triangles, const std::vector<float> &voxel_size,
+                                 const std::vector<int64_t> &grid_range)
+{
+    TORCH_CHECK(triangles.is_cuda(), "triangles must be a CUDA tensor");
+    TORCH_CHECK(triangles.scalar_type() == torch::kFloat32, "triangles must be float32");
+    TORCH_CHECK(triangles.dim() == 3 && triangles.size(1) == 3 && triangles.size(2) == 3, "triangles must be [T,3,3]");
+    auto t = triangles.contiguous();
+    const ovx_fdg_grid grid = make_grid(voxel_size, grid_range);
+    const c10::cuda::CUDAGuard guard(t.device());
+    const int device = t.get_device();
+    cudaStream_t stream = at::cuda::getCurrentCUDAStream(device).stream();
+    DeviceContext &dc = context_for(device);
+    std::lock_guard<std::mutex> lock(dc.mu);
+    int64_t n = 0;
+    check(ovx_fdg_occupancy_begin(dc.ctx, stream, t.numel() ? t.data_ptr<float>() : nullptr, t.size(0), &grid, &n), dc.ctx,
+          "intersect_occ");
+    auto vox = torch::empty({n, 3}, torch::TensorOptions().device(t.device()).dtype(torch::kInt32));
+    check(ovx_fdg_occupancy_finish(dc.ctx, stream, n ? vox.data_ptr<int32_t>() : nullptr), dc.ctx, "intersect_occ");
+    return vox;
+}
+
+PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
+{
+    m.def("mesh_to_flexible_dual_grid_cuda", &mesh_to_flexible_dual_grid_cuda, py::call_guard<py::gil_scoped_release>());
+    m.def("mesh_to_flexible_dual_grid_cuda_ex", &mesh_to_flexible_dual_grid_cuda_ex, py::call_guard<py::gil_scoped_release>());
+    m.def("intersect_occ_cuda", &intersect_occ_cuda, py::call_guard<py::gil_scoped_release>());
+}

@@ -1,0 +1,215 @@
+"""Mesh -> flexible dual grid, B200 implementation behind the reference API.
+
+Signature, defaults, argument checks and the derivation of ``aabb`` /
+``voxel_size`` / ``grid_size`` follow the reference wrapper
+(``o_voxel/convert/flexible_dual_grid.py:38-205`` and ``:208-329``): the same
+assertions with the same messages, float32 ``voxel_size = (aabb1 - aabb0) /
+grid_size`` computed on the host, ``grid_range = [0, 0, 0, gx, gy, gz]``, and
+vertices shifted by ``aabb[0]`` in float32 before the conversion (fused into the
+kernels here when ``aabb[0]`` is known on the host).
+
+Differences, all deliberate:
+  * CUDA tensors only.  There is no CPU path in this product; CPU inputs raise
+    ``RuntimeError`` (the reference would run its single-threaded CPU code).
+  * int64 faces are consumed directly instead of being cast to int32; indices
+    outside ``[0, V)`` raise ``RuntimeError`` (the reference reads out of bounds).
+  * Output rows are in a deterministic brick order (8x8x8 bricks, x fastest),
+    not in an arbitrary order.  Values are bit-identical to the reference CPU path.
+"""
+from typing import Any, List, Optional, Tuple, Union
+
+import numpy as np
+import torch
+
+FloatArrayLike = Union[float, List[Any], Tuple[Any, ...], np.ndarray, torch.Tensor]
+IntArrayLike = Union[int, List[Any], Tuple[Any, ...], np.ndarray, torch.Tensor]
+ArrayLike = Union[List[Any], Tuple[Any, ...], np.ndarray, torch.Tensor]
+
+__all__ = [
+    "mesh_to_flexible_dual_grid",
+    "intersect_occ",
+]
+
+_C = None
+
+
+def _ext():
+    """The compiled extension; importing it fails loudly if it was not built."""
+    global _C
+    if _C is None:
+        from .. import _C as ext  # noqa: WPS433
+
+        _C = ext
+    return _C
+
+
+def _grid_setup(vertices, faces, voxel_size, grid_size, aabb):
+    """Argument normalisation shared by both entry points (reference wrapper :79-178)."""
+    assert isinstance(vertices, torch.Tensor), f"vertices must be a torch.Tensor, but got {type(vertices)}"
+    assert isinstance(faces, torch.Tensor), f"faces must be a torch.Tensor, but got {type(faces)}"
+    assert vertices.dim() == 2, f"vertices must be a 2D tensor, but got {vertices.shape}"
+    assert vertices.size(1) == 3, f"vertices must have 3 columns, but got {vertices.size(1)}"
+    assert faces.dim() == 2, f"faces must be a 2D tensor, but got {faces.shape}"
+    assert faces.size(1) == 3, f"faces must have 3 columns, but got {faces.size(1)}"
+    assert vertices.device == faces.device, "vertices and faces must be on the same device"
+    assert voxel_size is not None or grid_size is not None, "Either voxel_size or grid_size must be provided"
+
+    device = vertices.device
+    vertices = vertices.to(device=device, dtype=torch.float32).contiguous()
+    if faces.dtype not in (torch.int32, torch.int64):
+        faces = faces.to(device=device, dtype=torch.int32)
+    faces = faces.contiguous()
+    voxel_size_cpu = None
+    grid_size_cpu = None
+    aabb_cpu = None
+
+    if voxel_size is not None:
+        if isinstance(voxel_size, float):
+            voxel_size = [voxel_size, voxel_size, voxel_size]
+        if isinstance(voxel_size, (list, tuple)):
+            voxel_size = np.array(voxel_size)
+        if isinstance(voxel_size, np.ndarray):
+            voxel_size_cpu = torch.tensor(voxel_size, dtype=torch.float32)
+            voxel_size = voxel_size_cpu
+        else:
+            assert isinstance(voxel_size, torch.Tensor), f"voxel_size must be a float, list, tuple, np.ndarray, or torch.Tensor, but got {type(voxel_size)}"
+            assert not voxel_size.is_cuda, "voxel_size Tensor metadata must be on CPU; pass Python values to avoid implicit CUDA sync"
+            voxel_size_cpu = voxel_size.to(dtype=torch.float32).contiguous()
+        assert isinstance(voxel_size, torch.Tensor), f"voxel_size must be a float, list, tuple, np.ndarray, or torch.Tensor, but got {type(voxel_size)}"
+        voxel_size = voxel_size_cpu.to(device=device).contiguous()
+        assert voxel_size.dim() == 1, f"voxel_size must be a 1D tensor, but got {voxel_size.shape}"
+        assert voxel_size.size(0) == 3, f"voxel_size must have 3 elements, but got {voxel_size.size(0)}"
+
+    if grid_size is not None:
+        if isinstance(grid_size, int):
+            grid_size = [grid_size, grid_size, grid_size]
+        if isinstance(grid_size, (list, tuple)):
+            grid_size = np.array(grid_size)
+        if isinstance(grid_size, np.ndarray):
+            grid_size_cpu = torch.tensor(grid_size, dtype=torch.int32)
+            grid_size = grid_size_cpu
+        else:
+            assert isinstance(grid_size, torch.Tensor), f"grid_size must be an int, list, tuple, np.ndarray, or torch.Tensor, but got {type(grid_size)}"
+            assert not grid_size.is_cuda, "grid_size Tensor metadata must be on CPU; pass Python values to avoid implicit CUDA sync"
+            grid_size_cpu = grid_size.to(dtype=torch.int32).contiguous()
+        assert isinstance(grid_size, torch.Tensor), f"grid_size must be an int, list, tuple, np.ndarray, or torch.Tensor, but got {type(grid_size)}"
+        grid_size = grid_size_cpu.to(device=device).contiguous()
+        assert grid_size.dim() == 1, f"grid_size must be a 1D tensor, but got {grid_size.shape}"
+        assert grid_size.size(0) == 3, f"grid_size must have 3 elements, but got {grid_size.size(0)}"
+
+    if aabb is not None:
+        if isinstance(aabb, (list, tuple)):
+            aabb = np.array(aabb)
+        if isinstance(aabb, np.ndarray):
+            aabb_cpu = torch.tensor(aabb, dtype=torch.float32)
+            aabb = aabb_cpu
+        else:
+            assert isinstance(aabb, torch.Tensor), f"aabb must be a list, tuple, np.ndarray, or torch.Tensor, but got {type(aabb)}"
+            assert not aabb.is_cuda, "aabb Tensor metadata must be on CPU; pass Python values to avoid implicit CUDA sync"
+            aabb_cpu = aabb.to(dtype=torch.float32).contiguous()
+        assert isinstance(aabb, torch.Tensor), f"aabb must be a list, tuple, np.ndarray, or torch.Tensor, but got {type(aabb)}"
+        aabb = aabb_cpu.to(device=device).contiguous()
+        assert aabb.dim() == 2, f"aabb must be a 2D tensor, but got {aabb.shape}"
+        assert aabb.size(0) == 2, f"aabb must have 2 rows, but got {aabb.size(0)}"
+        assert aabb.size(1) == 3, f"aabb must have 3 columns, but got {aabb.size(1)}"
+
+    if aabb is None:
+        min_xyz = vertices.min(dim=0).values
+        max_xyz = vertices.max(dim=0).values
+        if voxel_size is not None:
+            padding = torch.ceil((max_xyz - min_xyz) / voxel_size) * voxel_size - (max_xyz - min_xyz)
+            min_xyz -= padding * 0.5
+            max_xyz += padding * 0.5
+        if grid_size is not None:
+            padding = (max_xyz - min_xyz) / (grid_size - 1)
+            min_xyz -= padding * 0.5
+            max_xyz += padding * 0.5
+        aabb = torch.stack([min_xyz, max_xyz], dim=0).float().contiguous()
+
+    if voxel_size_cpu is None:
+        assert grid_size_cpu is not None
+        if aabb_cpu is None:
+            assert not aabb.is_cuda, "CUDA inputs require CPU aabb or explicit voxel_size to avoid implicit CUDA sync"
+            aabb_cpu = aabb.detach()
+        voxel_size_cpu = ((aabb_cpu[1] - aabb_cpu[0]) / grid_size_cpu).to(dtype=torch.float32).contiguous()
+    if grid_size_cpu is None:
+        assert voxel_size_cpu is not None
+        if aabb_cpu is None:
+            assert not aabb.is_cuda, "CUDA inputs require CPU aabb or explicit grid_size to avoid implicit CUDA sync"
+            aabb_cpu = aabb.detach()
+        grid_size_cpu = ((aabb_cpu[1] - aabb_cpu[0]) / voxel_size_cpu).round().to(dtype=torch.int32).contiguous()
+    voxel_size_arg = [float(x) for x in voxel_size_cpu.tolist()]
+    grid_range_arg = [0, 0, 0] + [int(x) for x in grid_size_cpu.tolist()]
+    return vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg
+
+
+def _require_cuda(t: torch.Tensor, name: str):
+    if not t.is_cuda:
+        raise RuntimeError(f"{name}: this implementation runs on CUDA tensors only (got a {t.device} tensor)")
+
+
+@torch.no_grad()
+def mesh_to_flexible_dual_grid(
+    vertices: torch.Tensor,
+    faces: torch.Tensor,
+    voxel_size: Optional[FloatArrayLike] = None,
+    grid_size: Optional[IntArrayLike] = None,
+    aabb: Optional[ArrayLike] = None,
+    face_weight: float = 1.0,
+    boundary_weight: float = 1.0,
+    regularization_weight: float = 0.1,
+    timing: bool = False,
+) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+    """
+    Convert a triangle mesh into a sparse flexible dual grid.
+
+    Args:
+        vertices (torch.Tensor): [V, 3] mesh vertices (CUDA).
+        faces (torch.Tensor): [F, 3] triangle vertex indices (CUDA, int32 or int64).
+        voxel_size: size of each voxel (float or 3 values); one of voxel_size/grid_size is required.
+        grid_size: voxels per axis (int or 3 values).
+        aabb: [[x0, y0, z0], [x1, y1, z1]] bounding box; computed from the vertices if omitted.
+        face_weight (float): gates the face term of the QEF (> 0 adds it).
+        boundary_weight (float): weight of the boundary-edge term of the QEF (> 0 adds it).
+        regularization_weight (float): weight pulling each dual vertex toward the mean intersection point.
+        timing (bool): accepted for compatibility; ignored (as on the reference CUDA path).
+
+    Returns:
+        voxel_indices (torch.Tensor): [N, 3] int32 occupied voxel coordinates.
+        dual_vertices (torch.Tensor): [N, 3] float32 dual vertices in grid-local coordinates
+            (``aabb[0]`` subtracted, not added back, as in the reference).
+        intersected (torch.Tensor): [N, 3] bool; axis a is set when the voxel's edge along a
+            starting at its min corner crosses the surface.
+    """
+    vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg = _grid_setup(vertices, faces, voxel_size, grid_size, aabb)
+    _require_cuda(vertices, "mesh_to_flexible_dual_grid")
+    if aabb_cpu is not None:
+        origin = [float(x) for x in aabb_cpu[0].tolist()]
+        return _ext().mesh_to_flexible_dual_grid_cuda_ex(vertices, faces, origin, voxel_size_arg, grid_range_arg,
+                                                         float(face_weight), float(boundary_weight),
+                                                         float(regularization_weight))
+    # aabb derived on the device: shift with torch, exactly like the reference wrapper
+    vertices = vertices - aabb[0].reshape(1, 3)
+    return _ext().mesh_to_flexible_dual_grid_cuda(vertices, faces, voxel_size_arg, grid_range_arg, float(face_weight),
+                                                  float(boundary_weight), float(regularization_weight))
+
+
+@torch.no_grad()
+def intersect_occ(
+    vertices: torch.Tensor,
+    faces: torch.Tensor,
+    voxel_size: Optional[FloatArrayLike] = None,
+    grid_size: Optional[IntArrayLike] = None,
+    aabb: Optional[ArrayLike] = None,
+) -> torch.Tensor:
+    """
+    Return only the voxel coordinates intersected by a triangle mesh ([N, 3] int32).
+
+    Same grid setup and occupancy rules as mesh_to_flexible_dual_grid, without
+    quadrics or dual vertices.
+    """
+    vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg = _grid_setup(vertices, faces, voxel_size, grid_size, aabb)
+    _require_cuda(vertices, "intersect_occ")
+    vertices = vertices - aabb[0].reshape(1, 3)
+    triangles = vertices[faces.to(dtype=torch.long)].contiguous()
+    return _ext().intersect_occ_cuda(triangles, voxel_size_arg, grid_range_arg)

@@ -1,0 +1,137 @@
+"""ctypes binding of the C ABI in include/ovx_fdg.h (libovx_fdg.so).
+
+This is the binding a non-torch host (or a test) uses to reach the library
+without the torch extension.  Device memory for inputs and outputs is supplied
+by the caller as raw CUDA pointers; the helpers below take torch CUDA tensors
+for convenience.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libovx_fdg.so")
+
+OK = 0
+STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "BAD_FACE_INDEX", 3: "CUDA_ERROR", 4: "OUT_OF_MEMORY", 5: "CAPACITY",
+          6: "INTERNAL"}
+
+# (name, restype, argtypes) for every function declared in include/ovx_fdg.h
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_F = ctypes.c_float
+PROTOTYPES = [
+    ("ovx_fdg_context_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    ("ovx_fdg_context_destroy", None, [_P]),
+    ("ovx_fdg_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("ovx_fdg_last_error", ctypes.c_char_p, [_P]),
+    ("ovx_fdg_workspace_bytes", _I64, [_P]),
+    ("ovx_fdg_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.c_int32, _I64, _P, _P, _F, _F, _F, ctypes.POINTER(_I64)]),
+    ("ovx_fdg_finish", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("ovx_fdg_occupancy_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.POINTER(_I64)]),
+    ("ovx_fdg_occupancy_finish", ctypes.c_int, [_P, _P, _P]),
+]
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("voxel_size", ctypes.c_float * 3), ("grid_min", ctypes.c_int32 * 3), ("grid_max", ctypes.c_int32 * 3)]
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libovx_fdg.so is not built ({LIB_PATH}); run o-voxel-gpu_b200/build.py")
+        _LIB = ctypes.CDLL(LIB_PATH)
+        for name, res, args in PROTOTYPES:
+            fn = getattr(_LIB, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _LIB
+
+
+class FdgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def make_grid(voxel_size, grid_range) -> Grid:
+    g = Grid()
+    for a in range(3):
+        g.voxel_size[a] = float(voxel_size[a])
+        g.grid_min[a] = int(grid_range[a])
+        g.grid_max[a] = int(grid_range[3 + a])
+    return g
+
+
+class Context:
+    """One ovx_fdg_context on one device."""
+
+    def __init__(self, device: int = 0):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.ovx_fdg_context_create(int(device), ctypes.byref(h))
+        if rc != OK:
+            raise FdgError(rc, "ovx_fdg_context_create")
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            self._lib.ovx_fdg_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != OK:
+            msg = self._lib.ovx_fdg_last_error(self.handle)
+            raise FdgError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def workspace_bytes(self) -> int:
+        return int(self._lib.ovx_fdg_workspace_bytes(self.handle))
+
+    def mesh_to_fdg(self, vertices, faces, origin, voxel_size, grid_range, fw, bw, rw, stream=None):
+        """vertices: CUDA float32 [V,3]; faces: CUDA int32/int64 [F,3]; returns torch tensors."""
+        import torch
+
+        st = ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream(vertices.device).cuda_stream)
+        grid = make_grid(voxel_size, grid_range)
+        org = (ctypes.c_float * 3)(*[float(x) for x in origin]) if origin is not None else None
+        n = ctypes.c_int64(0)
+        rc = self._lib.ovx_fdg_begin(self.handle, st, ctypes.c_void_p(vertices.data_ptr()), vertices.shape[0],
+                                     ctypes.c_void_p(faces.data_ptr() if faces.numel() else 0), faces.element_size(),
+                                     faces.shape[0], ctypes.cast(org, ctypes.c_void_p) if org is not None else None,
+                                     ctypes.byref(grid), float(fw), float(bw), float(rw), ctypes.byref(n))
+        self._check(rc, "ovx_fdg_begin")
+        N = n.value
+        vox = torch.empty((N, 3), dtype=torch.int32, device=vertices.device)
+        dual = torch.empty((N, 3), dtype=torch.float32, device=vertices.device)
+        inter = torch.empty((N, 3), dtype=torch.bool, device=vertices.device)
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t.numel() else 0)  # noqa: E731
+        rc = self._lib.ovx_fdg_finish(self.handle, st, ptr(vox), ptr(dual), ptr(inter))
+        self._check(rc, "ovx_fdg_finish")
+        return vox, dual, inter
+
+    def occupancy(self, triangles, voxel_size, grid_range, stream=None):
+        import torch
+
+        st = ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream(triangles.device).cuda_stream)
+        grid = make_grid(voxel_size, grid_range)
+        n = ctypes.c_int64(0)
+        rc = self._lib.ovx_fdg_occupancy_begin(self.handle, st, ctypes.c_void_p(triangles.data_ptr() if triangles.numel() else 0),
+                                               triangles.shape[0], ctypes.byref(grid), ctypes.byref(n))
+        self._check(rc, "ovx_fdg_occupancy_begin")
+        vox = torch.empty((n.value, 3), dtype=torch.int32, device=triangles.device)
+        rc = self._lib.ovx_fdg_occupancy_finish(self.handle, st, ctypes.c_void_p(vox.data_ptr() if vox.numel() else 0))
+        self._check(rc, "ovx_fdg_occupancy_finish")
+        return vox
