@@ -99,6 +99,14 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
                    uint8_t *intersected);
 
 /*
+ * Waits for the work `finish` enqueued on `stream` and reports device-side
+ * consistency checks of that stage (the reference has no counterpart: its
+ * stages synchronise after every step).  Optional: finish already reports
+ * argument and launch errors.
+ */
+int ovx_fdg_sync_status(ovx_fdg_context *ctx, void *stream);
+
+/*
  * Occupancy only (reference intersect_occ).  triangles: device float32
  * [num_triangles, 3, 3] in grid-local coordinates (already shifted), as the
  * reference operator takes them.  begin returns N; finish writes int32 [N,3].

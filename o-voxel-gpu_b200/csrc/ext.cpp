@@ -13,6 +13,8 @@
 // extra cast and shift passes over the inputs.
 //
 // All compute goes through the C ABI in include/ovx_fdg.h (libovx_fdg.so).
+// Setting OVX_FDG_CHECK in the environment makes every call wait for its
+// device-side consistency checks (ovx_fdg_sync_status) and raise on failure.
 // Outputs come from torch's caching allocator on the input's device, work runs
 // on torch's current stream, and the GIL is released during the call, as in
 // the reference.  Errors raise RuntimeError (TORCH_CHECK), as in the reference.
@@ -20,6 +22,7 @@
 #include <ATen/cuda/CUDAContext.h>
 #include <c10/cuda/CUDAGuard.h>
 
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -106,6 +109,9 @@ std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Ten
     check(ovx_fdg_finish(dc.ctx, stream, n ? vox.data_ptr<int32_t>() : nullptr, n ? dual.data_ptr<float>() : nullptr,
                          n ? reinterpret_cast<uint8_t *>(inter.data_ptr<bool>()) : nullptr),
           dc.ctx, "mesh_to_flexible_dual_grid (quadrics)");
+    static const bool sync_check = std::getenv("OVX_FDG_CHECK") != nullptr;
+    if (sync_check)
+        check(ovx_fdg_sync_status(dc.ctx, stream), dc.ctx, "mesh_to_flexible_dual_grid (device checks)");
     return std::make_tuple(vox, dual, inter);
 }
 

@@ -33,6 +33,7 @@ struct Grid
     int size[3];  // gmax - gmin
     int nb[3];    // bricks per axis
     long long nbricks;
+    double rv[3]; // 1 / (double)vs, for trunc_div
 };
 
 // ---- x86 conversion semantics: out-of-range and NaN give INT_MIN ----
@@ -47,6 +48,27 @@ __device__ __forceinline__ int trunc_f2i(float f)
 __device__ __forceinline__ int clampi(int v, int lo, int hi)
 {
     return (v < lo) ? lo : (hi < v) ? hi : v;
+}
+
+// trunc_d2i(a / b) with the IEEE quotient, computed from q = a * rb
+// (rb = 1/b) when that is provably equivalent.  |q - a/b| and |RN(a/b) - a/b|
+// are both below 2.3e-16 |a/b|, so if q's fractional part keeps 1e-12|q| away
+// from an integer, RN(a/b) lies in the same open unit interval and truncates
+// to the same integer.  Otherwise (near an integer, near zero, out of int
+// range, NaN) the exact division decides.
+__device__ __forceinline__ int trunc_div(double a, double b, double rb)
+{
+    const double q = a * rb;
+    const double aq = fabs(q);
+    if (aq < 2.0e9)
+    {
+        const double fl = floor(q);
+        const double fr = q - fl;
+        const double d = 1e-12 * (aq > 1.0 ? aq : 1.0);
+        if (fr > d && fr < 1.0 - d)
+            return (int)(q >= 0.0 ? fl : fl + 1.0);
+    }
+    return trunc_d2i(a / b);
 }
 __device__ __forceinline__ float dot3f(float a0, float a1, float a2, float b0, float b1, float b2)
 {
@@ -179,10 +201,11 @@ __device__ __forceinline__ void axis_setup(const float v[3][3], int ax2, const G
         for (int c = 0; c < 3; ++c)
             s.t[k][c] = t[k][c];
     const double vy = (double)g.vs[s.ax1];
+    const double ry = g.rv[s.ax1];
     const int lo = g.gmin[s.ax1], hi = g.gmax[s.ax1] - 1;
-    s.start = clampi(trunc_d2i(t[0][1] / vy), lo, hi);
-    s.mid = clampi(trunc_d2i(t[1][1] / vy), lo, hi);
-    s.end = clampi(trunc_d2i(t[2][1] / vy), lo, hi);
+    s.start = clampi(trunc_div(t[0][1], vy, ry), lo, hi);
+    s.mid = clampi(trunc_div(t[1][1], vy, ry), lo, hi);
+    s.end = clampi(trunc_div(t[2][1], vy, ry), lo, hi);
 }
 
 // Column bound of the projected triangle on ax0 (for work estimates and tiling):
@@ -196,8 +219,9 @@ __device__ __forceinline__ void axis_col_bounds(const AxisScan &s, const Grid &g
         mx = s.t[k][0] > mx ? s.t[k][0] : mx;
     }
     const double vx = (double)g.vs[s.ax0];
-    clo = clampi(trunc_d2i(mn / vx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
-    chi = clampi(trunc_d2i(mx / vx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
+    const double rx = g.rv[s.ax0];
+    clo = clampi(trunc_div(mn, vx, rx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
+    chi = clampi(trunc_div(mx, vx, rx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
 }
 
 // Events of one scan row, columns restricted to [col_lo, col_hi).
@@ -246,11 +270,13 @@ __device__ __forceinline__ void scan_row(const AxisScan &s, int yi, int col_lo, 
         t4z = tmp;
     }
     const double vx = (double)g.vs[s.ax0];
-    const int ls = clampi(trunc_d2i(t3x / vx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
-    const int le = clampi(trunc_d2i(t4x / vx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
+    const double rx = g.rv[s.ax0];
+    const int ls = clampi(trunc_div(t3x, vx, rx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
+    const int le = clampi(trunc_div(t4x, vx, rx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
     const int x0 = ls > col_lo ? ls : col_lo;
     const int x1 = le < col_hi ? le : col_hi;
     const double vz = (double)g.vs[s.ax2];
+    const double rz = g.rv[s.ax2];
     for (int xi = x0; xi < x1; ++xi)
     {
         const float xf = (float)(xi + 1) * g.vs[s.ax0];
@@ -263,7 +289,7 @@ __device__ __forceinline__ void scan_row(const AxisScan &s, int yi, int col_lo, 
             const double al = (x - t3x) / (t4x - t3x);
             z = (1.0 - al) * t3z + al * t4z;
         }
-        const int zi = trunc_d2i(z / vz);
+        const int zi = trunc_div(z, vz, rz);
         if (zi >= g.gmin[s.ax2] && zi < g.gmax[s.ax2])
             emit(xi, yi, zi, xf, yf, z);
     }
@@ -282,6 +308,24 @@ struct FaceSetup
     int bmin[3], bmax[3];
 };
 
+// Face-test voxel box [bmin, bmax) of a triangle (flexible_dual_grid.cpp:314-322).
+__device__ __forceinline__ void face_box(const float v[3][3], const Grid &g, int bmin[3], int bmax[3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+    {
+        float mn = v[0][i], mx = v[0][i];
+        mn = (v[1][i] < mn) ? v[1][i] : mn;
+        mn = (v[2][i] < mn) ? v[2][i] : mn;
+        mx = (mx < v[1][i]) ? v[1][i] : mx;
+        mx = (mx < v[2][i]) ? v[2][i] : mx;
+        const int l = trunc_f2i(mn / g.vs[i]);
+        const int h = trunc_f2i(mx / g.vs[i] + 1.0f);
+        bmin[i] = (l < g.gmin[i]) ? g.gmin[i] : l;
+        bmax[i] = (g.gmax[i] < h) ? g.gmax[i] : h;
+    }
+}
+
 __device__ __forceinline__ void face_setup(const float v[3][3], const Grid &g, FaceSetup &fs)
 {
     float e[3][3];
@@ -293,18 +337,7 @@ __device__ __forceinline__ void face_setup(const float v[3][3], const Grid &g, F
     }
     tri_normal(v, fs.n);
     const float *n = fs.n;
-    for (int i = 0; i < 3; ++i)
-    {
-        float mn = v[0][i], mx = v[0][i];
-        mn = (v[1][i] < mn) ? v[1][i] : mn;
-        mn = (v[2][i] < mn) ? v[2][i] : mn;
-        mx = (mx < v[1][i]) ? v[1][i] : mx;
-        mx = (mx < v[2][i]) ? v[2][i] : mx;
-        const int l = trunc_f2i(mn / g.vs[i]);
-        const int h = trunc_f2i(mx / g.vs[i] + 1.0f);
-        fs.bmin[i] = (l < g.gmin[i]) ? g.gmin[i] : l;
-        fs.bmax[i] = (g.gmax[i] < h) ? g.gmax[i] : h;
-    }
+    face_box(v, g, fs.bmin, fs.bmax);
     const float c0 = n[0] > 0.0f ? g.vs[0] : 0.0f;
     const float c1 = n[1] > 0.0f ? g.vs[1] : 0.0f;
     const float c2 = n[2] > 0.0f ? g.vs[2] : 0.0f;
@@ -668,21 +701,12 @@ __device__ __forceinline__ float qef_err4(const float Q[16], const float p[4])
     return dot4v(r, p);
 }
 
-// Regularise toward the mass point, solve, and run the constrained search.
-__device__ __forceinline__ void solve_voxel(const int coord[3], const Grid &g, const float q_in[10], const float mean[3], float cnt,
-                                            float rw, float out[3])
+// Regularisation toward the mass point (flexible_dual_grid.cpp:780-792): Q += (rw*cnt) * Qreg.
+__device__ __forceinline__ void regularize(const float q_in[10], const float mean[3], float cnt, float rw, float q[10])
 {
-    float q[10];
 #pragma unroll
     for (int i = 0; i < 10; ++i)
         q[i] = q_in[i];
-    float mn[3], mx[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-    {
-        mn[i] = (float)coord[i] * g.vs[i];
-        mx[i] = (float)(coord[i] + 1) * g.vs[i];
-    }
     if (rw > 0.0f)
     {
         const float p0 = mean[0] / cnt, p1 = mean[1] / cnt, p2 = mean[2] / cnt;
@@ -699,96 +723,116 @@ __device__ __forceinline__ void solve_voxel(const int coord[3], const Grid &g, c
         q[8] = q[8] + s * (-p2);
         q[9] = q[9] + s * pp;
     }
-    const float Q[16] = {q[0], q[1], q[2], q[3], q[1], q[4], q[5], q[6], q[2], q[5], q[7], q[8], q[3], q[6], q[8], q[9]};
-    const float A[9] = {Q[0], Q[1], Q[2], Q[4], Q[5], Q[6], Q[8], Q[9], Q[10]};
-    const float bb[3] = {-Q[3], -Q[7], -Q[11]};
-    float v[3];
-    cpqr_solve<3>(A, bb, v);
-    if (!(v[0] >= mn[0] && v[0] <= mx[0] && v[1] >= mn[1] && v[1] <= mx[1] && v[2] >= mn[2] && v[2] <= mx[2]))
+}
+
+__device__ __forceinline__ void voxel_box(const int coord[3], const Grid &g, float mn[3], float mx[3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
     {
-        float best = __int_as_float(0x7f800000);
+        mn[i] = (float)coord[i] * g.vs[i];
+        mx[i] = (float)(coord[i] + 1) * g.vs[i];
+    }
+}
+
+// Unconstrained minimiser A v = -b (flexible_dual_grid.cpp:795-797); true if it lies in the voxel box.
+__device__ __forceinline__ bool solve_unconstrained(const int coord[3], const Grid &g, const float q[10], float v[3])
+{
+    const float A[9] = {q[0], q[1], q[2], q[1], q[4], q[5], q[2], q[5], q[7]};
+    const float bb[3] = {-q[3], -q[6], -q[8]};
+    cpqr_solve<3>(A, bb, v);
+    float mn[3], mx[3];
+    voxel_box(coord, g, mn, mx);
+    return v[0] >= mn[0] && v[0] <= mx[0] && v[1] >= mn[1] && v[1] <= mx[1] && v[2] >= mn[2] && v[2] <= mx[2];
+}
+
+// Constrained search over the box faces, edges and corners (flexible_dual_grid.cpp:799-979),
+// starting from the unconstrained solution, strict `<` in the reference order.
+__device__ __forceinline__ void solve_constrained(const int coord[3], const Grid &g, const float q[10], float v[3])
+{
+    solve_unconstrained(coord, g, q, v);
+    float mn[3], mx[3];
+    voxel_box(coord, g, mn, mx);
+    const float Q[16] = {q[0], q[1], q[2], q[3], q[1], q[4], q[5], q[6], q[2], q[5], q[7], q[8], q[3], q[6], q[8], q[9]};
+    float best = __int_as_float(0x7f800000);
 #pragma unroll 1
-        for (int fa = 0; fa < 3; ++fa)
+    for (int fa = 0; fa < 3; ++fa)
+    {
+        const int a1 = (fa + 1) % 3, a2 = (fa + 2) % 3;
+        const float A2[4] = {Q[a1 * 4 + a1], Q[a1 * 4 + a2], Q[a2 * 4 + a1], Q[a2 * 4 + a2]};
+        const float B2[4] = {Q[a1 * 4 + fa], Q[a1 * 4 + 3], Q[a2 * 4 + fa], Q[a2 * 4 + 3]};
+#pragma unroll 1
+        for (int bound = 0; bound < 2; ++bound)
         {
-            const int a1 = (fa + 1) % 3, a2 = (fa + 2) % 3;
-            const float A2[4] = {Q[a1 * 4 + a1], Q[a1 * 4 + a2], Q[a2 * 4 + a1], Q[a2 * 4 + a2]};
-            const float B2[4] = {Q[a1 * 4 + fa], Q[a1 * 4 + 3], Q[a2 * 4 + fa], Q[a2 * 4 + 3]};
-#pragma unroll 1
-            for (int bound = 0; bound < 2; ++bound)
+            const float fv = bound == 0 ? mn[fa] : mx[fa];
+            const float rhs[2] = {(-B2[0]) * fv + (-B2[1]) * 1.0f, (-B2[2]) * fv + (-B2[3]) * 1.0f};
+            float x2[2];
+            cpqr_solve<2>(A2, rhs, x2);
+            if (x2[0] >= mn[a1] && x2[0] <= mx[a1] && x2[1] >= mn[a2] && x2[1] <= mx[a2])
             {
-                const float fv = bound == 0 ? mn[fa] : mx[fa];
-                const float rhs[2] = {(-B2[0]) * fv + (-B2[1]) * 1.0f, (-B2[2]) * fv + (-B2[3]) * 1.0f};
-                float x2[2];
-                cpqr_solve<2>(A2, rhs, x2);
-                if (x2[0] >= mn[a1] && x2[0] <= mx[a1] && x2[1] >= mn[a2] && x2[1] <= mx[a2])
+                float p[4];
+                p[fa] = fv;
+                p[a1] = x2[0];
+                p[a2] = x2[1];
+                p[3] = 1.0f;
+                const float err = qef_err4(Q, p);
+                if (err < best)
                 {
-                    float p[4];
-                    p[fa] = fv;
-                    p[a1] = x2[0];
-                    p[a2] = x2[1];
-                    p[3] = 1.0f;
-                    const float err = qef_err4(Q, p);
-                    if (err < best)
-                    {
-                        best = err;
-                        v[0] = p[0];
-                        v[1] = p[1];
-                        v[2] = p[2];
-                    }
+                    best = err;
+                    v[0] = p[0];
+                    v[1] = p[1];
+                    v[2] = p[2];
                 }
-            }
-        }
-#pragma unroll 1
-        for (int fr = 0; fr < 3; ++fr)
-        {
-            const int a1 = (fr + 1) % 3, a2 = (fr + 2) % 3;
-            const float a = Q[fr * 4 + fr];
-            const float b0 = Q[fr * 4 + a1], b1 = Q[fr * 4 + a2], b2 = Q[fr * 4 + 3];
-#pragma unroll 1
-            for (int cc = 0; cc < 4; ++cc)
-            {
-                const float u1 = (cc >> 1) == 0 ? mn[a1] : mx[a1];
-                const float u2 = (cc & 1) == 0 ? mn[a2] : mx[a2];
-                const float xf = -(dot3f(b0, b1, b2, u1, u2, 1.0f)) / a;
-                if (xf >= mn[fr] && xf <= mx[fr])
-                {
-                    float p[4];
-                    p[fr] = xf;
-                    p[a1] = u1;
-                    p[a2] = u2;
-                    p[3] = 1.0f;
-                    const float err = qef_err4(Q, p);
-                    if (err < best)
-                    {
-                        best = err;
-                        v[0] = p[0];
-                        v[1] = p[1];
-                        v[2] = p[2];
-                    }
-                }
-            }
-        }
-#pragma unroll 1
-        for (int cn = 0; cn < 8; ++cn)
-        {
-            float p[4];
-            p[0] = (cn & 4) ? mn[0] : mx[0];
-            p[1] = (cn & 2) ? mn[1] : mx[1];
-            p[2] = (cn & 1) ? mn[2] : mx[2];
-            p[3] = 1.0f;
-            const float err = qef_err4(Q, p);
-            if (err < best)
-            {
-                best = err;
-                v[0] = p[0];
-                v[1] = p[1];
-                v[2] = p[2];
             }
         }
     }
-    out[0] = v[0];
-    out[1] = v[1];
-    out[2] = v[2];
+#pragma unroll 1
+    for (int fr = 0; fr < 3; ++fr)
+    {
+        const int a1 = (fr + 1) % 3, a2 = (fr + 2) % 3;
+        const float a = Q[fr * 4 + fr];
+        const float b0 = Q[fr * 4 + a1], b1 = Q[fr * 4 + a2], b2 = Q[fr * 4 + 3];
+#pragma unroll 1
+        for (int cc = 0; cc < 4; ++cc)
+        {
+            const float u1 = (cc >> 1) == 0 ? mn[a1] : mx[a1];
+            const float u2 = (cc & 1) == 0 ? mn[a2] : mx[a2];
+            const float xf = -(dot3f(b0, b1, b2, u1, u2, 1.0f)) / a;
+            if (xf >= mn[fr] && xf <= mx[fr])
+            {
+                float p[4];
+                p[fr] = xf;
+                p[a1] = u1;
+                p[a2] = u2;
+                p[3] = 1.0f;
+                const float err = qef_err4(Q, p);
+                if (err < best)
+                {
+                    best = err;
+                    v[0] = p[0];
+                    v[1] = p[1];
+                    v[2] = p[2];
+                }
+            }
+        }
+    }
+#pragma unroll 1
+    for (int cn = 0; cn < 8; ++cn)
+    {
+        float p[4];
+        p[0] = (cn & 4) ? mn[0] : mx[0];
+        p[1] = (cn & 2) ? mn[1] : mx[1];
+        p[2] = (cn & 1) ? mn[2] : mx[2];
+        p[3] = 1.0f;
+        const float err = qef_err4(Q, p);
+        if (err < best)
+        {
+            best = err;
+            v[0] = p[0];
+            v[1] = p[1];
+            v[2] = p[2];
+        }
+    }
 }
 
 } // namespace ovx

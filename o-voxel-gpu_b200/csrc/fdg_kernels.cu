@@ -1,34 +1,44 @@
 // fdg_kernels.cu -- B200 mesh -> flexible dual grid: kernels, host
 // orchestration and the C ABI declared in include/ovx_fdg.h.
 //
-// Pipeline (one mesh; every stage is a plain SIMT kernel -- nothing here is a
-// dense contraction, so there is no tensor-core work):
+// Everything is plain SIMT work (scanline rasterisation, bitsets, counting
+// sorts, 3x3 solves): nothing is a dense contraction, so no tensor cores.
 //
-//  begin (occupancy)
-//   tri_pass<MARK>        one thread per triangle: scanline events of the three
-//                         projection axes (FP64, reference arithmetic) set bits in
-//                         a dense brick-ordered occupancy bitmap; (triangle,axis)
-//                         pairs with many events and triangles with a large face
-//                         box go to two work lists.
-//   large_scan<MARK>      one CTA per listed (triangle,axis), threads over
-//                         (row, 8-column chunk) tiles.
-//   brick_count + scan    popcount per 8^3 brick, exclusive scan -> N.
-//   edge_* (boundary_weight>0)
-//                         undirected edges bucketed by their smaller vertex
-//                         (counting sort); edges used by one face -> boundary list.
-//  finish (quadrics + solve)
-//   brick_emit            voxel rows in brick order + per-word row bases.
-//   *<COUNT>              replay events / face tests / boundary walks, count
-//                         quadric contributions per voxel.
-//   scan                  per-voxel segment offsets -> E.
-//   *<FILL>               replay again, write (order key, payload) per contribution.
-//   final_short/long      per voxel: sort its contributions by the reference's
-//                         accumulation order, sum them sequentially in FP32 (the
-//                         reference order, so the sums are bit-identical),
-//                         regularise, solve, write dual vertex and flags.
+// Data layout in HBM (one conversion):
+//   bits    dense occupancy bitmap, brick-major: brick b (x-fastest over the
+//           brick grid) owns 16 consecutive 32-bit words; word lz*2+(ly>>2),
+//           bit (ly&3)*8+lx (64 B per 8^3 brick, 16.7 MB at grid 512)
+//   bbase   exclusive scan of per-brick popcounts = first output row of each
+//           brick; rows are brick-major, x-fastest inside a brick
+//   roff    exclusive scan of per-brick record counts; records (12 B) are the
+//           quadric contributions landing in a brick, bucketed by brick:
+//             event    {t, 0<<30 | w<<10 | v<<6 | u<<2 | axis, float z}
+//                      one per scanline event and brick it touches; (u,v,w) is
+//                      the event's base voxel in projection coordinates,
+//                      relative to the brick (u,v offset by one)
+//             face     {t, 1<<30 | local voxel, 0}
+//             boundary {v_min, 2<<30 | local voxel, v_max}
+//   qtab    plane quadric per triangle (10 floats)
 //
-// Order keys (64 bit, unique per voxel; ascending = reference CPU order,
-// flexible_dual_grid.cpp:173-283, :298-414, :741-757):
+// begin (ends with the one host synchronisation of a conversion):
+//   tri_events<COUNT>   one thread per (triangle, axis): scanline events (FP64,
+//                       reference arithmetic) set occupancy bits and count
+//                       event records per brick; the quadric table is written
+//   compaction          brick popcounts, scans -> N, active bricks
+//   edges               undirected edges bucketed by smaller vertex; edges
+//                       used once -> boundary list
+//   face_records<COUNT>, boundary_records<COUNT>, scan -> record offsets
+// finish (no synchronisation):
+//   *_records<FILL>     the same generators write the records
+//   brick_consume       one CTA per active brick: records -> per-voxel lists in
+//                       shared memory, ordered by the reference accumulation
+//                       order, summed sequentially in FP32 (bit-identical to
+//                       the reference CPU sums), regularised, CPQR-solved
+//   constrained_solve   box-constrained search for the few voxels whose
+//                       unconstrained solution leaves the voxel
+//
+// Contribution order keys (64 bit, unique per voxel; ascending = reference CPU
+// order, flexible_dual_grid.cpp:173-283, :298-414, :741-757):
 //   intersection  (0<<62) | ((t*3 + axis)*4 + (1-dy)*2 + (1-dx))
 //   face          (1<<62) | t
 //   boundary      (2<<62) | (v_min<<31) | v_max
@@ -48,19 +58,13 @@ using namespace ovx;
 namespace
 {
 
-enum Mode
-{
-    MARK = 0,
-    COUNT = 1,
-    FILL = 2
-};
-
-constexpr int kInlineScanWork = 256; // rows x column span of one (triangle, axis) done by the triangle's thread
-constexpr int kInlineFaceVoxels = 64; // face-box voxels done by the triangle's thread
-constexpr int kChunk = 8;            // columns per tile in the large path
-constexpr int kShortSeg = 32;        // contributions per voxel sorted inside one thread
-constexpr int kLongSmem = 2048;      // contributions per voxel sorted in shared memory by one CTA
+constexpr int kInlineScanWork = 256;  // rows x column span of one (triangle, axis) rasterised by one thread
+constexpr int kInlineFaceBricks = 64; // face boxes over more bricks go to the CTA-per-triangle path
+constexpr int kChunk = 8;             // columns per tile for large (triangle, axis) pairs
 constexpr int kThreads = 256;
+constexpr int kConsumeThreads = 128;
+constexpr int kWindow = 2048;   // per-voxel contributions held in shared memory per pass of a brick
+constexpr int kThreadSort = 48; // lists longer than this are ranked by the whole CTA
 
 // device counter words
 enum
@@ -68,8 +72,8 @@ enum
     C_SCAN_LARGE = 0,
     C_FACE_LARGE = 1,
     C_BOUNDARY = 2,
-    C_LONG = 3,
-    C_STATUS = 4,
+    C_STATUS = 3,
+    C_CONSTRAINED = 4,
     C_WORDS = 8
 };
 enum
@@ -80,31 +84,20 @@ enum
     ST_REPLAY = 8
 };
 
-constexpr unsigned long long kStageFace = 1ull << 62;
-constexpr unsigned long long kStageBoundary = 2ull << 62;
-
-struct Pass
+enum Mode
 {
-    Grid g;
-    const float *verts;
-    long long nv;
-    const void *faces;
-    long long nf;
-    float ox, oy, oz;
-    uint32_t *bits;
-    const uint32_t *word_base;
-    uint32_t *ecount;
-    const unsigned long long *eseg;
-    unsigned long long *ekey;
-    uint32_t *epay;
-    uint32_t *counters;
-    uint32_t *scan_large;
-    uint32_t scan_large_cap;
-    uint32_t *face_large;
-    uint32_t face_large_cap;
-    const uint2 *blist;
-    uint32_t blist_cap;
-    int face_on;
+    COUNT = 0,
+    FILL = 1
+};
+
+constexpr uint32_t kRecFace = 1u << 30;
+constexpr uint32_t kRecBoundary = 2u << 30;
+constexpr unsigned long long kKeyFace = 1ull << 62;
+constexpr unsigned long long kKeyBoundary = 2ull << 62;
+
+struct Rec
+{
+    uint32_t a, b, c;
 };
 
 // (u, v, w) are coordinates along (ax0, ax1, ax2) of projection axis ax2.
@@ -115,312 +108,464 @@ __device__ __forceinline__ void place(int ax2, int u, int v, int w, int &x, int 
     z = ax2 == 0 ? v : (ax2 == 1 ? u : w);
 }
 
-template <int M>
-__device__ __forceinline__ void contribute(const Pass &P, long long w, uint32_t bit, unsigned long long key, uint32_t pay)
+struct Mesh
 {
-    const uint32_t m = 1u << bit;
-    if (M == MARK)
+    Grid g;
+    const float *verts;
+    long long nv;
+    const void *faces; // NULL: triangle soup, vertex 3t+k
+    long long nf;
+    float ox, oy, oz;
+};
+
+template <typename IdxT>
+__device__ __forceinline__ bool tri_load(const Mesh &M, long long t, float v[3][3])
+{
+    long long idx[3];
+    const float o[3] = {M.ox, M.oy, M.oz};
+    return load_triangle<IdxT>(M.verts, M.nv, (const IdxT *)M.faces, t, o, v, idx);
+}
+
+__device__ __forceinline__ void vertex_load(const Mesh &M, long long i, float p[3])
+{
+    p[0] = M.verts[i * 3 + 0] - M.ox;
+    p[1] = M.verts[i * 3 + 1] - M.oy;
+    p[2] = M.verts[i * 3 + 2] - M.oz;
+}
+
+__device__ __forceinline__ void brick_origin(const Grid &g, long long b, int o[3])
+{
+    o[0] = g.gmin[0] + (int)(b % g.nb[0]) * kBrick;
+    o[1] = g.gmin[1] + (int)((b / g.nb[0]) % g.nb[1]) * kBrick;
+    o[2] = g.gmin[2] + (int)(b / ((long long)g.nb[0] * g.nb[1])) * kBrick;
+}
+
+// ===========================================================================
+// record generation
+// ===========================================================================
+struct GenArgs
+{
+    Mesh m;
+    uint32_t *bits;
+    uint32_t *rcnt;                 // records per brick (COUNT) / cursor (FILL)
+    const unsigned long long *roff; // FILL
+    Rec *rec;                       // FILL
+    float *qtab;                    // COUNT of the intersection pass
+    uint32_t *counters;
+    uint32_t *scan_large;
+    uint32_t scan_large_cap;
+    uint32_t *face_large;
+    uint32_t face_large_cap;
+    const unsigned long long *bkeys;
+    uint32_t bkeys_cap;
+};
+
+// Add n to rcnt[b] once per group of lanes of the calling warp that target the
+// same brick (neighbouring triangles mostly write the same bricks); returns the
+// value of the counter before this lane's share.
+__device__ __forceinline__ uint32_t agg_add(uint32_t *cnt, long long b, uint32_t n)
+{
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, (unsigned long long)b);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    // exclusive prefix of n over the lower lanes of the group
+    uint32_t pre = 0, tot = 0;
+    for (unsigned m = peers; m; m &= m - 1u)
     {
-        if (!(P.bits[w] & m))
-            atomicOr(&P.bits[w], m);
+        const int l = __ffs(m) - 1;
+        const uint32_t v = __shfl_sync(peers, n, l);
+        if (l < lane)
+            pre += v;
+        tot += v;
     }
+    uint32_t base = 0;
+    if (lane == leader)
+        base = atomicAdd(&cnt[b], tot);
+    base = __shfl_sync(peers, base, leader);
+    return base + pre;
+}
+
+// One record for brick b (scanline events and boundary walks; these call sites
+// sit in divergent loops, where plain atomics beat warp aggregation).
+template <int M>
+__device__ __forceinline__ void put_record(const GenArgs &A, long long b, uint32_t a0, uint32_t a1, uint32_t a2)
+{
+    if (M == COUNT)
+        atomicAdd(&A.rcnt[b], 1u);
     else
     {
-        const uint32_t row = P.word_base[w] + __popc(P.bits[w] & (m - 1u));
-        if (M == COUNT)
+        const uint32_t k = atomicAdd(&A.rcnt[b], 1u);
+        const unsigned long long base = A.roff[b];
+        if (k >= A.roff[b + 1] - base)
         {
-            atomicAdd(&P.ecount[row], 1u);
+            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
+            return;
         }
-        else
-        {
-            const uint32_t left = atomicSub(&P.ecount[row], 1u);
-            if (left == 0u)
-            {
-                // the replay produced more contributions than the count pass: never write out of the segment
-                atomicOr(&P.counters[C_STATUS], (uint32_t)ST_REPLAY);
-                return;
-            }
-            const unsigned long long pos = P.eseg[row] + (unsigned long long)(left - 1u);
-            P.ekey[pos] = key;
-            P.epay[pos] = pay;
-        }
+        Rec r;
+        r.a = a0;
+        r.b = a1;
+        r.c = a2;
+        A.rec[base + k] = r;
     }
 }
 
+// Scanline event sink: (COUNT) sets the occupancy bits of the four voxels
+// around the grid line and counts one record per distinct brick; (FILL)
+// writes those records.
 template <int M>
 struct EventSink
 {
-    const Pass &P;
-    long long t;
+    const GenArgs &A;
+    uint32_t t;
     int ax2;
     __device__ __forceinline__ void operator()(int xi, int yi, int zi, float, float, double z) const
     {
+        const Grid &g = A.m.g;
+        long long w[4];
+        uint32_t m[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+            int x, y, zz;
+            place(ax2, xi + (k >> 1), yi + (k & 1), zi, x, y, zz);
+            uint32_t bit;
+            w[k] = voxel_word(g, x, y, zz, bit);
+            m[k] = 1u << bit;
+        }
+        if (M == COUNT)
+        {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+            {
+                bool dup = false;
+#pragma unroll
+                for (int j = 0; j < k; ++j)
+                    dup |= (w[j] == w[k]);
+                if (dup)
+                    continue;
+                uint32_t mk = m[k];
+#pragma unroll
+                for (int j = k + 1; j < 4; ++j)
+                    if (w[j] == w[k])
+                        mk |= m[j];
+                atomicOr(&A.bits[w[k]], mk);
+            }
+        }
         const uint32_t zb = __float_as_uint((float)z);
 #pragma unroll
-        for (int dx = 0; dx < 2; ++dx)
+        for (int k = 0; k < 4; ++k)
+        {
+            const long long b = w[k] >> 4;
+            bool dup = false;
 #pragma unroll
-            for (int dy = 0; dy < 2; ++dy)
+            for (int j = 0; j < k; ++j)
+                dup |= ((w[j] >> 4) == b);
+            if (dup)
+                continue;
+            uint32_t code = 0;
+            if (M == FILL)
             {
-                int x, y, zz;
-                place(ax2, xi + dx, yi + dy, zi, x, y, zz);
-                uint32_t bit;
-                const long long w = voxel_word(P.g, x, y, zz, bit);
-                const unsigned long long key = (unsigned long long)((t * 3 + ax2) * 4 + (1 - dy) * 2 + (1 - dx));
-                contribute<M>(P, w, bit, key, zb);
+                int o[3];
+                brick_origin(g, b, o);
+                const int ax0 = (ax2 + 1) % 3, ax1 = (ax2 + 2) % 3;
+                const int o0 = ax0 == 0 ? o[0] : (ax0 == 1 ? o[1] : o[2]);
+                const int o1 = ax1 == 0 ? o[0] : (ax1 == 1 ? o[1] : o[2]);
+                const int o2 = ax2 == 0 ? o[0] : (ax2 == 1 ? o[1] : o[2]);
+                code = (uint32_t)ax2 | ((uint32_t)(xi - o0 + 1) << 2) | ((uint32_t)(yi - o1 + 1) << 6) |
+                       ((uint32_t)(zi - o2) << 10);
             }
+            put_record<M>(A, b, t, code, zb);
+        }
     }
 };
 
-__device__ __forceinline__ void face_box(const float v[3][3], const Grid &g, int bmin[3], int bmax[3])
-{
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-    {
-        float mn = v[0][i], mx = v[0][i];
-        mn = (v[1][i] < mn) ? v[1][i] : mn;
-        mn = (v[2][i] < mn) ? v[2][i] : mn;
-        mx = (mx < v[1][i]) ? v[1][i] : mx;
-        mx = (mx < v[2][i]) ? v[2][i] : mx;
-        const int l = trunc_f2i(mn / g.vs[i]);
-        const int h = trunc_f2i(mx / g.vs[i] + 1.0f);
-        bmin[i] = (l < g.gmin[i]) ? g.gmin[i] : l;
-        bmax[i] = (g.gmax[i] < h) ? g.gmax[i] : h;
-    }
-}
-
-template <typename IdxT>
-__device__ __forceinline__ bool tri_load(const Pass &P, long long t, float v[3][3])
-{
-    long long idx[3];
-    const float o[3] = {P.ox, P.oy, P.oz};
-    return load_triangle<IdxT>(P.verts, P.nv, (const IdxT *)P.faces, t, o, v, idx);
-}
-
-// Face test of the active voxels of one brick inside the triangle's face box.
-template <int M>
-__device__ __forceinline__ void face_brick(const Pass &P, const FaceSetup &fs, long long t, int bx, int by, int bz)
-{
-    const Grid &g = P.g;
-    const long long brick = (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
-    const int x0 = g.gmin[0] + bx * kBrick, y0 = g.gmin[1] + by * kBrick, z0 = g.gmin[2] + bz * kBrick;
-    uint32_t xmask = 0;
-#pragma unroll
-    for (int lx = 0; lx < 8; ++lx)
-        if (x0 + lx >= fs.bmin[0] && x0 + lx < fs.bmax[0])
-            xmask |= 1u << lx;
-    for (int w = 0; w < kWordsPerBrick; ++w)
-    {
-        const int z = z0 + (w >> 1);
-        if (z < fs.bmin[2] || z >= fs.bmax[2])
-            continue;
-        uint32_t mask = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-        {
-            const int y = y0 + (w & 1) * 4 + q;
-            if (y >= fs.bmin[1] && y < fs.bmax[1])
-                mask |= xmask << (q * 8);
-        }
-        uint32_t word = P.bits[brick * kWordsPerBrick + w] & mask;
-        while (word)
-        {
-            const int b = __ffs(word) - 1;
-            word &= word - 1u;
-            const int x = x0 + (b & 7), y = y0 + (w & 1) * 4 + (b >> 3);
-            if (face_test(fs, g, x, y, z))
-                contribute<M>(P, brick * kWordsPerBrick + w, (uint32_t)b, kStageFace | (unsigned long long)t, 0u);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// per-triangle pass
-// ---------------------------------------------------------------------------
 template <int M, typename IdxT>
-__global__ void __launch_bounds__(kThreads) tri_pass(Pass P)
+__global__ void __launch_bounds__(kThreads) tri_events(GenArgs A)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.nf)
+    // one thread per (triangle, projection axis)
+    const long long ta = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ta >= 3 * A.m.nf)
         return;
+    const long long t = ta / 3;
+    const int ax2 = (int)(ta - 3 * t);
     float v[3][3];
-    if (!tri_load<IdxT>(P, t, v))
+    if (!tri_load<IdxT>(A.m, t, v))
     {
-        if (M == MARK)
-            atomicOr(&P.counters[C_STATUS], (uint32_t)ST_BAD_INDEX);
+        if (M == COUNT)
+            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_BAD_INDEX);
         return;
     }
-#pragma unroll 1
-    for (int ax2 = 0; ax2 < 3; ++ax2)
+    if (M == COUNT && ax2 == 0 && A.qtab)
     {
-        AxisScan s;
-        axis_setup(v, ax2, P.g, s);
-        const int rows = s.end - s.start;
-        if (rows <= 0)
-            continue;
-        int clo, chi;
-        axis_col_bounds(s, P.g, clo, chi);
-        const long long work = (long long)rows * (long long)(chi - clo + 1);
-        if (work > kInlineScanWork)
-        {
-            if (M == MARK)
-            {
-                const uint32_t slot = atomicAdd(&P.counters[C_SCAN_LARGE], 1u);
-                if (slot < P.scan_large_cap)
-                    P.scan_large[slot] = (uint32_t)(t * 3 + ax2);
-                else
-                    atomicOr(&P.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
-            }
-            continue;
-        }
-        EventSink<M> sink{P, t, ax2};
-#pragma unroll 1
-        for (int yi = s.start; yi < s.end; ++yi)
-            scan_row(s, yi, INT_MIN, INT_MAX, P.g, sink);
+        float q[10];
+        tri_quadric(v, q);
+#pragma unroll
+        for (int i = 0; i < 10; ++i)
+            A.qtab[t * 10 + i] = q[i];
     }
-    if (!P.face_on)
+    AxisScan s;
+    axis_setup(v, ax2, A.m.g, s);
+    const int rows = s.end - s.start;
+    if (rows <= 0)
         return;
-    int bmin[3], bmax[3];
-    face_box(v, P.g, bmin, bmax);
-    const long long ex = bmax[0] - bmin[0], ey = bmax[1] - bmin[1], ez = bmax[2] - bmin[2];
-    if (ex <= 0 || ey <= 0 || ez <= 0)
-        return;
-    if (ex * ey * ez > kInlineFaceVoxels)
+    int clo, chi;
+    axis_col_bounds(s, A.m.g, clo, chi);
+    if ((long long)rows * (long long)(chi - clo + 1) > kInlineScanWork)
     {
-        if (M == MARK)
+        if (M == COUNT)
         {
-            const uint32_t slot = atomicAdd(&P.counters[C_FACE_LARGE], 1u);
-            if (slot < P.face_large_cap)
-                P.face_large[slot] = (uint32_t)t;
+            const uint32_t slot = atomicAdd(&A.counters[C_SCAN_LARGE], 1u);
+            if (slot < A.scan_large_cap)
+                A.scan_large[slot] = (uint32_t)ta;
             else
-                atomicOr(&P.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+                atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
         }
         return;
     }
-    if (M == MARK)
-        return;
-    FaceSetup fs;
-    face_setup(v, P.g, fs);
+    EventSink<M> sink{A, (uint32_t)t, ax2};
 #pragma unroll 1
-    for (int z = bmin[2]; z < bmax[2]; ++z)
-#pragma unroll 1
-        for (int y = bmin[1]; y < bmax[1]; ++y)
-#pragma unroll 1
-            for (int x = bmin[0]; x < bmax[0]; ++x)
-            {
-                uint32_t bit;
-                const long long w = voxel_word(P.g, x, y, z, bit);
-                if (!(P.bits[w] & (1u << bit)))
-                    continue;
-                if (face_test(fs, P.g, x, y, z))
-                    contribute<M>(P, w, bit, kStageFace | (unsigned long long)t, 0u);
-            }
+    for (int yi = s.start; yi < s.end; ++yi)
+        scan_row(s, yi, INT_MIN, INT_MAX, A.m.g, sink);
 }
 
 // One CTA per listed (triangle, axis); threads over (row, column chunk) tiles.
 template <int M, typename IdxT>
-__global__ void __launch_bounds__(128) large_scan(Pass P)
+__global__ void __launch_bounds__(128) large_events(GenArgs A)
 {
-    const uint32_t n = min(P.counters[C_SCAN_LARGE], P.scan_large_cap);
+    const uint32_t n = min(A.counters[C_SCAN_LARGE], A.scan_large_cap);
     for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
     {
-        const uint32_t e = P.scan_large[i];
+        const uint32_t e = A.scan_large[i];
         const long long t = e / 3;
         const int ax2 = (int)(e % 3);
         float v[3][3];
-        if (!tri_load<IdxT>(P, t, v))
+        if (!tri_load<IdxT>(A.m, t, v))
             continue;
         AxisScan s;
-        axis_setup(v, ax2, P.g, s);
+        axis_setup(v, ax2, A.m.g, s);
         const int rows = s.end - s.start;
         int clo, chi;
-        axis_col_bounds(s, P.g, clo, chi);
+        axis_col_bounds(s, A.m.g, clo, chi);
         const int nch = (chi - clo + 1 + kChunk - 1) / kChunk;
         const long long tiles = (long long)rows * nch;
-        EventSink<M> sink{P, t, ax2};
+        EventSink<M> sink{A, (uint32_t)t, ax2};
         for (long long k = threadIdx.x; k < tiles; k += blockDim.x)
         {
             const int yi = s.start + (int)(k / nch);
             const int ch = (int)(k % nch);
             const int lo = ch == 0 ? INT_MIN : clo + ch * kChunk;
             const int hi = ch == nch - 1 ? INT_MAX : clo + (ch + 1) * kChunk;
-            scan_row(s, yi, lo, hi, P.g, sink);
+            scan_row(s, yi, lo, hi, A.m.g, sink);
         }
     }
+}
+
+// Face tests of the active voxels of one brick inside a triangle's face box,
+// evaluated once into a 512-bit pass mask: COUNT adds the number of passing
+// voxels to the brick's record count, FILL reserves that many slots at once and
+// writes the records.
+template <int M>
+__device__ __forceinline__ void face_brick(const GenArgs &A, const FaceSetup &fs, uint32_t t, int bx, int by, int bz)
+{
+    const Grid &g = A.m.g;
+    const long long b = (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
+    const int o[3] = {g.gmin[0] + bx * kBrick, g.gmin[1] + by * kBrick, g.gmin[2] + bz * kBrick};
+    int lo[3], hi[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        lo[a] = (fs.bmin[a] > o[a] ? fs.bmin[a] : o[a]) - o[a];
+        hi[a] = (fs.bmax[a] < o[a] + 8 ? fs.bmax[a] : o[a] + 8) - o[a];
+        if (hi[a] <= lo[a])
+            return;
+    }
+    const uint32_t xmask = ((1u << hi[0]) - 1u) & ~((1u << lo[0]) - 1u);
+    const uint4 *bw4 = reinterpret_cast<const uint4 *>(A.bits + b * kWordsPerBrick);
+    uint32_t pm[kWordsPerBrick];
+    uint32_t count = 0;
+#pragma unroll
+    for (int q4 = 0; q4 < 4; ++q4)
+    {
+        const uint4 wv = bw4[q4];
+        const uint32_t words[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+            const int w = q4 * 4 + k;
+            pm[w] = 0u;
+            if ((w >> 1) < lo[2] || (w >> 1) >= hi[2])
+                continue;
+            uint32_t mask = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const int ly = (w & 1) * 4 + q;
+                if (ly >= lo[1] && ly < hi[1])
+                    mask |= xmask << (q * 8);
+            }
+            uint32_t word = words[k] & mask;
+            uint32_t pass = 0u;
+            while (word)
+            {
+                const int bt = __ffs(word) - 1;
+                word &= word - 1u;
+                if (face_test(fs, g, o[0] + (bt & 7), o[1] + (w & 1) * 4 + (bt >> 3), o[2] + (w >> 1)))
+                    pass |= 1u << bt;
+            }
+            pm[w] = pass;
+            count += __popc(pass);
+        }
+    }
+    if (count == 0)
+        return;
+    if (M == COUNT)
+    {
+        agg_add(A.rcnt, b, count);
+        return;
+    }
+    const uint32_t k0 = agg_add(A.rcnt, b, count);
+    if ((unsigned long long)k0 + count > A.roff[b + 1] - A.roff[b])
+    {
+        atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
+        return;
+    }
+    unsigned long long pos = A.roff[b] + k0;
+#pragma unroll
+    for (int w = 0; w < kWordsPerBrick; ++w)
+    {
+        uint32_t pass = pm[w];
+        while (pass)
+        {
+            const int bt = __ffs(pass) - 1;
+            pass &= pass - 1u;
+            Rec r;
+            r.a = t;
+            r.b = kRecFace | (uint32_t)(w * 32 + bt);
+            r.c = 0u;
+            A.rec[pos++] = r;
+        }
+    }
+}
+
+__device__ __forceinline__ void face_bricks(const FaceSetup &fs, const Grid &g, int b0[3], int b1[3])
+{
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        b0[a] = (fs.bmin[a] - g.gmin[a]) >> 3;
+        b1[a] = (fs.bmax[a] - 1 - g.gmin[a]) >> 3;
+    }
+}
+
+constexpr int kFaceSlots = 4; // threads per triangle in the face pass
+
+// kFaceSlots threads per triangle: thread j tests bricks j, j+kFaceSlots, ... of the face box.
+template <int M, typename IdxT>
+__global__ void __launch_bounds__(kThreads) face_records(GenArgs A)
+{
+    const long long tj = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tj >= (long long)kFaceSlots * A.m.nf)
+        return;
+    const long long t = tj / kFaceSlots;
+    const int j = (int)(tj - t * kFaceSlots);
+    float v[3][3];
+    if (!tri_load<IdxT>(A.m, t, v))
+        return;
+    const Grid &g = A.m.g;
+    int bmin[3], bmax[3];
+    face_box(v, g, bmin, bmax);
+    if (bmax[0] <= bmin[0] || bmax[1] <= bmin[1] || bmax[2] <= bmin[2])
+        return;
+    int b0[3], b1[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        b0[a] = (bmin[a] - g.gmin[a]) >> 3;
+        b1[a] = (bmax[a] - 1 - g.gmin[a]) >> 3;
+    }
+    const long long nx = b1[0] - b0[0] + 1, ny = b1[1] - b0[1] + 1, nz = b1[2] - b0[2] + 1;
+    const long long nbk = nx * ny * nz;
+    if (nbk > kInlineFaceBricks)
+    {
+        if (M == COUNT && j == 0)
+        {
+            const uint32_t slot = atomicAdd(&A.counters[C_FACE_LARGE], 1u);
+            if (slot < A.face_large_cap)
+                A.face_large[slot] = (uint32_t)t;
+            else
+                atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+        }
+        return;
+    }
+    if (j >= nbk)
+        return;
+    FaceSetup fs;
+    face_setup(v, g, fs);
+#pragma unroll 1
+    for (long long k = j; k < nbk; k += kFaceSlots)
+        face_brick<M>(A, fs, (uint32_t)t, b0[0] + (int)(k % nx), b0[1] + (int)((k / nx) % ny), b0[2] + (int)(k / (nx * ny)));
 }
 
 // One CTA per listed triangle; threads over the bricks of its face box.
 template <int M, typename IdxT>
-__global__ void __launch_bounds__(128) large_face(Pass P)
+__global__ void __launch_bounds__(128) large_face_records(GenArgs A)
 {
-    const uint32_t n = min(P.counters[C_FACE_LARGE], P.face_large_cap);
+    const uint32_t n = min(A.counters[C_FACE_LARGE], A.face_large_cap);
     for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
     {
-        const long long t = P.face_large[i];
+        const long long t = A.face_large[i];
         float v[3][3];
-        if (!tri_load<IdxT>(P, t, v))
+        if (!tri_load<IdxT>(A.m, t, v))
             continue;
         FaceSetup fs;
-        face_setup(v, P.g, fs);
-        const Grid &g = P.g;
+        face_setup(v, A.m.g, fs);
         int b0[3], b1[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-        {
-            b0[a] = (fs.bmin[a] - g.gmin[a]) >> 3;
-            b1[a] = (fs.bmax[a] - 1 - g.gmin[a]) >> 3;
-        }
+        face_bricks(fs, A.m.g, b0, b1);
         const long long nx = b1[0] - b0[0] + 1, ny = b1[1] - b0[1] + 1, nz = b1[2] - b0[2] + 1;
-        const long long total = nx * ny * nz;
-        for (long long k = threadIdx.x; k < total; k += blockDim.x)
-        {
-            const int bx = b0[0] + (int)(k % nx);
-            const int by = b0[1] + (int)((k / nx) % ny);
-            const int bz = b0[2] + (int)(k / (nx * ny));
-            face_brick<M>(P, fs, t, bx, by, bz);
-        }
+        for (long long k = threadIdx.x; k < nx * ny * nz; k += blockDim.x)
+            face_brick<M>(A, fs, (uint32_t)t, b0[0] + (int)(k % nx), b0[1] + (int)((k / nx) % ny), b0[2] + (int)(k / (nx * ny)));
     }
 }
 
-// Boundary walks, one thread per boundary edge.
+// One thread per boundary edge: the reference DDA walk; one record per active voxel visited.
 template <int M>
-__global__ void __launch_bounds__(kThreads) boundary_pass(Pass P)
+__global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
 {
-    const uint32_t n = min(P.counters[C_BOUNDARY], P.blist_cap);
+    const uint32_t n = min(A.counters[C_BOUNDARY], A.bkeys_cap);
+    const Grid &g = A.m.g;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
-        const uint2 e = P.blist[i];
+        const unsigned long long e = A.bkeys[i];
+        const uint32_t ia = (uint32_t)(e >> 32), ib = (uint32_t)(e & 0xffffffffull);
         float v0[3], v1[3];
-        v0[0] = P.verts[(long long)e.x * 3 + 0] - P.ox;
-        v0[1] = P.verts[(long long)e.x * 3 + 1] - P.oy;
-        v0[2] = P.verts[(long long)e.x * 3 + 2] - P.oz;
-        v1[0] = P.verts[(long long)e.y * 3 + 0] - P.ox;
-        v1[1] = P.verts[(long long)e.y * 3 + 1] - P.oy;
-        v1[2] = P.verts[(long long)e.y * 3 + 2] - P.oz;
+        vertex_load(A.m, ia, v0);
+        vertex_load(A.m, ib, v1);
         Dda d;
-        if (!boundary_setup(v0, v1, P.g, d, nullptr))
+        if (!boundary_setup(v0, v1, g, d, nullptr))
             continue;
-        const unsigned long long key = kStageBoundary | ((unsigned long long)e.x << 31) | (unsigned long long)e.y;
         for (;;)
         {
-            if (in_grid(P.g, d.cur[0], d.cur[1], d.cur[2]))
+            if (in_grid(g, d.cur[0], d.cur[1], d.cur[2]))
             {
                 uint32_t bit;
-                const long long w = voxel_word(P.g, d.cur[0], d.cur[1], d.cur[2], bit);
-                if (P.bits[w] & (1u << bit))
-                    contribute<M>(P, w, bit, key, 0u);
+                const long long w = voxel_word(g, d.cur[0], d.cur[1], d.cur[2], bit);
+                if (A.bits[w] & (1u << bit))
+                    put_record<M>(A, w >> 4, ia, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), ib);
             }
             if (!dda_step(d))
                 break;
         }
         if (d.guard < 0)
-            atomicOr(&P.counters[C_STATUS], (uint32_t)ST_WALK_GUARD);
+            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_WALK_GUARD);
     }
 }
 
-// ---------------------------------------------------------------------------
-// occupancy compaction
-// ---------------------------------------------------------------------------
-__global__ void brick_count(const uint32_t *__restrict__ bits, long long nbricks, uint32_t *__restrict__ bcount)
+// ===========================================================================
+// compaction and active-brick map
+// ===========================================================================
+__global__ void brick_count(const uint32_t *__restrict__ bits, long long nbricks, uint32_t *__restrict__ bcount,
+                            uint32_t *__restrict__ aflag)
 {
     const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nbricks)
@@ -434,45 +579,22 @@ __global__ void brick_count(const uint32_t *__restrict__ bits, long long nbricks
         c += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
     }
     bcount[b] = c;
+    aflag[b] = c ? 1u : 0u;
 }
 
-// Row bases per occupancy word and voxel coordinates in brick order.
-__global__ void brick_emit(const uint32_t *__restrict__ bits, const unsigned long long *__restrict__ bbase, Grid g,
-                           uint32_t *__restrict__ word_base, int32_t *__restrict__ vox)
+__global__ void brick_slots(const uint32_t *__restrict__ aflag, const unsigned long long *__restrict__ aslot, long long nbricks,
+                            uint32_t *__restrict__ active)
 {
     const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= g.nbricks)
+    if (b >= nbricks)
         return;
-    unsigned long long base = bbase[b];
-    if (bbase[b + 1] == base)
-        return;
-    const int bx = (int)(b % g.nb[0]);
-    const int by = (int)((b / g.nb[0]) % g.nb[1]);
-    const int bz = (int)(b / ((long long)g.nb[0] * g.nb[1]));
-    for (int w = 0; w < kWordsPerBrick; ++w)
-    {
-        uint32_t word = bits[b * kWordsPerBrick + w];
-        if (word_base)
-            word_base[b * kWordsPerBrick + w] = (uint32_t)base;
-        while (word)
-        {
-            const int bit = __ffs(word) - 1;
-            word &= word - 1u;
-            const int li = w * 32 + bit;
-            if (vox)
-            {
-                vox[base * 3 + 0] = g.gmin[0] + bx * kBrick + (li & 7);
-                vox[base * 3 + 1] = g.gmin[1] + by * kBrick + ((li >> 3) & 7);
-                vox[base * 3 + 2] = g.gmin[2] + bz * kBrick + (li >> 6);
-            }
-            ++base;
-        }
-    }
+    if (aflag[b])
+        active[aslot[b]] = (uint32_t)b;
 }
 
-// ---------------------------------------------------------------------------
-// boundary edge extraction: edges bucketed by their smaller vertex
-// ---------------------------------------------------------------------------
+// ===========================================================================
+// boundary edges (edges used by exactly one face)
+// ===========================================================================
 template <typename IdxT>
 __device__ __forceinline__ bool face_edge(const IdxT *faces, long long nv, long long f, int k, uint32_t &a, uint32_t &b)
 {
@@ -513,8 +635,10 @@ __global__ void edge_fill(const IdxT *__restrict__ faces, long long nf, long lon
         uint32_t a, b;
         if (face_edge(faces, nv, f, k, a, b))
         {
-            const unsigned long long pos = voff[a] + (unsigned long long)(atomicSub(&vcnt[a], 1u) - 1u);
-            emax[pos] = b;
+            const uint32_t left = atomicSub(&vcnt[a], 1u);
+            if (left == 0u)
+                continue; // cannot happen: same faces as edge_count
+            emax[voff[a] + (unsigned long long)(left - 1u)] = b;
         }
     }
 }
@@ -539,9 +663,19 @@ __device__ void heap_sift(uint32_t *a, long long start, long long end)
     }
 }
 
-// Per vertex: the other endpoints of its edges; keep those that occur once.
-__global__ void edge_find(const unsigned long long *__restrict__ voff, uint32_t *__restrict__ emax, long long nv, uint2 *__restrict__ blist,
-                          uint32_t cap, uint32_t *__restrict__ counters)
+__device__ __forceinline__ void push_boundary(unsigned long long *bkeys, uint32_t cap, uint32_t *counters, uint32_t a, uint32_t b)
+{
+    const uint32_t slot = atomicAdd(&counters[C_BOUNDARY], 1u);
+    if (slot < cap)
+        bkeys[slot] = ((unsigned long long)a << 32) | b;
+    else
+        atomicOr(&counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+}
+
+// Per vertex a: the larger endpoints of edges whose smaller endpoint is a;
+// those occurring once are boundary edges (reference: std::map count == 1).
+__global__ void edge_find(const unsigned long long *__restrict__ voff, uint32_t *__restrict__ emax, long long nv,
+                          unsigned long long *__restrict__ bkeys, uint32_t cap, uint32_t *__restrict__ counters)
 {
     const long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= nv)
@@ -559,17 +693,10 @@ __global__ void edge_find(const unsigned long long *__restrict__ voff, uint32_t 
             for (long long j = 0; j < n; ++j)
                 c += (l[j] == l[i]);
             if (c == 1)
-            {
-                const uint32_t slot = atomicAdd(&counters[C_BOUNDARY], 1u);
-                if (slot < cap)
-                    blist[slot] = make_uint2((uint32_t)a, l[i]);
-                else
-                    atomicOr(&counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
-            }
+                push_boundary(bkeys, cap, counters, (uint32_t)a, l[i]);
         }
         return;
     }
-    // heap sort in place, then runs of length one
     for (long long i = n / 2 - 1; i >= 0; --i)
         heap_sift(l, i, n);
     for (long long end = n - 1; end > 0; --end)
@@ -585,38 +712,109 @@ __global__ void edge_find(const unsigned long long *__restrict__ voff, uint32_t 
         while (j < n && l[j] == l[i])
             ++j;
         if (j - i == 1)
-        {
-            const uint32_t slot = atomicAdd(&counters[C_BOUNDARY], 1u);
-            if (slot < cap)
-                blist[slot] = make_uint2((uint32_t)a, l[i]);
-            else
-                atomicOr(&counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
-        }
+            push_boundary(bkeys, cap, counters, (uint32_t)a, l[i]);
         i = j;
     }
 }
 
-// ---------------------------------------------------------------------------
-// per-voxel reduction in reference order + solve
-// ---------------------------------------------------------------------------
-struct Final
+// ===========================================================================
+// per-brick accumulation in reference order + solve
+// ===========================================================================
+struct SolveArgs
 {
-    Grid g;
-    const float *verts;
-    long long nv;
-    const void *faces;
-    int fbytes;
-    float ox, oy, oz;
+    Mesh m;
     float bw, rw;
-    const unsigned long long *eseg;
-    const unsigned long long *ekey;
-    const uint32_t *epay;
-    const int32_t *vox;
+    const uint32_t *bits;
+    const unsigned long long *bbase;
+    const uint32_t *active;
+    const unsigned long long *roff;
+    const Rec *rec;
+    const float *qtab;
+    int32_t *vox;
     float *dual;
     uint8_t *flags;
     uint32_t *counters;
-    uint32_t *long_list;
-    long long n;
+    float *clist; // deferred constrained searches, 16 words each
+    uint32_t clist_cap;
+};
+
+struct BrickShared
+{
+    uint32_t bits[kWordsPerBrick];
+    uint32_t wpre[kWordsPerBrick];
+    uint16_t vl[512]; // brick-local index of the i-th active voxel (i = output row - brick base)
+    uint32_t cnt[512];
+    uint32_t off[512];
+    uint32_t fill[512];
+    unsigned long long key[kWindow];
+    uint32_t pay[kWindow];
+    uint16_t perm[kWindow];
+    uint32_t scan_tmp[kConsumeThreads / 32 + 1];
+    int nvox, win_lo, win_hi, big_n, long_n;
+    uint32_t win_base, total, status;
+    uint16_t big[512];
+    uint16_t longl[512];
+};
+
+__device__ __forceinline__ int dense_index(const BrickShared &S, int lv)
+{
+    const int w = lv >> 5, b = lv & 31;
+    return (int)(S.wpre[w] + __popc(S.bits[w] & ((1u << b) - 1u)));
+}
+
+// Expand one record of the brick into (dense voxel index, order key, payload) contributions.
+template <typename Sink>
+__device__ __forceinline__ void expand(const BrickShared &S, const Rec &r, Sink &sink)
+{
+    const uint32_t kind = r.b >> 30;
+    if (kind == 0)
+    {
+        const int ax2 = (int)(r.b & 3u);
+        const int u = (int)((r.b >> 2) & 15u) - 1, v = (int)((r.b >> 6) & 15u) - 1, w = (int)((r.b >> 10) & 15u);
+        const unsigned long long kb = ((unsigned long long)r.a * 3ull + (unsigned long long)ax2) * 4ull;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+            const int dx = k >> 1, dy = k & 1;
+            const int lu = u + dx, lv = v + dy;
+            if (lu < 0 || lu >= 8 || lv < 0 || lv >= 8)
+                continue;
+            int lx, ly, lz;
+            place(ax2, lu, lv, w, lx, ly, lz);
+            sink(dense_index(S, lx + 8 * ly + 64 * lz), kb + (unsigned long long)((1 - dy) * 2 + (1 - dx)), r.c);
+        }
+    }
+    else if (kind == 1)
+        sink(dense_index(S, (int)(r.b & 511u)), kKeyFace | (unsigned long long)r.a, 0u);
+    else
+        sink(dense_index(S, (int)(r.b & 511u)), kKeyBoundary | ((unsigned long long)r.a << 31) | (unsigned long long)r.c, 0u);
+}
+
+struct CountSink
+{
+    BrickShared &S;
+    __device__ __forceinline__ void operator()(int i, unsigned long long, uint32_t) const
+    {
+        atomicAdd(&S.cnt[i], 1u);
+    }
+};
+
+struct FillSink
+{
+    BrickShared &S;
+    int lo, hi;
+    uint32_t base;
+    __device__ __forceinline__ void operator()(int i, unsigned long long key, uint32_t pay) const
+    {
+        if (i < lo || i >= hi || S.cnt[i] > (uint32_t)kWindow)
+            return;
+        const uint32_t k = atomicAdd(&S.fill[i], 1u);
+        if (k >= S.cnt[i])
+            return; // cannot happen: the count pass read the same records
+        const uint32_t pos = S.off[i] - base + k;
+        S.key[pos] = key;
+        S.pay[pos] = pay;
+    }
 };
 
 struct Acc
@@ -626,8 +824,6 @@ struct Acc
     float cnt;
     uint32_t flags;
     bool first;
-    long long qt_tri;
-    float qt[10];
 };
 
 __device__ __forceinline__ void acc_init(Acc &a)
@@ -639,39 +835,25 @@ __device__ __forceinline__ void acc_init(Acc &a)
     a.cnt = 0.0f;
     a.flags = 0;
     a.first = true;
-    a.qt_tri = -1;
 }
 
-__device__ __forceinline__ void tri_q_cached(const Final &F, long long t, Acc &a)
-{
-    if (a.qt_tri == t)
-        return;
-    float v[3][3];
-    long long idx[3];
-    const float o[3] = {F.ox, F.oy, F.oz};
-    if (F.fbytes == 8)
-        load_triangle<long long>(F.verts, F.nv, (const long long *)F.faces, t, o, v, idx);
-    else
-        load_triangle<int>(F.verts, F.nv, (const int *)F.faces, t, o, v, idx);
-    tri_quadric(v, a.qt);
-    a.qt_tri = t;
-}
-
-__device__ __forceinline__ void acc_entry(const Final &F, const int vc[3], unsigned long long key, uint32_t pay, Acc &a)
+// Add one contribution in reference order (flexible_dual_grid.cpp:251-271, :409, :521).
+__device__ __forceinline__ void acc_entry(const SolveArgs &A, const int vc[3], unsigned long long key, uint32_t pay, Acc &a)
 {
     const unsigned stage = (unsigned)(key >> 62);
+    float qt[10];
     if (stage == 0)
     {
-        const unsigned sub = (unsigned)(key & 3ull);
         const unsigned long long ta = key >> 2;
         const long long t = (long long)(ta / 3ull);
-        const int ax2 = (int)(ta % 3ull);
-        const int dx = 1 - (int)(sub & 1u), dy = 1 - (int)(sub >> 1);
+        const int ax2 = (int)(ta - (unsigned long long)t * 3ull);
+        const int dx = 1 - (int)(key & 1ull), dy = 1 - (int)((key >> 1) & 1ull);
         const int ax0 = (ax2 + 1) % 3, ax1 = (ax2 + 2) % 3;
         const int c0 = ax0 == 0 ? vc[0] : (ax0 == 1 ? vc[1] : vc[2]);
         const int c1 = ax1 == 0 ? vc[0] : (ax1 == 1 ? vc[1] : vc[2]);
-        const float vs0 = ax0 == 0 ? F.g.vs[0] : (ax0 == 1 ? F.g.vs[1] : F.g.vs[2]);
-        const float vs1 = ax1 == 0 ? F.g.vs[0] : (ax1 == 1 ? F.g.vs[1] : F.g.vs[2]);
+        const Grid &g = A.m.g;
+        const float vs0 = ax0 == 0 ? g.vs[0] : (ax0 == 1 ? g.vs[1] : g.vs[2]);
+        const float vs1 = ax1 == 0 ? g.vs[0] : (ax1 == 1 ? g.vs[1] : g.vs[2]);
         const float pu = (float)(c0 - dx + 1) * vs0;
         const float pv = (float)(c1 - dy + 1) * vs1;
         const float pw = __uint_as_float(pay);
@@ -679,7 +861,9 @@ __device__ __forceinline__ void acc_entry(const Final &F, const int vc[3], unsig
         p[0] = ax2 == 0 ? pw : (ax2 == 1 ? pv : pu);
         p[1] = ax2 == 0 ? pu : (ax2 == 1 ? pw : pv);
         p[2] = ax2 == 0 ? pv : (ax2 == 1 ? pu : pw);
-        tri_q_cached(F, t, a);
+#pragma unroll
+        for (int i = 0; i < 10; ++i)
+            qt[i] = A.qtab[t * 10 + i];
         if (a.first)
         {
             a.mean[0] = p[0];
@@ -688,7 +872,7 @@ __device__ __forceinline__ void acc_entry(const Final &F, const int vc[3], unsig
             a.cnt = 1.0f;
 #pragma unroll
             for (int i = 0; i < 10; ++i)
-                a.q[i] = a.qt[i];
+                a.q[i] = qt[i];
             a.first = false;
         }
         else
@@ -699,7 +883,7 @@ __device__ __forceinline__ void acc_entry(const Final &F, const int vc[3], unsig
             a.cnt = a.cnt + 1.0f;
 #pragma unroll
             for (int i = 0; i < 10; ++i)
-                a.q[i] = a.q[i] + a.qt[i];
+                a.q[i] = a.q[i] + qt[i];
         }
         if (dx == 0 && dy == 0)
             a.flags |= 1u << ax2;
@@ -707,145 +891,384 @@ __device__ __forceinline__ void acc_entry(const Final &F, const int vc[3], unsig
     else if (stage == 1)
     {
         const long long t = (long long)(key & ((1ull << 62) - 1ull));
-        tri_q_cached(F, t, a);
 #pragma unroll
         for (int i = 0; i < 10; ++i)
-            a.q[i] = a.q[i] + a.qt[i];
+            a.q[i] = a.q[i] + A.qtab[t * 10 + i];
     }
     else
     {
-        const long long ia = (long long)((key >> 31) & 0x7fffffffull);
-        const long long ib = (long long)(key & 0x7fffffffull);
-        float v0[3], v1[3], bq[10];
-        v0[0] = F.verts[ia * 3 + 0] - F.ox;
-        v0[1] = F.verts[ia * 3 + 1] - F.oy;
-        v0[2] = F.verts[ia * 3 + 2] - F.oz;
-        v1[0] = F.verts[ib * 3 + 0] - F.ox;
-        v1[1] = F.verts[ib * 3 + 1] - F.oy;
-        v1[2] = F.verts[ib * 3 + 2] - F.oz;
+        float v0[3], v1[3];
+        vertex_load(A.m, (long long)((key >> 31) & 0x7fffffffull), v0);
+        vertex_load(A.m, (long long)(key & 0x7fffffffull), v1);
         Dda d;
-        if (boundary_setup(v0, v1, F.g, d, bq))
+        if (boundary_setup(v0, v1, A.m.g, d, qt))
         {
 #pragma unroll
             for (int i = 0; i < 10; ++i)
-                a.q[i] = a.q[i] + F.bw * bq[i];
+                a.q[i] = a.q[i] + A.bw * qt[i];
         }
     }
 }
 
-__device__ __forceinline__ void finish_voxel(const Final &F, long long r, const int vc[3], const Acc &a)
+// Regularise and solve; voxels whose unconstrained solution leaves the box go to the constrained-search list.
+__device__ __forceinline__ void finish_voxel(const SolveArgs &A, long long row, const int vc[3], const Acc &a)
 {
-    float out[3];
-    solve_voxel(vc, F.g, a.q, a.mean, a.cnt, F.rw, out);
-    F.dual[r * 3 + 0] = out[0];
-    F.dual[r * 3 + 1] = out[1];
-    F.dual[r * 3 + 2] = out[2];
-    F.flags[r * 3 + 0] = (uint8_t)(a.flags & 1u);
-    F.flags[r * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
-    F.flags[r * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
-}
-
-__global__ void __launch_bounds__(128) final_short(Final F)
-{
-    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= F.n)
-        return;
-    const unsigned long long s = F.eseg[r];
-    const int n = (int)(F.eseg[r + 1] - s);
-    if (n > kShortSeg)
+    float q[10];
+    regularize(a.q, a.mean, a.cnt, A.rw, q);
+    float v[3];
+    const bool inside = solve_unconstrained(vc, A.m.g, q, v);
+    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
+    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
+    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
+    if (inside)
     {
-        const uint32_t slot = atomicAdd(&F.counters[C_LONG], 1u);
-        F.long_list[slot] = (uint32_t)r;
+        A.dual[row * 3 + 0] = v[0];
+        A.dual[row * 3 + 1] = v[1];
+        A.dual[row * 3 + 2] = v[2];
         return;
     }
-    unsigned long long k[kShortSeg];
-    uint32_t p[kShortSeg];
-    for (int i = 0; i < n; ++i)
+    const uint32_t slot = atomicAdd(&A.counters[C_CONSTRAINED], 1u);
+    if (slot >= A.clist_cap)
     {
-        const unsigned long long key = F.ekey[s + i];
-        const uint32_t pay = F.epay[s + i];
-        int j = i;
-        while (j > 0 && k[j - 1] > key)
+        atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+        return;
+    }
+    float *c = A.clist + (size_t)slot * 16;
+    c[0] = __int_as_float((int)row);
+    c[1] = __int_as_float(vc[0]);
+    c[2] = __int_as_float(vc[1]);
+    c[3] = __int_as_float(vc[2]);
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        c[4 + i] = q[i];
+}
+
+// block-wide exclusive scan of S.cnt[0..nvox) (lists longer than the window count 0) into S.off
+__device__ __forceinline__ void scan_counts(BrickShared &S, int nvox)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int per = 512 / kConsumeThreads;
+    uint32_t v[per], sum = 0;
+#pragma unroll
+    for (int i = 0; i < per; ++i)
+    {
+        const int j = tid * per + i;
+        const uint32_t c = j < nvox ? S.cnt[j] : 0u;
+        v[i] = c > (uint32_t)kWindow ? 0u : c;
+        sum += v[i];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d)
+            incl += y;
+    }
+    if (lane == 31)
+        S.scan_tmp[warp] = incl;
+    __syncthreads();
+    if (tid == 0)
+    {
+        uint32_t r = 0;
+        for (int i = 0; i < kConsumeThreads / 32; ++i)
         {
-            k[j] = k[j - 1];
-            p[j] = p[j - 1];
-            --j;
+            const uint32_t x = S.scan_tmp[i];
+            S.scan_tmp[i] = r;
+            r += x;
         }
-        k[j] = key;
-        p[j] = pay;
+        S.total = r;
     }
-    const int vc[3] = {F.vox[r * 3 + 0], F.vox[r * 3 + 1], F.vox[r * 3 + 2]};
+    __syncthreads();
+    uint32_t run = S.scan_tmp[warp] + incl - sum;
+#pragma unroll
+    for (int i = 0; i < per; ++i)
+    {
+        S.off[tid * per + i] = run;
+        run += v[i];
+    }
+}
+
+struct SelectSink
+{
+    int target;
+    unsigned long long last;
+    bool any;
+    unsigned long long best;
+    uint32_t pay;
+    __device__ __forceinline__ void operator()(int j, unsigned long long key, uint32_t p)
+    {
+        if (j != target || (any && key <= last))
+            return;
+        if (key < best)
+        {
+            best = key;
+            pay = p;
+        }
+    }
+};
+
+// A voxel whose list exceeds the window: its contributions in key order by
+// repeated selection over the brick's records (one thread; rare).
+__device__ __noinline__ void select_voxel(const SolveArgs &A, const BrickShared &S, int i, const Rec *rec, unsigned long long nrec,
+                                          long long row, const int vc[3])
+{
     Acc a;
     acc_init(a);
-    for (int i = 0; i < n; ++i)
-        acc_entry(F, vc, k[i], p[i], a);
-    finish_voxel(F, r, vc, a);
+    const uint32_t n = S.cnt[i];
+    unsigned long long last = 0;
+    for (uint32_t step = 0; step < n; ++step)
+    {
+        SelectSink sel{i, last, step > 0, ~0ull, 0u};
+        for (unsigned long long r = 0; r < nrec; ++r)
+            expand(S, rec[r], sel);
+        acc_entry(A, vc, sel.best, sel.pay, a);
+        last = sel.best;
+    }
+    finish_voxel(A, row, vc, a);
 }
 
-// One CTA per voxel with more than kShortSeg contributions.
-__global__ void __launch_bounds__(128) final_long(Final F)
+__global__ void __launch_bounds__(kConsumeThreads, 8) brick_consume(SolveArgs A)
 {
-    __shared__ unsigned long long skey[kLongSmem];
-    __shared__ uint32_t spay[kLongSmem];
-    __shared__ uint16_t sperm[kLongSmem];
-    const uint32_t nl = F.counters[C_LONG];
-    for (uint32_t li = blockIdx.x; li < nl; li += gridDim.x)
+    __shared__ BrickShared S;
+    const int tid = threadIdx.x;
+    const uint32_t slot = blockIdx.x;
+    const Grid &g = A.m.g;
+    const long long b = A.active[slot];
+    int o[3];
+    brick_origin(g, b, o);
+    const Rec *rec = A.rec + A.roff[b];
+    const unsigned long long nrec = A.roff[b + 1] - A.roff[b];
+
+    // occupancy words, their prefix counts and the dense list of active voxels
+    if (tid < 32)
     {
-        const long long r = F.long_list[li];
-        const unsigned long long s = F.eseg[r];
-        const long long n = (long long)(F.eseg[r + 1] - s);
-        const int vc[3] = {F.vox[r * 3 + 0], F.vox[r * 3 + 1], F.vox[r * 3 + 2]};
-        if (n <= kLongSmem)
+        const uint32_t w = tid < kWordsPerBrick ? A.bits[b * kWordsPerBrick + tid] : 0u;
+        const uint32_t c = __popc(w);
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
         {
-            for (long long i = threadIdx.x; i < n; i += blockDim.x)
-            {
-                skey[i] = F.ekey[s + i];
-                spay[i] = F.epay[s + i];
-            }
-            __syncthreads();
-            for (long long i = threadIdx.x; i < n; i += blockDim.x)
-            {
-                const unsigned long long ki = skey[i];
-                int rank = 0;
-                for (long long j = 0; j < n; ++j)
-                    rank += (skey[j] < ki) || (skey[j] == ki && j < i);
-                sperm[rank] = (uint16_t)i;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0)
-            {
-                Acc a;
-                acc_init(a);
-                for (long long i = 0; i < n; ++i)
-                    acc_entry(F, vc, skey[sperm[i]], spay[sperm[i]], a);
-                finish_voxel(F, r, vc, a);
-            }
-            __syncthreads();
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (tid >= d)
+                incl += y;
         }
-        else if (threadIdx.x == 0)
+        if (tid < kWordsPerBrick)
         {
-            // very long segment: repeated selection of the next key (keys are unique per voxel)
+            S.bits[tid] = w;
+            S.wpre[tid] = incl - c;
+            uint32_t x = w, k = incl - c;
+            while (x)
+            {
+                const int bt = __ffs(x) - 1;
+                x &= x - 1u;
+                S.vl[k++] = (uint16_t)(tid * 32 + bt);
+            }
+        }
+        if (tid == 31)
+        {
+            S.nvox = (int)incl;
+            S.big_n = 0;
+            S.status = 0;
+        }
+    }
+    for (int i = tid; i < 512; i += blockDim.x)
+    {
+        S.cnt[i] = 0;
+        S.fill[i] = 0;
+    }
+    __syncthreads();
+    const int nvox = S.nvox;
+    const unsigned long long vbase = A.bbase[b];
+
+    for (int i = tid; i < nvox; i += blockDim.x)
+    {
+        const int lv = S.vl[i];
+        const long long row = (long long)(vbase + i);
+        A.vox[row * 3 + 0] = o[0] + (lv & 7);
+        A.vox[row * 3 + 1] = o[1] + ((lv >> 3) & 7);
+        A.vox[row * 3 + 2] = o[2] + (lv >> 6);
+    }
+
+    {
+        CountSink cs{S};
+        for (unsigned long long r = tid; r < nrec; r += blockDim.x)
+            expand(S, rec[r], cs);
+    }
+    __syncthreads();
+    for (int i = tid; i < nvox; i += blockDim.x)
+    {
+        const uint32_t c = S.cnt[i];
+        if (c > (uint32_t)kWindow)
+            S.big[atomicAdd(&S.big_n, 1)] = (uint16_t)i;
+        else if (c == 0)
+            S.status = ST_REPLAY; // every active voxel receives at least one scanline contribution
+    }
+    scan_counts(S, nvox);
+    __syncthreads();
+    if (tid == 0 && S.status)
+        atomicOr(&A.counters[C_STATUS], S.status);
+
+    // windows of consecutive voxels whose contributions fit in shared memory
+    int lo = 0;
+    while (lo < nvox)
+    {
+        if (tid == 0)
+        {
+            int hi = lo;
+            const uint32_t base = S.off[lo];
+            if (S.total - base <= (uint32_t)kWindow)
+                hi = nvox;
+            else
+                while (hi < nvox && S.off[hi] + (S.cnt[hi] > (uint32_t)kWindow ? 0u : S.cnt[hi]) - base <= (uint32_t)kWindow)
+                    ++hi;
+            S.win_lo = lo;
+            S.win_hi = hi;
+            S.win_base = base;
+            S.long_n = 0;
+        }
+        __syncthreads();
+        const int wlo = S.win_lo, whi = S.win_hi;
+        const uint32_t wbase = S.win_base;
+        {
+            FillSink fs{S, wlo, whi, wbase};
+            for (unsigned long long r = tid; r < nrec; r += blockDim.x)
+                expand(S, rec[r], fs);
+        }
+        __syncthreads();
+        for (int i = wlo + tid; i < whi; i += blockDim.x)
+        {
+            const uint32_t n = S.cnt[i];
+            if (n == 0 || n > (uint32_t)kWindow)
+                continue;
+            if (n > (uint32_t)kThreadSort)
+            {
+                S.longl[atomicAdd(&S.long_n, 1)] = (uint16_t)i;
+                continue;
+            }
+            const uint32_t s0 = S.off[i] - wbase;
+            for (uint32_t x = 1; x < n; ++x)
+            {
+                const unsigned long long k = S.key[s0 + x];
+                const uint32_t p = S.pay[s0 + x];
+                uint32_t j = x;
+                while (j > 0 && S.key[s0 + j - 1] > k)
+                {
+                    S.key[s0 + j] = S.key[s0 + j - 1];
+                    S.pay[s0 + j] = S.pay[s0 + j - 1];
+                    --j;
+                }
+                S.key[s0 + j] = k;
+                S.pay[s0 + j] = p;
+            }
+            for (uint32_t x = 0; x < n; ++x)
+                S.perm[s0 + x] = (uint16_t)x;
+        }
+        __syncthreads();
+        const int nlong = S.long_n;
+        for (int li = 0; li < nlong; ++li)
+        {
+            const int i = S.longl[li];
+            const uint32_t n = S.cnt[i];
+            const uint32_t s0 = S.off[i] - wbase;
+            for (uint32_t x = tid; x < n; x += blockDim.x)
+            {
+                const unsigned long long kx = S.key[s0 + x];
+                uint32_t r = 0;
+                for (uint32_t j = 0; j < n; ++j)
+                {
+                    const unsigned long long kj = S.key[s0 + j];
+                    r += (kj < kx) || (kj == kx && j < x);
+                }
+                S.perm[s0 + r] = (uint16_t)x;
+            }
+        }
+        __syncthreads();
+        for (int i = wlo + tid; i < whi; i += blockDim.x)
+        {
+            const uint32_t n = S.cnt[i];
+            if (n == 0 || n > (uint32_t)kWindow)
+                continue;
+            const uint32_t s0 = S.off[i] - wbase;
+            const int lv = S.vl[i];
+            const int vc[3] = {o[0] + (lv & 7), o[1] + ((lv >> 3) & 7), o[2] + (lv >> 6)};
             Acc a;
             acc_init(a);
-            unsigned long long last = 0;
-            for (long long step = 0; step < n; ++step)
+            for (uint32_t x = 0; x < n; ++x)
             {
-                unsigned long long best = ~0ull;
-                uint32_t bp = 0;
-                for (long long j = 0; j < n; ++j)
-                {
-                    const unsigned long long kj = F.ekey[s + j];
-                    if ((step == 0 || kj > last) && kj <= best)
-                    {
-                        best = kj;
-                        bp = F.epay[s + j];
-                    }
-                }
-                acc_entry(F, vc, best, bp, a);
-                last = best;
+                const uint32_t j = s0 + S.perm[s0 + x];
+                acc_entry(A, vc, S.key[j], S.pay[j], a);
             }
-            finish_voxel(F, r, vc, a);
+            finish_voxel(A, (long long)(vbase + i), vc, a);
         }
+        __syncthreads();
+        lo = whi;
+    }
+
+    const int nbig = S.big_n;
+    for (int k = tid; k < nbig; k += blockDim.x)
+    {
+        const int i = S.big[k];
+        const int lv = S.vl[i];
+        const int vc[3] = {o[0] + (lv & 7), o[1] + ((lv >> 3) & 7), o[2] + (lv >> 6)};
+        select_voxel(A, S, i, rec, nrec, (long long)(vbase + i), vc);
+    }
+}
+
+// Constrained search (faces, edges, corners of the voxel box) for the voxels
+// whose unconstrained solution left the box; one thread per listed voxel.
+__global__ void __launch_bounds__(128) constrained_solve(const float *__restrict__ clist, const uint32_t *__restrict__ counters,
+                                                         uint32_t cap, Grid g, float *__restrict__ dual)
+{
+    const uint32_t n = min(counters[C_CONSTRAINED], cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const float *c = clist + (size_t)i * 16;
+        const long long row = __float_as_int(c[0]);
+        const int vc[3] = {__float_as_int(c[1]), __float_as_int(c[2]), __float_as_int(c[3])};
+        float q[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k)
+            q[k] = c[4 + k];
+        float v[3];
+        solve_constrained(vc, g, q, v);
+        dual[row * 3 + 0] = v[0];
+        dual[row * 3 + 1] = v[1];
+        dual[row * 3 + 2] = v[2];
+    }
+}
+
+// Occupancy only: coordinates of every active voxel, one CTA per active brick.
+__global__ void __launch_bounds__(128) brick_coords(const uint32_t *__restrict__ bits, const unsigned long long *__restrict__ bbase,
+                                                    const uint32_t *__restrict__ active, Grid g, int32_t *__restrict__ vox)
+{
+    __shared__ uint32_t sb[kWordsPerBrick], sp[kWordsPerBrick];
+    const long long b = active[blockIdx.x];
+    if (threadIdx.x < kWordsPerBrick)
+        sb[threadIdx.x] = bits[b * kWordsPerBrick + threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint32_t r = 0;
+        for (int w = 0; w < kWordsPerBrick; ++w)
+        {
+            sp[w] = r;
+            r += __popc(sb[w]);
+        }
+    }
+    __syncthreads();
+    int o[3];
+    brick_origin(g, b, o);
+    const unsigned long long base = bbase[b];
+    for (int lv = threadIdx.x; lv < 512; lv += blockDim.x)
+    {
+        const int w = lv >> 5, bt = lv & 31;
+        if (!((sb[w] >> bt) & 1u))
+            continue;
+        const long long row = (long long)(base + sp[w] + __popc(sb[w] & ((1u << bt) - 1u)));
+        vox[row * 3 + 0] = o[0] + (lv & 7);
+        vox[row * 3 + 1] = o[1] + ((lv >> 3) & 7);
+        vox[row * 3 + 2] = o[2] + (lv >> 6);
     }
 }
 
@@ -864,9 +1287,9 @@ struct ovx_fdg_context
 {
     int device = 0;
     int sms = 148;
-    Buf bits, bcount, bbase, word_base, counters, scan_large, face_large;
-    Buf vcnt, voff, emax, blist;
-    Buf ecount, eseg, ekey, epay, long_list, cub_tmp;
+    Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
+    Buf vcnt, voff, emax, bkeys;
+    Buf rcnt, roff, rec, clist, cub_tmp;
     unsigned long long *host = nullptr; // pinned readback words
     std::string err;
     // state between begin and finish
@@ -879,11 +1302,24 @@ struct ovx_fdg_context
     long long nf = 0;
     float origin[3] = {0, 0, 0};
     float fw = 0, bw = 0, rw = 0;
-    long long n_vox = 0;
+    long long n_vox = 0, n_active = 0, n_rec = 0, n_boundary = 0;
+    int finished = 0;
 };
 
 namespace
 {
+
+template <typename Ctx>
+int buffer_list(Ctx *c, Buf **out)
+{
+    Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
+                &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->rcnt, &c->roff, &c->rec,
+                &c->clist, &c->cub_tmp};
+    const int n = (int)(sizeof(b) / sizeof(b[0]));
+    for (int i = 0; i < n; ++i)
+        out[i] = b[i];
+    return n;
+}
 
 int fail(ovx_fdg_context *c, int status, const char *what)
 {
@@ -963,6 +1399,7 @@ int check_grid(ovx_fdg_context *ctx, const ovx_fdg_grid *grid, Grid &g)
         if (!(vs > 0.0f) || !(vs < 3.0e38f))
             return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "voxel_size must be positive and finite");
         g.vs[a] = vs;
+        g.rv[a] = 1.0 / (double)vs;
         g.gmin[a] = grid->grid_min[a];
         g.gmax[a] = grid->grid_max[a];
         const long long sz = (long long)grid->grid_max[a] - (long long)grid->grid_min[a];
@@ -972,58 +1409,30 @@ int check_grid(ovx_fdg_context *ctx, const ovx_fdg_grid *grid, Grid &g)
         g.nb[a] = (int)((sz + kBrick - 1) / kBrick);
         nb *= g.nb[a];
     }
-    if (nb * kWordsPerBrick * 4ll > (64ll << 30))
+    if (nb * kWordsPerBrick * 4ll > (64ll << 30) || nb >= (1ll << 31))
         return fail(ctx, OVX_FDG_CAPACITY, "grid too large for the dense brick bitmap (64 GiB limit)");
     g.nbricks = nb;
     return OVX_FDG_OK;
 }
 
-template <typename IdxT>
-void launch_mark(Pass &P, cudaStream_t st, int sms)
+Mesh make_mesh(const ovx_fdg_context *c)
 {
-    if (P.nf > 0)
-        tri_pass<MARK, IdxT><<<blocks_for(P.nf, kThreads), kThreads, 0, st>>>(P);
-    large_scan<MARK, IdxT><<<sms * 4, 128, 0, st>>>(P);
+    Mesh m{};
+    m.g = c->g;
+    m.verts = c->verts;
+    m.nv = c->nv;
+    m.faces = c->faces;
+    m.nf = c->nf;
+    m.ox = c->origin[0];
+    m.oy = c->origin[1];
+    m.oz = c->origin[2];
+    return m;
 }
 
-template <int M, typename IdxT>
-void launch_replay(Pass &P, cudaStream_t st, int sms, bool boundary)
+uint32_t cap_u32(const Buf &b, size_t elem)
 {
-    if (P.nf > 0)
-        tri_pass<M, IdxT><<<blocks_for(P.nf, kThreads), kThreads, 0, st>>>(P);
-    large_scan<M, IdxT><<<sms * 4, 128, 0, st>>>(P);
-    if (P.face_on)
-        large_face<M, IdxT><<<sms * 4, 128, 0, st>>>(P);
-    if (boundary)
-        boundary_pass<M><<<sms * 8, kThreads, 0, st>>>(P);
-}
-
-Pass make_pass(ovx_fdg_context *c)
-{
-    Pass P{};
-    P.g = c->g;
-    P.verts = c->verts;
-    P.nv = c->nv;
-    P.faces = c->faces;
-    P.nf = c->nf;
-    P.ox = c->origin[0];
-    P.oy = c->origin[1];
-    P.oz = c->origin[2];
-    P.bits = (uint32_t *)c->bits.p;
-    P.word_base = (const uint32_t *)c->word_base.p;
-    P.ecount = (uint32_t *)c->ecount.p;
-    P.eseg = (const unsigned long long *)c->eseg.p;
-    P.ekey = (unsigned long long *)c->ekey.p;
-    P.epay = (uint32_t *)c->epay.p;
-    P.counters = (uint32_t *)c->counters.p;
-    P.scan_large = (uint32_t *)c->scan_large.p;
-    P.scan_large_cap = (uint32_t)(c->scan_large.cap / 4 < 0xffffffffull ? c->scan_large.cap / 4 : 0xffffffffull);
-    P.face_large = (uint32_t *)c->face_large.p;
-    P.face_large_cap = (uint32_t)(c->face_large.cap / 4 < 0xffffffffull ? c->face_large.cap / 4 : 0xffffffffull);
-    P.blist = (const uint2 *)c->blist.p;
-    P.blist_cap = (uint32_t)(c->blist.cap / 8 < 0xffffffffull ? c->blist.cap / 8 : 0xffffffffull);
-    P.face_on = c->fw > 0.0f ? 1 : 0;
-    return P;
+    const size_t n = b.cap / elem;
+    return (uint32_t)(n < 0xffffffffull ? n : 0xffffffffull);
 }
 
 int status_to_error(ovx_fdg_context *ctx, uint32_t st)
@@ -1033,47 +1442,103 @@ int status_to_error(ovx_fdg_context *ctx, uint32_t st)
     if (st & ST_LIST_OVERFLOW)
         return fail(ctx, OVX_FDG_INTERNAL, "work list overflow");
     if (st & ST_REPLAY)
-        return fail(ctx, OVX_FDG_INTERNAL, "contribution replay mismatch");
+        return fail(ctx, OVX_FDG_INTERNAL, "record replay mismatch");
     if (st & ST_WALK_GUARD)
         return fail(ctx, OVX_FDG_INTERNAL, "boundary walk exceeded its step bound (non-finite vertex?)");
     return OVX_FDG_OK;
 }
 
-// Occupancy stage shared by the full conversion and intersect_occ.
-int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool with_boundary, int64_t *num_voxels)
+GenArgs make_gen(ovx_fdg_context *ctx)
+{
+    GenArgs A{};
+    A.m = make_mesh(ctx);
+    A.bits = (uint32_t *)ctx->bits.p;
+    A.rcnt = (uint32_t *)ctx->rcnt.p;
+    A.roff = (const unsigned long long *)ctx->roff.p;
+    A.rec = (Rec *)ctx->rec.p;
+    A.qtab = (float *)ctx->qtab.p;
+    A.counters = (uint32_t *)ctx->counters.p;
+    A.scan_large = (uint32_t *)ctx->scan_large.p;
+    A.scan_large_cap = cap_u32(ctx->scan_large, 4);
+    A.face_large = (uint32_t *)ctx->face_large.p;
+    A.face_large_cap = cap_u32(ctx->face_large, 4);
+    A.bkeys = (const unsigned long long *)ctx->bkeys.p;
+    A.bkeys_cap = cap_u32(ctx->bkeys, 8);
+    return A;
+}
+
+template <int M, typename IdxT>
+void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
+{
+    if (ctx->nf > 0)
+        tri_events<M, IdxT><<<blocks_for(3 * ctx->nf, kThreads), kThreads, 0, st>>>(A);
+    large_events<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
+}
+
+template <int M, typename IdxT>
+void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
+{
+    if (ctx->fw > 0.0f && ctx->nf > 0)
+    {
+        face_records<M, IdxT><<<blocks_for((long long)kFaceSlots * ctx->nf, kThreads), kThreads, 0, st>>>(A);
+        large_face_records<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
+    }
+    if (ctx->bw > 0.0f && ctx->nf > 0)
+        boundary_records<M><<<ctx->sms * 8, kThreads, 0, st>>>(A);
+}
+
+// Occupancy stage shared by the full conversion and intersect_occ; ends with
+// the one host synchronisation of a conversion.
+int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *num_voxels)
 {
     const Grid &g = ctx->g;
-    const long long nf = ctx->nf;
-    OVX_CUDA(ensure(ctx->bits, (size_t)g.nbricks * kWordsPerBrick * 4));
-    OVX_CUDA(ensure(ctx->bcount, (size_t)(g.nbricks + 1) * 4));
-    OVX_CUDA(ensure(ctx->bbase, (size_t)(g.nbricks + 1) * 8));
+    const long long nf = ctx->nf, nb = g.nbricks;
+    const bool boundary = full && ctx->bw > 0.0f;
+    OVX_CUDA(ensure(ctx->bits, (size_t)nb * kWordsPerBrick * 4));
+    OVX_CUDA(ensure(ctx->bcount, (size_t)(nb + 1) * 4));
+    OVX_CUDA(ensure(ctx->bbase, (size_t)(nb + 1) * 8));
+    OVX_CUDA(ensure(ctx->aflag, (size_t)(nb + 1) * 4));
+    OVX_CUDA(ensure(ctx->aslot, (size_t)(nb + 1) * 8));
+    OVX_CUDA(ensure(ctx->active, (size_t)(nb + 1) * 4));
     OVX_CUDA(ensure(ctx->counters, C_WORDS * 4));
     OVX_CUDA(ensure(ctx->scan_large, (size_t)(3 * nf + 1) * 4));
     OVX_CUDA(ensure(ctx->face_large, (size_t)(nf + 1) * 4));
-    if (with_boundary)
+    OVX_CUDA(ensure(ctx->rcnt, (size_t)(nb + 1) * 4));
+    OVX_CUDA(ensure(ctx->roff, (size_t)(nb + 1) * 8));
+    if (full)
+        OVX_CUDA(ensure(ctx->qtab, (size_t)(nf + 1) * 40));
+    if (boundary)
     {
         OVX_CUDA(ensure(ctx->vcnt, (size_t)(ctx->nv + 1) * 4));
         OVX_CUDA(ensure(ctx->voff, (size_t)(ctx->nv + 1) * 8));
         OVX_CUDA(ensure(ctx->emax, (size_t)(3 * nf + 1) * 4));
-        OVX_CUDA(ensure(ctx->blist, (size_t)(3 * nf + 1) * 8));
+        OVX_CUDA(ensure(ctx->bkeys, (size_t)(3 * nf + 1) * 8));
     }
-    OVX_CUDA(cudaMemsetAsync(ctx->bits.p, 0, (size_t)g.nbricks * kWordsPerBrick * 4, st));
+    OVX_CUDA(cudaMemsetAsync(ctx->bits.p, 0, (size_t)nb * kWordsPerBrick * 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->counters.p, 0, C_WORDS * 4, st));
-    OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->bcount.p + g.nbricks, 0, 4, st));
+    OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
+    OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->bcount.p + nb, 0, 4, st));
+    OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->aflag.p + nb, 0, 4, st));
 
-    Pass P = make_pass(ctx);
+    GenArgs A = make_gen(ctx);
+    if (!full)
+        A.qtab = nullptr;
     if (ctx->fbytes == 8)
-        launch_mark<long long>(P, st, ctx->sms);
+        launch_events<COUNT, long long>(ctx, A, st);
     else
-        launch_mark<int>(P, st, ctx->sms);
+        launch_events<COUNT, int>(ctx, A, st);
     OVX_CUDA(cudaGetLastError());
 
-    brick_count<<<blocks_for(g.nbricks, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->bits.p, g.nbricks,
-                                                                      (uint32_t *)ctx->bcount.p);
+    brick_count<<<blocks_for(nb, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->bits.p, nb, (uint32_t *)ctx->bcount.p,
+                                                               (uint32_t *)ctx->aflag.p);
     OVX_CUDA(cudaGetLastError());
-    OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->bcount.p, (unsigned long long *)ctx->bbase.p, g.nbricks + 1, st));
+    OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->bcount.p, (unsigned long long *)ctx->bbase.p, nb + 1, st));
+    OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->aflag.p, (unsigned long long *)ctx->aslot.p, nb + 1, st));
+    brick_slots<<<blocks_for(nb, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->aflag.p, (const unsigned long long *)ctx->aslot.p,
+                                                               nb, (uint32_t *)ctx->active.p);
+    OVX_CUDA(cudaGetLastError());
 
-    if (with_boundary && nf > 0)
+    if (boundary && nf > 0)
     {
         OVX_CUDA(cudaMemsetAsync(ctx->vcnt.p, 0, (size_t)(ctx->nv + 1) * 4, st));
         uint32_t *vcnt = (uint32_t *)ctx->vcnt.p;
@@ -1091,16 +1556,29 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool with_boundary, i
             edge_fill<int><<<blocks_for(nf, kThreads), kThreads, 0, st>>>((const int *)ctx->faces, nf, ctx->nv, voff, vcnt,
                                                                          (uint32_t *)ctx->emax.p);
         OVX_CUDA(cudaGetLastError());
-        if (ctx->nv > 0)
-            edge_find<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (uint32_t *)ctx->emax.p, ctx->nv, (uint2 *)ctx->blist.p,
-                                                                         P.blist_cap, (uint32_t *)ctx->counters.p);
+        edge_find<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (uint32_t *)ctx->emax.p, ctx->nv,
+                                                                     (unsigned long long *)ctx->bkeys.p, cap_u32(ctx->bkeys, 8),
+                                                                     (uint32_t *)ctx->counters.p);
         OVX_CUDA(cudaGetLastError());
     }
 
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[0], (unsigned long long *)ctx->bbase.p + g.nbricks, 8, cudaMemcpyDeviceToHost, st));
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[1], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
+    if (full)
+    {
+        A = make_gen(ctx);
+        if (ctx->fbytes == 8)
+            launch_faces_boundary<COUNT, long long>(ctx, A, st);
+        else
+            launch_faces_boundary<COUNT, int>(ctx, A, st);
+        OVX_CUDA(cudaGetLastError());
+        OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->rcnt.p, (unsigned long long *)ctx->roff.p, nb + 1, st));
+        OVX_CUDA(cudaMemcpyAsync(&ctx->host[2], (unsigned long long *)ctx->roff.p + nb, 8, cudaMemcpyDeviceToHost, st));
+    }
+
+    OVX_CUDA(cudaMemcpyAsync(&ctx->host[0], (unsigned long long *)ctx->bbase.p + nb, 8, cudaMemcpyDeviceToHost, st));
+    OVX_CUDA(cudaMemcpyAsync(&ctx->host[1], (unsigned long long *)ctx->aslot.p + nb, 8, cudaMemcpyDeviceToHost, st));
+    OVX_CUDA(cudaMemcpyAsync(&ctx->host[4], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
     OVX_CUDA(cudaStreamSynchronize(st));
-    const uint32_t *hc = (const uint32_t *)&ctx->host[1];
+    const uint32_t *hc = (const uint32_t *)&ctx->host[4];
     const int rc = status_to_error(ctx, hc[C_STATUS]);
     if (rc != OVX_FDG_OK)
         return rc;
@@ -1108,6 +1586,9 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool with_boundary, i
     if (n >= (1ull << 31))
         return fail(ctx, OVX_FDG_CAPACITY, "more than 2^31-1 occupied voxels");
     ctx->n_vox = (long long)n;
+    ctx->n_active = (long long)ctx->host[1];
+    ctx->n_rec = full ? (long long)ctx->host[2] : 0;
+    ctx->n_boundary = hc[C_BOUNDARY];
     *num_voxels = (int64_t)n;
     return OVX_FDG_OK;
 }
@@ -1136,7 +1617,7 @@ int ovx_fdg_context_create(int device, ovx_fdg_context **out)
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
-    cudaError_t e = cudaMallocHost((void **)&ctx->host, 16 * sizeof(unsigned long long));
+    cudaError_t e = cudaMallocHost((void **)&ctx->host, 32 * sizeof(unsigned long long));
     cudaSetDevice(prev);
     if (e != cudaSuccess)
     {
@@ -1154,12 +1635,11 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(ctx->device);
-    Buf *all[] = {&ctx->bits, &ctx->bcount, &ctx->bbase, &ctx->word_base, &ctx->counters, &ctx->scan_large, &ctx->face_large,
-                  &ctx->vcnt, &ctx->voff, &ctx->emax, &ctx->blist, &ctx->ecount, &ctx->eseg, &ctx->ekey, &ctx->epay,
-                  &ctx->long_list, &ctx->cub_tmp};
-    for (Buf *b : all)
-        if (b->p)
-            cudaFree(b->p);
+    Buf *list[32];
+    const int n = buffer_list(ctx, list);
+    for (int i = 0; i < n; ++i)
+        if (list[i]->p)
+            cudaFree(list[i]->p);
     if (ctx->host)
         cudaFreeHost(ctx->host);
     cudaSetDevice(prev);
@@ -1198,12 +1678,11 @@ int64_t ovx_fdg_workspace_bytes(const ovx_fdg_context *ctx)
 {
     if (!ctx)
         return 0;
-    const Buf *all[] = {&ctx->bits, &ctx->bcount, &ctx->bbase, &ctx->word_base, &ctx->counters, &ctx->scan_large, &ctx->face_large,
-                        &ctx->vcnt, &ctx->voff, &ctx->emax, &ctx->blist, &ctx->ecount, &ctx->eseg, &ctx->ekey, &ctx->epay,
-                        &ctx->long_list, &ctx->cub_tmp};
+    Buf *list[32];
+    const int n = buffer_list(const_cast<ovx_fdg_context *>(ctx), list);
     int64_t s = 0;
-    for (const Buf *b : all)
-        s += (int64_t)b->cap;
+    for (int i = 0; i < n; ++i)
+        s += (int64_t)list[i]->cap;
     return s;
 }
 
@@ -1244,7 +1723,7 @@ int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int
     ctx->fw = face_weight;
     ctx->bw = boundary_weight;
     ctx->rw = regularization_weight;
-    rc = occupancy_stage(ctx, (cudaStream_t)stream, boundary_weight > 0.0f, num_voxels);
+    rc = occupancy_stage(ctx, (cudaStream_t)stream, true, num_voxels);
     if (rc != OVX_FDG_OK)
         return rc;
     ctx->phase = 1;
@@ -1258,6 +1737,7 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     if (ctx->phase != 1)
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "ovx_fdg_finish without a successful ovx_fdg_begin");
     ctx->phase = 0;
+    ctx->finished = 0;
     const long long n = ctx->n_vox;
     if (n == 0)
         return OVX_FDG_OK;
@@ -1265,67 +1745,62 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "NULL output buffer");
     cudaStream_t st = (cudaStream_t)stream;
     OVX_CUDA(cudaSetDevice(ctx->device));
-    const Grid &g = ctx->g;
-    OVX_CUDA(ensure(ctx->word_base, (size_t)g.nbricks * kWordsPerBrick * 4));
-    OVX_CUDA(ensure(ctx->ecount, (size_t)(n + 1) * 4));
-    OVX_CUDA(ensure(ctx->eseg, (size_t)(n + 1) * 8));
-    OVX_CUDA(ensure(ctx->long_list, (size_t)(n + 1) * 4));
+    const long long nb = ctx->g.nbricks;
+    OVX_CUDA(ensure(ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
+    OVX_CUDA(ensure(ctx->clist, (size_t)(n + 1) * 16 * 4));
+    OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
+    OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONSTRAINED, 0, 4, st));
 
-    brick_emit<<<blocks_for(g.nbricks, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->bits.p,
-                                                                     (const unsigned long long *)ctx->bbase.p, g,
-                                                                     (uint32_t *)ctx->word_base.p, voxel_indices);
-    OVX_CUDA(cudaGetLastError());
-    OVX_CUDA(cudaMemsetAsync(ctx->ecount.p, 0, (size_t)(n + 1) * 4, st));
-
-    const bool boundary = ctx->bw > 0.0f;
-    Pass P = make_pass(ctx);
+    GenArgs A = make_gen(ctx);
+    A.qtab = nullptr;
     if (ctx->fbytes == 8)
-        launch_replay<COUNT, long long>(P, st, ctx->sms, boundary);
+    {
+        launch_events<FILL, long long>(ctx, A, st);
+        launch_faces_boundary<FILL, long long>(ctx, A, st);
+    }
     else
-        launch_replay<COUNT, int>(P, st, ctx->sms, boundary);
-    OVX_CUDA(cudaGetLastError());
-    OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->ecount.p, (unsigned long long *)ctx->eseg.p, n + 1, st));
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[0], (unsigned long long *)ctx->eseg.p + n, 8, cudaMemcpyDeviceToHost, st));
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[1], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
-    OVX_CUDA(cudaStreamSynchronize(st));
-    int rc = status_to_error(ctx, ((const uint32_t *)&ctx->host[1])[C_STATUS]);
-    if (rc != OVX_FDG_OK)
-        return rc;
-    const unsigned long long E = ctx->host[0];
-    OVX_CUDA(ensure(ctx->ekey, (size_t)E * 8));
-    OVX_CUDA(ensure(ctx->epay, (size_t)E * 4));
-
-    P = make_pass(ctx);
-    if (ctx->fbytes == 8)
-        launch_replay<FILL, long long>(P, st, ctx->sms, boundary);
-    else
-        launch_replay<FILL, int>(P, st, ctx->sms, boundary);
+    {
+        launch_events<FILL, int>(ctx, A, st);
+        launch_faces_boundary<FILL, int>(ctx, A, st);
+    }
     OVX_CUDA(cudaGetLastError());
 
-    Final F{};
-    F.g = g;
-    F.verts = ctx->verts;
-    F.nv = ctx->nv;
-    F.faces = ctx->faces;
-    F.fbytes = ctx->fbytes;
-    F.ox = ctx->origin[0];
-    F.oy = ctx->origin[1];
-    F.oz = ctx->origin[2];
-    F.bw = ctx->bw;
-    F.rw = ctx->rw;
-    F.eseg = (const unsigned long long *)ctx->eseg.p;
-    F.ekey = (const unsigned long long *)ctx->ekey.p;
-    F.epay = (const uint32_t *)ctx->epay.p;
-    F.vox = voxel_indices;
-    F.dual = dual_vertices;
-    F.flags = intersected;
-    F.counters = (uint32_t *)ctx->counters.p;
-    F.long_list = (uint32_t *)ctx->long_list.p;
-    F.n = n;
-    final_short<<<blocks_for(n, 128), 128, 0, st>>>(F);
-    final_long<<<ctx->sms * 2, 128, 0, st>>>(F);
+    SolveArgs SA{};
+    SA.m = make_mesh(ctx);
+    SA.bw = ctx->bw;
+    SA.rw = ctx->rw;
+    SA.bits = (const uint32_t *)ctx->bits.p;
+    SA.bbase = (const unsigned long long *)ctx->bbase.p;
+    SA.active = (const uint32_t *)ctx->active.p;
+    SA.roff = (const unsigned long long *)ctx->roff.p;
+    SA.rec = (const Rec *)ctx->rec.p;
+    SA.qtab = (const float *)ctx->qtab.p;
+    SA.vox = voxel_indices;
+    SA.dual = dual_vertices;
+    SA.flags = intersected;
+    SA.counters = (uint32_t *)ctx->counters.p;
+    SA.clist = (float *)ctx->clist.p;
+    SA.clist_cap = (uint32_t)(n + 1);
+    if (ctx->n_active > 0)
+        brick_consume<<<(unsigned)ctx->n_active, kConsumeThreads, 0, st>>>(SA);
+    constrained_solve<<<ctx->sms * 8, 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
+                                                    ctx->g, dual_vertices);
     OVX_CUDA(cudaGetLastError());
+    OVX_CUDA(cudaMemcpyAsync(&ctx->host[8], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
+    ctx->finished = 1;
     return OVX_FDG_OK;
+}
+
+int ovx_fdg_sync_status(ovx_fdg_context *ctx, void *stream)
+{
+    if (!ctx)
+        return OVX_FDG_INVALID_ARGUMENT;
+    OVX_CUDA(cudaSetDevice(ctx->device));
+    OVX_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (!ctx->finished)
+        return OVX_FDG_OK;
+    ctx->finished = 0;
+    return status_to_error(ctx, ((const uint32_t *)&ctx->host[8])[C_STATUS]);
 }
 
 int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *triangles, int64_t num_triangles,
@@ -1377,9 +1852,8 @@ int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "NULL output buffer");
     cudaStream_t st = (cudaStream_t)stream;
     OVX_CUDA(cudaSetDevice(ctx->device));
-    brick_emit<<<blocks_for(ctx->g.nbricks, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->bits.p,
-                                                                          (const unsigned long long *)ctx->bbase.p, ctx->g,
-                                                                          nullptr, voxel_indices);
+    brick_coords<<<(unsigned)ctx->n_active, 128, 0, st>>>((const uint32_t *)ctx->bits.p, (const unsigned long long *)ctx->bbase.p,
+                                                          (const uint32_t *)ctx->active.p, ctx->g, voxel_indices);
     OVX_CUDA(cudaGetLastError());
     return OVX_FDG_OK;
 }

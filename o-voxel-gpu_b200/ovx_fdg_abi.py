@@ -29,6 +29,7 @@ PROTOTYPES = [
     ("ovx_fdg_workspace_bytes", _I64, [_P]),
     ("ovx_fdg_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.c_int32, _I64, _P, _P, _F, _F, _F, ctypes.POINTER(_I64)]),
     ("ovx_fdg_finish", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("ovx_fdg_sync_status", ctypes.c_int, [_P, _P]),
     ("ovx_fdg_occupancy_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.POINTER(_I64)]),
     ("ovx_fdg_occupancy_finish", ctypes.c_int, [_P, _P, _P]),
 ]
@@ -100,7 +101,7 @@ class Context:
     def workspace_bytes(self) -> int:
         return int(self._lib.ovx_fdg_workspace_bytes(self.handle))
 
-    def mesh_to_fdg(self, vertices, faces, origin, voxel_size, grid_range, fw, bw, rw, stream=None):
+    def mesh_to_fdg(self, vertices, faces, origin, voxel_size, grid_range, fw, bw, rw, stream=None, check=True):
         """vertices: CUDA float32 [V,3]; faces: CUDA int32/int64 [F,3]; returns torch tensors."""
         import torch
 
@@ -120,6 +121,8 @@ class Context:
         ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t.numel() else 0)  # noqa: E731
         rc = self._lib.ovx_fdg_finish(self.handle, st, ptr(vox), ptr(dual), ptr(inter))
         self._check(rc, "ovx_fdg_finish")
+        if check:
+            self._check(self._lib.ovx_fdg_sync_status(self.handle, st), "ovx_fdg_sync_status")
         return vox, dual, inter
 
     def occupancy(self, triangles, voxel_size, grid_range, stream=None):

@@ -3,6 +3,8 @@ import sys
 
 import pytest
 
+os.environ.setdefault("OVX_FDG_CHECK", "1")  # the extension waits for and reports device-side checks
+
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 for p in (os.path.join(REPO, "o-voxel-gpu_b200"), REPO, os.path.dirname(os.path.abspath(__file__))):
     if p not in sys.path:
