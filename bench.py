@@ -1,0 +1,342 @@
+"""Benchmark: mesh -> flexible dual grid on B200.
+
+One step = one full conversion (occupancy, quadrics, solve) of the seeded
+280k-face / grid-512 primitives mesh (the reference's headline single-mesh
+case; its asset is not distributed, so a synthetic stand-in with the same
+size is used).  Prints one JSON line on rank 0.
+
+  value      Mfaces/s with inputs resident in HBM, through the C ABI
+             (libovx_fdg), CUDA events per step, L2 flushed between steps
+  e2e        the same metric through o_voxel.convert.mesh_to_flexible_dual_grid
+             with pinned host inputs: H2D copy, conversion, D2H of all outputs
+  roofline   compulsory bytes of a conversion (12V + 8*3F + 27N) over the
+             conversion time against the measured HBM copy bandwidth
+  cpu_baseline  the reference's CPU implementation on the host cores
+
+--impl reference times the reference CPU implementation alone.
+Multi-GPU: replicas only (each rank converts its own copy; no collective).
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "o-voxel-gpu_b200"))
+sys.path.insert(0, REPO)
+
+METRIC = "Mfaces/s & meshes/s mesh→FDG @grid512, batched vs plain GPU, exact occ"
+PUBLISHED_MFACES = 10.3  # reference CUDA path, RTX 4090, 280k faces, grid 512 (derived in BASELINE.md)
+CPU_SAMPLE_FACES = 48_000
+
+
+def load_workload():
+    import fdg_workloads as W
+
+    return W.primitives(1)
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def _ref_worker(args):
+    """Runs in a spawned process: one conversion of the sample by the reference CPU code."""
+    kind, v, f, vs, gr, fw, bw, rw = args
+    sys.path.insert(0, REPO)
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    if kind == "reference":
+        O.ref_mesh_to_fdg(v, f, vs, gr, fw, bw, rw)
+    else:
+        O.mesh_to_fdg(v, f, vs, gr, fw, bw, rw)
+    return time.perf_counter() - t0
+
+
+class CpuBaseline:
+    """The reference CPU implementation on all host cores: one conversion of a
+    bounded face sample per core per step (the reference CPU path is single-threaded)."""
+
+    def __init__(self, w, sample_faces=CPU_SAMPLE_FACES, cores=None):
+        from oracle import oracle as O
+
+        self.kind = "reference" if O.ref_module() is not None else "port"
+        v, f, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
+        self.faces = min(sample_faces, f.shape[0])
+        self.cores = cores or os.cpu_count() or 1
+        self.job = (self.kind, v, f[: self.faces], vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+        self.pool.map(_ref_worker, [self.job] * self.cores)  # warm the workers
+
+    def step(self):
+        t0 = time.perf_counter()
+        self.pool.map(_ref_worker, [self.job] * self.cores)
+        return time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def describe(self, value):
+        return {"value": value, "unit": "Mfaces/s", "cores": self.cores, "kind": self.kind,
+                "sample": f"first {self.faces} faces of the 282k-face grid-512 mesh, one conversion per core per step "
+                          f"({'reference src/convert/flexible_dual_grid.cpp built against the Eigen-API shim' if self.kind == 'reference' else 'C restatement of it'})"}
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            return
+        while not self._stop.is_set():
+            line = p.stdout.readline()
+            if not line:
+                break
+            self.samples.append([x.strip() for x in line.split(",")])
+        p.terminate()
+        try:
+            p.wait(timeout=5)
+        except Exception:
+            p.kill()
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, name in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    w = load_workload()
+    cb = CpuBaseline(w)
+    for _ in range(args.warmup):
+        cb.step()
+    times = [cb.step() for _ in range(args.steps)]
+    cb.close()
+    t = sum(times) / len(times)
+    value = cb.cores * cb.faces / t / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mfaces/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64,f32", "data": "synthetic (seeded primitives mesh)",
+            "config": {"workload": "primitives-282k-faces-grid512", "grid": 512, "faces": int(w.num_faces)},
+            "cpu_baseline": cb.describe(value),
+            "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+
+    import ovx_fdg_abi as abi
+    import o_voxel
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    w = load_workload()
+    F, V = w.num_faces, w.vertices.shape[0]
+    v_np, f_np, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
+    origin = np.asarray(w.aabb, np.float32)[0]
+    vd = torch.from_numpy(w.vertices).to(dev)
+    fd = torch.from_numpy(w.faces).to(dev)  # int64, consumed as supplied
+    ctx = abi.Context(dev.index)
+    kw = (origin, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def one():
+        return ctx.mesh_to_fdg(vd, fd, *kw, check=False)
+
+    out = None
+    for _ in range(max(args.warmup, 3)):
+        out = one()
+    torch.cuda.synchronize()
+    N = int(out[0].shape[0])
+
+    # device-resident timed region
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    launches0 = ctx.kernel_launches()
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = one()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    launches = ctx.kernel_launches() - launches0
+    clk = clocks.stop()
+    t_local = sum(ms)
+    t = torch.tensor([t_local], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    t_total = float(t.item())
+    ms_per_step = t_total / args.steps
+    value = world * F / (ms_per_step / 1e3) / 1e6
+    if ctx.handle:
+        ctx._check(abi.lib().ovx_fdg_sync_status(ctx.handle, abi.ctypes.c_void_p(stream.cuda_stream)), "status")
+
+    # stage breakdown (separate, profiled conversion)
+    ctx.set_profiling(True)
+    flush.zero_()
+    one()
+    stages = ctx.stage_times()
+    ctx.set_profiling(False)
+
+    # end to end through the public API, host buffers
+    vh = torch.from_numpy(w.vertices).pin_memory()
+    fh = torch.from_numpy(w.faces).pin_memory()
+    vox_h = torch.empty((N, 3), dtype=torch.int32).pin_memory()
+    dual_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
+    flag_h = torch.empty((N, 3), dtype=torch.bool).pin_memory()
+
+    def e2e_step():
+        vdev = vh.to(dev, non_blocking=True)
+        fdev = fh.to(dev, non_blocking=True)
+        a, b, c = o_voxel.convert.mesh_to_flexible_dual_grid(vdev, fdev, **w.kwargs())
+        vox_h.copy_(a, non_blocking=True)
+        dual_h.copy_(b, non_blocking=True)
+        flag_h.copy_(c, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    ems = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        ems.append(e0.elapsed_time(e1))
+    te = torch.tensor([sum(ems)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = float(te.item()) / args.steps
+    e2e_value = world * F / (e2e_ms / 1e3) / 1e6
+
+    if rank != 0:
+        ctx.close()
+        return
+    peak, peak_kind = peaks()
+    b_alg = 12 * V + 8 * 3 * F + 27 * N
+    achieved = b_alg / (ms_per_step / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(REPO, "profiles", "fdg_traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as fh_:
+            traffic = json.load(fh_).get("dram_bytes_per_conversion")
+    total_stage = sum(x for x in stages.values() if x > 0) or 1.0
+    dom = max(stages.items(), key=lambda kv: kv[1]) if stages else ("", 0.0)
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cb = CpuBaseline(w)
+        cpu_t = statistics.median([cb.step() for _ in range(2)])
+        cb.close()
+        cpu = cb.describe(cb.cores * cb.faces / cpu_t / 1e6)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mfaces/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": value / PUBLISHED_MFACES, "dtype": "f64,f32",
+        "data": "synthetic: seeded 48-primitive mesh (no dataset on the box)",
+        "config": {"workload": "primitives-282k-faces-grid512", "faces": F, "vertices": V, "voxels": N, "grid": 512,
+                   "weights": [w.face_weight, w.boundary_weight, w.regularization_weight], "faces_dtype": "int64",
+                   "l2": "flushed between steps (256 MB write outside the timed events)", "parallelism": f"replicas x{world}"},
+        "meshes_per_s": world / (ms_per_step / 1e3),
+        "e2e": {"value": e2e_value, "unit": "Mfaces/s", "ms_per_step": e2e_ms, "h2d_bytes_per_step": 12 * V + 8 * 3 * F,
+                "d2h_bytes_per_step": 27 * N, "api": "o_voxel.convert.mesh_to_flexible_dual_grid"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "scope": "whole conversion: compulsory bytes 12V+24F+27N over the conversion time",
+                     "dominant_stage": {"name": dom[0], "ms": dom[1], "share": dom[1] / total_stage}},
+        "stage_ms": stages,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": int(launches),
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -74,6 +74,20 @@ const char *ovx_fdg_last_error(const ovx_fdg_context *ctx);
 int64_t ovx_fdg_workspace_bytes(const ovx_fdg_context *ctx);
 
 /*
+ * Instrumentation (no counterpart in the reference, which has no CUDA-side
+ * timers).  With profiling on, the context records CUDA events between the
+ * pipeline stages of each conversion; ovx_fdg_stage_times waits for the last
+ * conversion and writes up to `capacity` stage durations in milliseconds
+ * (names from ovx_fdg_stage_name), returning how many it wrote.
+ * ovx_fdg_kernel_launches counts the kernels the library itself launched
+ * (library scans it calls are not counted).
+ */
+int ovx_fdg_set_profiling(ovx_fdg_context *ctx, int enable);
+int ovx_fdg_stage_times(ovx_fdg_context *ctx, float *ms, int capacity);
+const char *ovx_fdg_stage_name(int stage);
+int64_t ovx_fdg_kernel_launches(const ovx_fdg_context *ctx);
+
+/*
  * Occupancy stage of mesh -> flexible dual grid.
  *   vertices: device float32 [num_vertices, 3], NOT shifted; origin (host
  *             float[3], may be NULL for zero) is subtracted in float32 exactly

@@ -1275,6 +1275,25 @@ __global__ void __launch_bounds__(128) brick_coords(const uint32_t *__restrict__
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// Stage timers: CUDA events recorded at these points when profiling is on.
+enum
+{
+    EV_BEGIN = 0,
+    EV_EVENTS_COUNT,
+    EV_COMPACT,
+    EV_EDGES,
+    EV_RECORD_COUNT,
+    EV_FINISH,
+    EV_EVENTS_FILL,
+    EV_RECORD_FILL,
+    EV_CONSUME,
+    EV_CONSTRAINED,
+    kStageEvents
+};
+const char *const kStageNames[] = {"scanline_mark_count", "compaction", "boundary_edges", "face_boundary_count",
+                                   "scanline_fill", "face_boundary_fill", "brick_consume", "constrained_solve"};
+constexpr int kStages = 8;
+
 struct Buf
 {
     void *p = nullptr;
@@ -1304,6 +1323,9 @@ struct ovx_fdg_context
     float fw = 0, bw = 0, rw = 0;
     long long n_vox = 0, n_active = 0, n_rec = 0, n_boundary = 0;
     int finished = 0;
+    long long launches = 0; // kernels this library launched (its own, not CUB's)
+    bool profiling = false;
+    cudaEvent_t ev[kStageEvents] = {};
 };
 
 namespace
@@ -1319,6 +1341,12 @@ int buffer_list(Ctx *c, Buf **out)
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
     return n;
+}
+
+void stage(ovx_fdg_context *c, int i, cudaStream_t st)
+{
+    if (c->profiling && c->ev[i])
+        cudaEventRecord(c->ev[i], st);
 }
 
 int fail(ovx_fdg_context *c, int status, const char *what)
@@ -1471,8 +1499,12 @@ template <int M, typename IdxT>
 void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
 {
     if (ctx->nf > 0)
+    {
         tri_events<M, IdxT><<<blocks_for(3 * ctx->nf, kThreads), kThreads, 0, st>>>(A);
+        ++ctx->launches;
+    }
     large_events<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
+    ++ctx->launches;
 }
 
 template <int M, typename IdxT>
@@ -1482,9 +1514,13 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
     {
         face_records<M, IdxT><<<blocks_for((long long)kFaceSlots * ctx->nf, kThreads), kThreads, 0, st>>>(A);
         large_face_records<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
+        ctx->launches += 2;
     }
     if (ctx->bw > 0.0f && ctx->nf > 0)
+    {
         boundary_records<M><<<ctx->sms * 8, kThreads, 0, st>>>(A);
+        ++ctx->launches;
+    }
 }
 
 // Occupancy stage shared by the full conversion and intersect_occ; ends with
@@ -1520,6 +1556,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->bcount.p + nb, 0, 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->aflag.p + nb, 0, 4, st));
 
+    stage(ctx, EV_BEGIN, st);
     GenArgs A = make_gen(ctx);
     if (!full)
         A.qtab = nullptr;
@@ -1528,6 +1565,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     else
         launch_events<COUNT, int>(ctx, A, st);
     OVX_CUDA(cudaGetLastError());
+    stage(ctx, EV_EVENTS_COUNT, st);
 
     brick_count<<<blocks_for(nb, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->bits.p, nb, (uint32_t *)ctx->bcount.p,
                                                                (uint32_t *)ctx->aflag.p);
@@ -1536,7 +1574,9 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->aflag.p, (unsigned long long *)ctx->aslot.p, nb + 1, st));
     brick_slots<<<blocks_for(nb, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->aflag.p, (const unsigned long long *)ctx->aslot.p,
                                                                nb, (uint32_t *)ctx->active.p);
+    ctx->launches += 2;
     OVX_CUDA(cudaGetLastError());
+    stage(ctx, EV_COMPACT, st);
 
     if (boundary && nf > 0)
     {
@@ -1559,8 +1599,10 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         edge_find<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (uint32_t *)ctx->emax.p, ctx->nv,
                                                                      (unsigned long long *)ctx->bkeys.p, cap_u32(ctx->bkeys, 8),
                                                                      (uint32_t *)ctx->counters.p);
+        ctx->launches += 3;
         OVX_CUDA(cudaGetLastError());
     }
+    stage(ctx, EV_EDGES, st);
 
     if (full)
     {
@@ -1573,6 +1615,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->rcnt.p, (unsigned long long *)ctx->roff.p, nb + 1, st));
         OVX_CUDA(cudaMemcpyAsync(&ctx->host[2], (unsigned long long *)ctx->roff.p + nb, 8, cudaMemcpyDeviceToHost, st));
     }
+    stage(ctx, EV_RECORD_COUNT, st);
 
     OVX_CUDA(cudaMemcpyAsync(&ctx->host[0], (unsigned long long *)ctx->bbase.p + nb, 8, cudaMemcpyDeviceToHost, st));
     OVX_CUDA(cudaMemcpyAsync(&ctx->host[1], (unsigned long long *)ctx->aslot.p + nb, 8, cudaMemcpyDeviceToHost, st));
@@ -1642,8 +1685,62 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
             cudaFree(list[i]->p);
     if (ctx->host)
         cudaFreeHost(ctx->host);
+    for (int i = 0; i < kStageEvents; ++i)
+        if (ctx->ev[i])
+            cudaEventDestroy(ctx->ev[i]);
     cudaSetDevice(prev);
     delete ctx;
+}
+
+int ovx_fdg_set_profiling(ovx_fdg_context *ctx, int enable)
+{
+    if (!ctx)
+        return OVX_FDG_INVALID_ARGUMENT;
+    OVX_CUDA(cudaSetDevice(ctx->device));
+    if (enable)
+        for (int i = 0; i < kStageEvents; ++i)
+            if (!ctx->ev[i])
+                OVX_CUDA(cudaEventCreate(&ctx->ev[i]));
+    ctx->profiling = enable != 0;
+    return OVX_FDG_OK;
+}
+
+int ovx_fdg_stage_times(ovx_fdg_context *ctx, float *ms, int capacity)
+{
+    if (!ctx || !ms)
+        return -OVX_FDG_INVALID_ARGUMENT;
+    if (!ctx->profiling)
+        return 0;
+    const int pairs[kStages][2] = {{EV_BEGIN, EV_EVENTS_COUNT}, {EV_EVENTS_COUNT, EV_COMPACT}, {EV_COMPACT, EV_EDGES},
+                                   {EV_EDGES, EV_RECORD_COUNT}, {EV_FINISH, EV_EVENTS_FILL}, {EV_EVENTS_FILL, EV_RECORD_FILL},
+                                   {EV_RECORD_FILL, EV_CONSUME}, {EV_CONSUME, EV_CONSTRAINED}};
+    if (cudaEventSynchronize(ctx->ev[EV_CONSTRAINED]) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return -OVX_FDG_CUDA_ERROR;
+    }
+    int n = 0;
+    for (int i = 0; i < kStages && i < capacity; ++i, ++n)
+    {
+        float t = -1.0f;
+        if (cudaEventElapsedTime(&t, ctx->ev[pairs[i][0]], ctx->ev[pairs[i][1]]) != cudaSuccess)
+        {
+            cudaGetLastError();
+            t = -1.0f;
+        }
+        ms[i] = t;
+    }
+    return n;
+}
+
+const char *ovx_fdg_stage_name(int i)
+{
+    return (i >= 0 && i < kStages) ? kStageNames[i] : "";
+}
+
+int64_t ovx_fdg_kernel_launches(const ovx_fdg_context *ctx)
+{
+    return ctx ? (int64_t)ctx->launches : 0;
 }
 
 const char *ovx_fdg_status_string(int status)
@@ -1751,19 +1848,20 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONSTRAINED, 0, 4, st));
 
+    stage(ctx, EV_FINISH, st);
     GenArgs A = make_gen(ctx);
     A.qtab = nullptr;
     if (ctx->fbytes == 8)
-    {
         launch_events<FILL, long long>(ctx, A, st);
-        launch_faces_boundary<FILL, long long>(ctx, A, st);
-    }
     else
-    {
         launch_events<FILL, int>(ctx, A, st);
+    stage(ctx, EV_EVENTS_FILL, st);
+    if (ctx->fbytes == 8)
+        launch_faces_boundary<FILL, long long>(ctx, A, st);
+    else
         launch_faces_boundary<FILL, int>(ctx, A, st);
-    }
     OVX_CUDA(cudaGetLastError());
+    stage(ctx, EV_RECORD_FILL, st);
 
     SolveArgs SA{};
     SA.m = make_mesh(ctx);
@@ -1782,9 +1880,15 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.clist = (float *)ctx->clist.p;
     SA.clist_cap = (uint32_t)(n + 1);
     if (ctx->n_active > 0)
+    {
         brick_consume<<<(unsigned)ctx->n_active, kConsumeThreads, 0, st>>>(SA);
+        ++ctx->launches;
+    }
+    stage(ctx, EV_CONSUME, st);
     constrained_solve<<<ctx->sms * 8, 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
                                                     ctx->g, dual_vertices);
+    ++ctx->launches;
+    stage(ctx, EV_CONSTRAINED, st);
     OVX_CUDA(cudaGetLastError());
     OVX_CUDA(cudaMemcpyAsync(&ctx->host[8], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
     ctx->finished = 1;
@@ -1854,6 +1958,7 @@ int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_
     OVX_CUDA(cudaSetDevice(ctx->device));
     brick_coords<<<(unsigned)ctx->n_active, 128, 0, st>>>((const uint32_t *)ctx->bits.p, (const unsigned long long *)ctx->bbase.p,
                                                           (const uint32_t *)ctx->active.p, ctx->g, voxel_indices);
+    ++ctx->launches;
     OVX_CUDA(cudaGetLastError());
     return OVX_FDG_OK;
 }

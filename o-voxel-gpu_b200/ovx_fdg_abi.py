@@ -27,6 +27,10 @@ PROTOTYPES = [
     ("ovx_fdg_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("ovx_fdg_last_error", ctypes.c_char_p, [_P]),
     ("ovx_fdg_workspace_bytes", _I64, [_P]),
+    ("ovx_fdg_set_profiling", ctypes.c_int, [_P, ctypes.c_int]),
+    ("ovx_fdg_stage_times", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    ("ovx_fdg_stage_name", ctypes.c_char_p, [ctypes.c_int]),
+    ("ovx_fdg_kernel_launches", _I64, [_P]),
     ("ovx_fdg_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.c_int32, _I64, _P, _P, _F, _F, _F, ctypes.POINTER(_I64)]),
     ("ovx_fdg_finish", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("ovx_fdg_sync_status", ctypes.c_int, [_P, _P]),
@@ -46,7 +50,7 @@ def lib():
     global _LIB
     if _LIB is None:
         if not os.path.exists(LIB_PATH):
-            raise RuntimeError(f"libovx_fdg.so is not built ({LIB_PATH}); run o-voxel-gpu_b200/build.py")
+            raise RuntimeError(f"libovx_fdg.so is not built ({LIB_PATH}); run o-voxel-gpu_b200/ovx_build.py")
         _LIB = ctypes.CDLL(LIB_PATH)
         for name, res, args in PROTOTYPES:
             fn = getattr(_LIB, name)
@@ -100,6 +104,20 @@ class Context:
 
     def workspace_bytes(self) -> int:
         return int(self._lib.ovx_fdg_workspace_bytes(self.handle))
+
+    def set_profiling(self, enable: bool = True):
+        self._check(self._lib.ovx_fdg_set_profiling(self.handle, 1 if enable else 0), "ovx_fdg_set_profiling")
+
+    def stage_times(self) -> dict:
+        """Stage durations (ms) of the last conversion; waits for it."""
+        buf = (ctypes.c_float * 16)()
+        n = self._lib.ovx_fdg_stage_times(self.handle, buf, 16)
+        if n < 0:
+            raise FdgError(-n, "ovx_fdg_stage_times")
+        return {self._lib.ovx_fdg_stage_name(i).decode(): float(buf[i]) for i in range(n)}
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.ovx_fdg_kernel_launches(self.handle))
 
     def mesh_to_fdg(self, vertices, faces, origin, voxel_size, grid_range, fw, bw, rw, stream=None, check=True):
         """vertices: CUDA float32 [V,3]; faces: CUDA int32/int64 [F,3]; returns torch tensors."""
