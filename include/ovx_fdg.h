@@ -129,6 +129,31 @@ int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *tri
                             const ovx_fdg_grid *grid, int64_t *num_voxels);
 int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices);
 
+/*
+ * Occupancy without any allocation (no counterpart in the reference; its
+ * operators always allocate).  For hosts that cannot let a library allocate
+ * device memory: an application that hands all device memory to its own pool
+ * at start-up, or a plugin host whose allocator owns the device, and callers
+ * on a latency-critical thread that must not run into the device-wide
+ * synchronisation cudaMalloc/cudaFree can imply.  It calls no cudaMalloc,
+ * cudaFree or allocating library routine: its scratch is one fixed device
+ * array inside the library (about 2.2 MiB, held on every device that loads the
+ * library until the process exits), sized for grids of at most 32768 8x8x8
+ * bricks (for example 256^3).  Larger grids return OVX_FDG_CAPACITY.
+ *
+ * Same semantics and output row order as ovx_fdg_occupancy_begin/finish:
+ * triangles float32 [num_triangles,3,3] in grid-local coordinates on the
+ * calling thread's current device; voxel_indices has room for `capacity` rows.
+ * *num_voxels receives N; if N > capacity nothing is written and
+ * OVX_FDG_CAPACITY is returned.  The call waits once on `stream` (to read N)
+ * and returns with the coordinate kernel enqueued on it.  The first call on a
+ * device looks up the scratch address there (it should come before any stream
+ * capture).  All calls on a device share the scratch array, so calls that
+ * overlap on the GPU (different streams or threads) race; serialise them.
+ */
+int ovx_fdg_occupancy_noalloc(void *stream, const float *triangles, int64_t num_triangles, const ovx_fdg_grid *grid,
+                              int32_t *voxel_indices, int64_t capacity, int64_t *num_voxels);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,7 @@
 
 #include <climits>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 
@@ -1272,6 +1273,133 @@ __global__ void __launch_bounds__(128) brick_coords(const uint32_t *__restrict__
     }
 }
 
+// ===========================================================================
+// allocation-free occupancy (ovx_fdg_occupancy_noalloc)
+// ===========================================================================
+// All scratch of this entry point lives in one file-scope device array: the
+// occupancy bitmap of up to kNoallocMaxBricks bricks, then one 32-bit row base
+// per brick plus the total.  Every call shares it; each call clears the bitmap
+// it uses before marking.
+constexpr long long kNoallocMaxBricks = 32768; // e.g. a 256^3 grid
+constexpr size_t kNoallocBitsBytes = (size_t)kNoallocMaxBricks * kWordsPerBrick * 4;
+constexpr size_t kNoallocBytes = kNoallocBitsBytes + (size_t)(kNoallocMaxBricks + 1) * 4;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+__global__ void noalloc_clear(uint32_t *__restrict__ bits, long long words)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (long long)gridDim.x * blockDim.x)
+        bits[i] = 0u;
+}
+
+// Scanline occupancy of a triangle soup, one thread per (triangle, axis), every row inline.
+__global__ void __launch_bounds__(kThreads) noalloc_mark(const float *__restrict__ tris, long long nt, Grid g, uint32_t *bits)
+{
+    const long long ta = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ta >= 3 * nt)
+        return;
+    const long long t = ta / 3;
+    const int ax2 = (int)(ta - 3 * t);
+    float v[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            v[k][c] = tris[t * 9 + k * 3 + c];
+    AxisScan s;
+    axis_setup(v, ax2, g, s);
+    auto sink = [&](int xi, int yi, int zi, float, float, double) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+            int x, y, z;
+            place(ax2, xi + (k >> 1), yi + (k & 1), zi, x, y, z);
+            uint32_t bit;
+            const long long w = voxel_word(g, x, y, z, bit);
+            atomicOr(&bits[w], 1u << bit);
+        }
+    };
+#pragma unroll 1
+    for (int yi = s.start; yi < s.end; ++yi)
+        scan_row(s, yi, INT_MIN, INT_MAX, g, sink);
+}
+
+// One CTA: popcount per brick and exclusive scan into row bases; base[nb] = total.
+__global__ void __launch_bounds__(1024) noalloc_scan(const uint32_t *__restrict__ bits, long long nb, uint32_t *__restrict__ base)
+{
+    __shared__ uint32_t warp_sum[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long per = (nb + blockDim.x - 1) / blockDim.x;
+    const long long b0 = (long long)tid * per;
+    const long long b1 = b0 + per < nb ? b0 + per : nb;
+    uint32_t local = 0;
+    for (long long b = b0; b < b1; ++b)
+        for (int w = 0; w < kWordsPerBrick; ++w)
+            local += __popc(bits[b * kWordsPerBrick + w]);
+    uint32_t incl = local;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d)
+            incl += y;
+    }
+    if (lane == 31)
+        warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0)
+    {
+        uint32_t ws = lane < (int)(blockDim.x >> 5) ? warp_sum[lane] : 0u;
+        uint32_t wi = ws;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wi, d);
+            if (lane >= d)
+                wi += y;
+        }
+        if (lane < (int)(blockDim.x >> 5))
+            warp_sum[lane] = wi - ws;
+        if (lane == (int)(blockDim.x >> 5) - 1)
+            base[nb] = wi;
+    }
+    __syncthreads();
+    uint32_t run = warp_sum[warp] + incl - local;
+    for (long long b = b0; b < b1; ++b)
+    {
+        base[b] = run;
+        for (int w = 0; w < kWordsPerBrick; ++w)
+            run += __popc(bits[b * kWordsPerBrick + w]);
+    }
+}
+
+// One thread per occupancy word: coordinates of its voxels at their rows (brick order).
+__global__ void noalloc_emit(const uint32_t *__restrict__ bits, const uint32_t *__restrict__ base, Grid g, int32_t *__restrict__ vox)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.nbricks * kWordsPerBrick)
+        return;
+    uint32_t word = bits[i];
+    if (!word)
+        return;
+    const long long b = i / kWordsPerBrick;
+    const int w = (int)(i - b * kWordsPerBrick);
+    uint32_t row = base[b];
+    for (int k = 0; k < w; ++k)
+        row += __popc(bits[b * kWordsPerBrick + k]);
+    int o[3];
+    brick_origin(g, b, o);
+    while (word)
+    {
+        const int bt = __ffs(word) - 1;
+        word &= word - 1u;
+        const int lv = w * 32 + bt;
+        vox[(long long)row * 3 + 0] = o[0] + (lv & 7);
+        vox[(long long)row * 3 + 1] = o[1] + ((lv >> 3) & 7);
+        vox[(long long)row * 3 + 2] = o[2] + (lv >> 6);
+        ++row;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -1964,3 +2092,98 @@ int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// allocation-free occupancy: host side
+// ---------------------------------------------------------------------------
+namespace
+{
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once per
+// device (the name itself is a host-side stand-in, not a device address).
+cudaError_t noalloc_scratch(int device, void **out)
+{
+    if (device < 0 || device >= kNoallocMaxDevices)
+        return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device])
+    {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return e;
+        g_noalloc_ptr[device] = p;
+    }
+    *out = g_noalloc_ptr[device];
+    return cudaSuccess;
+}
+} // namespace
+
+extern "C" int ovx_fdg_occupancy_noalloc(void *stream, const float *triangles, int64_t num_triangles, const ovx_fdg_grid *grid,
+                                         int32_t *voxel_indices, int64_t capacity, int64_t *num_voxels)
+{
+    if (!num_voxels || !grid || num_triangles < 0 || capacity < 0 || (num_triangles > 0 && !triangles) ||
+        (capacity > 0 && !voxel_indices))
+        return OVX_FDG_INVALID_ARGUMENT;
+    *num_voxels = 0;
+    if (num_triangles >= (1ll << 30))
+        return OVX_FDG_CAPACITY;
+    Grid g{};
+    long long nb = 1;
+    for (int a = 0; a < 3; ++a)
+    {
+        const float vs = grid->voxel_size[a];
+        if (!(vs > 0.0f) || !(vs < 3.0e38f))
+            return OVX_FDG_INVALID_ARGUMENT;
+        const long long sz = (long long)grid->grid_max[a] - (long long)grid->grid_min[a];
+        if (sz < 1 || sz > (1 << 20))
+            return OVX_FDG_INVALID_ARGUMENT;
+        g.vs[a] = vs;
+        g.rv[a] = 1.0 / (double)vs;
+        g.gmin[a] = grid->grid_min[a];
+        g.gmax[a] = grid->grid_max[a];
+        g.size[a] = (int)sz;
+        g.nb[a] = (int)((sz + kBrick - 1) / kBrick);
+        nb *= g.nb[a];
+    }
+    if (nb > kNoallocMaxBricks)
+        return OVX_FDG_CAPACITY; // grid larger than the fixed scratch covers
+    g.nbricks = nb;
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return OVX_FDG_CUDA_ERROR;
+    }
+    void *scratch = nullptr;
+    if (noalloc_scratch(device, &scratch) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return OVX_FDG_CUDA_ERROR;
+    }
+    uint32_t *bits = (uint32_t *)scratch;
+    uint32_t *base = (uint32_t *)((unsigned char *)scratch + kNoallocBitsBytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    noalloc_clear<<<256, 256, 0, st>>>(bits, nb * kWordsPerBrick);
+    if (num_triangles > 0)
+        noalloc_mark<<<blocks_for(3 * num_triangles, kThreads), kThreads, 0, st>>>(triangles, num_triangles, g, bits);
+    noalloc_scan<<<1, 1024, 0, st>>>(bits, nb, base);
+    uint32_t total = 0;
+    if (cudaGetLastError() != cudaSuccess || cudaMemcpyAsync(&total, base + nb, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return OVX_FDG_CUDA_ERROR;
+    }
+    *num_voxels = (int64_t)total;
+    if ((int64_t)total > capacity)
+        return OVX_FDG_CAPACITY; // output buffer too small; *num_voxels says how many rows are needed
+    if (total > 0)
+        noalloc_emit<<<blocks_for(nb * kWordsPerBrick, kThreads), kThreads, 0, st>>>(bits, base, g, voxel_indices);
+    if (cudaGetLastError() != cudaSuccess)
+        return OVX_FDG_CUDA_ERROR;
+    return OVX_FDG_OK;
+}

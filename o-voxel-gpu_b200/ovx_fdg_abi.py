@@ -36,6 +36,7 @@ PROTOTYPES = [
     ("ovx_fdg_sync_status", ctypes.c_int, [_P, _P]),
     ("ovx_fdg_occupancy_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.POINTER(_I64)]),
     ("ovx_fdg_occupancy_finish", ctypes.c_int, [_P, _P, _P]),
+    ("ovx_fdg_occupancy_noalloc", ctypes.c_int, [_P, _P, _I64, _P, _P, _I64, ctypes.POINTER(_I64)]),
 ]
 
 
@@ -156,3 +157,22 @@ class Context:
         rc = self._lib.ovx_fdg_occupancy_finish(self.handle, st, ctypes.c_void_p(vox.data_ptr() if vox.numel() else 0))
         self._check(rc, "ovx_fdg_occupancy_finish")
         return vox
+
+
+def occupancy_noalloc(triangles, voxel_size, grid_range, capacity=None, stream=None):
+    """Allocation-free occupancy (ovx_fdg_occupancy_noalloc): the library uses
+    only its fixed internal scratch; the output buffer is allocated here by
+    torch on behalf of the caller.  Returns (status, N, voxels[:N])."""
+    import torch
+
+    dev = triangles.device
+    st = ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream)
+    grid = make_grid(voxel_size, grid_range)
+    if capacity is None:
+        capacity = 4 * 1024 * 1024
+    out = torch.empty((max(capacity, 1), 3), dtype=torch.int32, device=dev)
+    n = ctypes.c_int64(0)
+    rc = lib().ovx_fdg_occupancy_noalloc(st, ctypes.c_void_p(triangles.data_ptr() if triangles.numel() else 0),
+                                         triangles.shape[0], ctypes.byref(grid), ctypes.c_void_p(out.data_ptr()),
+                                         capacity, ctypes.byref(n))
+    return rc, n.value, out[: min(n.value, capacity)]
