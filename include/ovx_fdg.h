@@ -27,8 +27,8 @@
  *
  * Two calls per conversion: `begin` runs the occupancy stage and returns the
  * number of voxel rows N (one stream synchronisation); the caller then
- * provides output buffers with N rows and `finish` runs the quadric and solve
- * stages (one more stream synchronisation, for the quadric entry count).  A
+ * provides output buffers with N rows and `finish` enqueues the quadric and
+ * solve stages on the stream and returns without synchronising.  A
  * context holds its device workspace and the state between the two calls; it
  * is not safe to use one context from two threads at once.
  */
@@ -86,6 +86,11 @@ int ovx_fdg_set_profiling(ovx_fdg_context *ctx, int enable);
 int ovx_fdg_stage_times(ovx_fdg_context *ctx, float *ms, int capacity);
 const char *ovx_fdg_stage_name(int stage);
 int64_t ovx_fdg_kernel_launches(const ovx_fdg_context *ctx);
+/* Sizes of the last conversion, known after ovx_fdg_begin: out[0] voxel rows,
+ * out[1] occupied 8^3 bricks, out[2] quadric records bucketed by brick,
+ * out[3] boundary edges, out[4] bricks of the grid.  Writes min(capacity, 5)
+ * values and returns how many it wrote (negative status on error). */
+int ovx_fdg_last_counts(const ovx_fdg_context *ctx, int64_t *out, int capacity);
 
 /*
  * Occupancy stage of mesh -> flexible dual grid.
@@ -107,7 +112,7 @@ int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int
  * Quadric + solve stages.  Output device buffers with room for N rows:
  *   voxel_indices int32 [N,3], dual_vertices float32 [N,3] (grid-local frame,
  *   like the reference), intersected uint8 [N,3] (0/1, torch.bool layout).
- * Work is enqueued on `stream`; the function synchronises once on it.
+ * Work is enqueued on `stream`; the function returns without synchronising.
  */
 int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, float *dual_vertices,
                    uint8_t *intersected);

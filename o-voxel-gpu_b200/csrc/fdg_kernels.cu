@@ -1871,6 +1871,17 @@ int64_t ovx_fdg_kernel_launches(const ovx_fdg_context *ctx)
     return ctx ? (int64_t)ctx->launches : 0;
 }
 
+int ovx_fdg_last_counts(const ovx_fdg_context *ctx, int64_t *out, int capacity)
+{
+    if (!ctx || (!out && capacity > 0) || capacity < 0)
+        return -OVX_FDG_INVALID_ARGUMENT;
+    const int64_t v[5] = {ctx->n_vox, ctx->n_active, ctx->n_rec, ctx->n_boundary, ctx->g.nbricks};
+    const int n = capacity < 5 ? capacity : 5;
+    for (int i = 0; i < n; ++i)
+        out[i] = v[i];
+    return n;
+}
+
 const char *ovx_fdg_status_string(int status)
 {
     switch (status)

@@ -31,6 +31,7 @@ PROTOTYPES = [
     ("ovx_fdg_stage_times", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     ("ovx_fdg_stage_name", ctypes.c_char_p, [ctypes.c_int]),
     ("ovx_fdg_kernel_launches", _I64, [_P]),
+    ("ovx_fdg_last_counts", ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.c_int]),
     ("ovx_fdg_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.c_int32, _I64, _P, _P, _F, _F, _F, ctypes.POINTER(_I64)]),
     ("ovx_fdg_finish", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("ovx_fdg_sync_status", ctypes.c_int, [_P, _P]),
@@ -119,6 +120,15 @@ class Context:
 
     def kernel_launches(self) -> int:
         return int(self._lib.ovx_fdg_kernel_launches(self.handle))
+
+    def last_counts(self) -> dict:
+        """Sizes of the last conversion (voxels, occupied bricks, records, boundary edges, grid bricks)."""
+        buf = (_I64 * 5)()
+        n = self._lib.ovx_fdg_last_counts(self.handle, buf, 5)
+        if n < 0:
+            raise FdgError(-n, "ovx_fdg_last_counts")
+        names = ("voxels", "bricks_occupied", "records", "boundary_edges", "bricks_grid")
+        return {names[i]: int(buf[i]) for i in range(n)}
 
     def mesh_to_fdg(self, vertices, faces, origin, voxel_size, grid_range, fw, bw, rw, stream=None, check=True):
         """vertices: CUDA float32 [V,3]; faces: CUDA int32/int64 [F,3]; returns torch tensors."""
