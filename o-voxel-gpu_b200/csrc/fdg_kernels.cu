@@ -17,8 +17,10 @@
 //                      the event's base voxel in projection coordinates,
 //                      relative to the brick (u,v offset by one)
 //             face     {t, 1<<30 | local voxel, 0}
-//             boundary {v_min, 2<<30 | local voxel, v_max}
+//             boundary {e, 2<<30 | local voxel, 0}, e = index in the
+//                      boundary edge list, which is sorted by (v_min, v_max)
 //   qtab    plane quadric per triangle (10 floats)
+//   btab    line quadric per boundary edge (10 floats)
 //
 // begin (ends with the one host synchronisation of a conversion):
 //   tri_events<COUNT>   one thread per (triangle, axis): scanline events (FP64,
@@ -41,7 +43,7 @@
 // order, flexible_dual_grid.cpp:173-283, :298-414, :741-757):
 //   intersection  (0<<62) | ((t*3 + axis)*4 + (1-dy)*2 + (1-dx))
 //   face          (1<<62) | t
-//   boundary      (2<<62) | (v_min<<31) | v_max
+//   boundary      (2<<62) | e   (edge list index; the list is in (v_min, v_max) order)
 #include "ovx_fdg.h"
 #include "fdg_device.cuh"
 
@@ -64,7 +66,10 @@ constexpr int kInlineFaceBricks = 64; // face boxes over more bricks go to the C
 constexpr int kChunk = 8;             // columns per tile for large (triangle, axis) pairs
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
-constexpr int kWindow = 2048;   // per-voxel contributions held in shared memory per pass of a brick
+#ifndef OVX_FDG_CONSUME_WINDOW
+#define OVX_FDG_CONSUME_WINDOW 2048
+#endif
+constexpr int kWindow = OVX_FDG_CONSUME_WINDOW; // per-voxel contributions held in shared memory per pass of a brick
 constexpr int kThreadSort = 48; // lists longer than this are ranked by the whole CTA
 
 // device counter words
@@ -152,6 +157,7 @@ struct GenArgs
     const unsigned long long *roff; // FILL
     Rec *rec;                       // FILL
     float *qtab;                    // COUNT of the intersection pass
+    float *btab;                    // FILL of the boundary pass
     uint32_t *counters;
     uint32_t *scan_large;
     uint32_t scan_large_cap;
@@ -543,7 +549,7 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
         vertex_load(A.m, ia, v0);
         vertex_load(A.m, ib, v1);
         Dda d;
-        if (!boundary_setup(v0, v1, g, d, nullptr))
+        if (!boundary_setup(v0, v1, g, d, M == FILL ? A.btab + (size_t)i * 10 : nullptr))
             continue;
         for (;;)
         {
@@ -552,7 +558,7 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
                 uint32_t bit;
                 const long long w = voxel_word(g, d.cur[0], d.cur[1], d.cur[2], bit);
                 if (A.bits[w] & (1u << bit))
-                    put_record<M>(A, w >> 4, ia, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), ib);
+                    put_record<M>(A, w >> 4, i, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), 0u);
             }
             if (!dda_step(d))
                 break;
@@ -664,37 +670,22 @@ __device__ void heap_sift(uint32_t *a, long long start, long long end)
     }
 }
 
-__device__ __forceinline__ void push_boundary(unsigned long long *bkeys, uint32_t cap, uint32_t *counters, uint32_t a, uint32_t b)
+// Sorts vertex a's list of larger endpoints (insertion sort for the usual
+// short lists, heap sort beyond 32 entries).
+__device__ void sort_list(uint32_t *l, long long n)
 {
-    const uint32_t slot = atomicAdd(&counters[C_BOUNDARY], 1u);
-    if (slot < cap)
-        bkeys[slot] = ((unsigned long long)a << 32) | b;
-    else
-        atomicOr(&counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
-}
-
-// Per vertex a: the larger endpoints of edges whose smaller endpoint is a;
-// those occurring once are boundary edges (reference: std::map count == 1).
-__global__ void edge_find(const unsigned long long *__restrict__ voff, uint32_t *__restrict__ emax, long long nv,
-                          unsigned long long *__restrict__ bkeys, uint32_t cap, uint32_t *__restrict__ counters)
-{
-    const long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= nv)
-        return;
-    const unsigned long long s = voff[a], e = voff[a + 1];
-    const long long n = (long long)(e - s);
-    if (n == 0)
-        return;
-    uint32_t *l = emax + s;
     if (n <= 32)
     {
-        for (long long i = 0; i < n; ++i)
+        for (long long i = 1; i < n; ++i)
         {
-            int c = 0;
-            for (long long j = 0; j < n; ++j)
-                c += (l[j] == l[i]);
-            if (c == 1)
-                push_boundary(bkeys, cap, counters, (uint32_t)a, l[i]);
+            const uint32_t x = l[i];
+            long long j = i;
+            while (j > 0 && l[j - 1] > x)
+            {
+                l[j] = l[j - 1];
+                --j;
+            }
+            l[j] = x;
         }
         return;
     }
@@ -707,13 +698,52 @@ __global__ void edge_find(const unsigned long long *__restrict__ voff, uint32_t 
         l[end] = t;
         heap_sift(l, 0, end);
     }
+}
+
+// Per vertex a: sort the larger endpoints of the edges whose smaller endpoint
+// is a and count those occurring once -- the boundary edges (a, b) (reference:
+// std::map count == 1, flexible_dual_grid.cpp:741-757).
+__global__ void edge_sort_count(const unsigned long long *__restrict__ voff, uint32_t *__restrict__ emax, long long nv,
+                                uint32_t *__restrict__ bcnt)
+{
+    const long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nv)
+        return;
+    const unsigned long long s = voff[a], e = voff[a + 1];
+    const long long n = (long long)(e - s);
+    uint32_t *l = emax + s;
+    sort_list(l, n);
+    uint32_t c = 0;
+    for (long long i = 0; i < n;)
+    {
+        long long j = i;
+        while (j < n && l[j] == l[i])
+            ++j;
+        c += (j - i == 1);
+        i = j;
+    }
+    bcnt[a] = c;
+}
+
+// Per vertex a: its boundary edges at their rank in (a, b) order, so the
+// boundary list is sorted like the reference's std::map.
+__global__ void edge_emit(const unsigned long long *__restrict__ voff, const uint32_t *__restrict__ emax, long long nv,
+                          const unsigned long long *__restrict__ boff, unsigned long long *__restrict__ bkeys)
+{
+    const long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nv)
+        return;
+    const unsigned long long s = voff[a], e = voff[a + 1];
+    const long long n = (long long)(e - s);
+    const uint32_t *l = emax + s;
+    unsigned long long k = boff[a];
     for (long long i = 0; i < n;)
     {
         long long j = i;
         while (j < n && l[j] == l[i])
             ++j;
         if (j - i == 1)
-            push_boundary(bkeys, cap, counters, (uint32_t)a, l[i]);
+            bkeys[k++] = ((unsigned long long)a << 32) | l[i];
         i = j;
     }
 }
@@ -731,10 +761,12 @@ struct SolveArgs
     const unsigned long long *roff;
     const Rec *rec;
     const float *qtab;
+    const float *btab;
     int32_t *vox;
     float *dual;
     uint8_t *flags;
     uint32_t *counters;
+    float4 *vacc; // per-voxel accumulated state, 4 float4 per output row
     float *clist; // deferred constrained searches, 16 words each
     uint32_t clist_cap;
 };
@@ -788,7 +820,7 @@ __device__ __forceinline__ void expand(const BrickShared &S, const Rec &r, Sink 
     else if (kind == 1)
         sink(dense_index(S, (int)(r.b & 511u)), kKeyFace | (unsigned long long)r.a, 0u);
     else
-        sink(dense_index(S, (int)(r.b & 511u)), kKeyBoundary | ((unsigned long long)r.a << 31) | (unsigned long long)r.c, 0u);
+        sink(dense_index(S, (int)(r.b & 511u)), kKeyBoundary | (unsigned long long)r.a, 0u);
 }
 
 struct CountSink
@@ -898,29 +930,46 @@ __device__ __forceinline__ void acc_entry(const SolveArgs &A, const int vc[3], u
     }
     else
     {
-        float v0[3], v1[3];
-        vertex_load(A.m, (long long)((key >> 31) & 0x7fffffffull), v0);
-        vertex_load(A.m, (long long)(key & 0x7fffffffull), v1);
-        Dda d;
-        if (boundary_setup(v0, v1, A.m.g, d, qt))
-        {
+        // line quadric of boundary edge e, computed once by the boundary pass
+        const float *bq = A.btab + (size_t)(key & 0xffffffffull) * 10;
 #pragma unroll
-            for (int i = 0; i < 10; ++i)
-                a.q[i] = a.q[i] + A.bw * qt[i];
-        }
+        for (int i = 0; i < 10; ++i)
+            a.q[i] = a.q[i] + A.bw * bq[i];
     }
 }
 
-// Regularise and solve; voxels whose unconstrained solution leaves the box go to the constrained-search list.
-__device__ __forceinline__ void finish_voxel(const SolveArgs &A, long long row, const int vc[3], const Acc &a)
+// Accumulated state of one voxel -> its row of the voxel state array
+// (quadric, mass sum, count, flag bits: 16 words, 64-byte aligned).
+__device__ __forceinline__ void store_acc(const SolveArgs &A, long long row, const Acc &a)
 {
+    float4 *d = A.vacc + row * 4;
+    d[0] = make_float4(a.q[0], a.q[1], a.q[2], a.q[3]);
+    d[1] = make_float4(a.q[4], a.q[5], a.q[6], a.q[7]);
+    d[2] = make_float4(a.q[8], a.q[9], a.mean[0], a.mean[1]);
+    d[3] = make_float4(a.mean[2], a.cnt, __uint_as_float(a.flags), 0.0f);
+}
+
+// One thread per voxel row: regularise and solve (flexible_dual_grid.cpp:763-797);
+// voxels whose unconstrained solution leaves the box go to the constrained-search list.
+__global__ void __launch_bounds__(128) voxel_solve(SolveArgs A, long long n)
+{
+    const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n)
+        return;
+    const float4 *s = A.vacc + row * 4;
+    const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
+    const float qa[10] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w, s2.x, s2.y};
+    const float mean[3] = {s2.z, s2.w, s3.x};
+    const float cnt = s3.y;
+    const uint32_t flags = __float_as_uint(s3.z);
+    const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
     float q[10];
-    regularize(a.q, a.mean, a.cnt, A.rw, q);
+    regularize(qa, mean, cnt, A.rw, q);
     float v[3];
     const bool inside = solve_unconstrained(vc, A.m.g, q, v);
-    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
-    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
-    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
+    A.flags[row * 3 + 0] = (uint8_t)(flags & 1u);
+    A.flags[row * 3 + 1] = (uint8_t)((flags >> 1) & 1u);
+    A.flags[row * 3 + 2] = (uint8_t)((flags >> 2) & 1u);
     if (inside)
     {
         A.dual[row * 3 + 0] = v[0];
@@ -1026,7 +1075,7 @@ __device__ __noinline__ void select_voxel(const SolveArgs &A, const BrickShared 
         acc_entry(A, vc, sel.best, sel.pay, a);
         last = sel.best;
     }
-    finish_voxel(A, row, vc, a);
+    store_acc(A, row, a);
 }
 
 __global__ void __launch_bounds__(kConsumeThreads, 8) brick_consume(SolveArgs A)
@@ -1200,7 +1249,7 @@ __global__ void __launch_bounds__(kConsumeThreads, 8) brick_consume(SolveArgs A)
                 const uint32_t j = s0 + S.perm[s0 + x];
                 acc_entry(A, vc, S.key[j], S.pay[j], a);
             }
-            finish_voxel(A, (long long)(vbase + i), vc, a);
+            store_acc(A, (long long)(vbase + i), a);
         }
         __syncthreads();
         lo = whi;
@@ -1415,12 +1464,14 @@ enum
     EV_EVENTS_FILL,
     EV_RECORD_FILL,
     EV_CONSUME,
+    EV_SOLVE,
     EV_CONSTRAINED,
     kStageEvents
 };
 const char *const kStageNames[] = {"scanline_mark_count", "compaction", "boundary_edges", "face_boundary_count",
-                                   "scanline_fill", "face_boundary_fill", "brick_consume", "constrained_solve"};
-constexpr int kStages = 8;
+                                   "scanline_fill", "face_boundary_fill", "brick_consume", "voxel_solve",
+                                   "constrained_solve"};
+constexpr int kStages = 9;
 
 struct Buf
 {
@@ -1435,8 +1486,8 @@ struct ovx_fdg_context
     int device = 0;
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
-    Buf vcnt, voff, emax, bkeys;
-    Buf rcnt, roff, rec, clist, cub_tmp;
+    Buf vcnt, voff, emax, bkeys, boff, btab;
+    Buf rcnt, roff, rec, clist, cub_tmp, vacc;
     unsigned long long *host = nullptr; // pinned readback words
     std::string err;
     // state between begin and finish
@@ -1463,8 +1514,8 @@ template <typename Ctx>
 int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
-                &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp};
+                &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
+                &c->clist, &c->cub_tmp, &c->vacc};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
@@ -1613,6 +1664,7 @@ GenArgs make_gen(ovx_fdg_context *ctx)
     A.roff = (const unsigned long long *)ctx->roff.p;
     A.rec = (Rec *)ctx->rec.p;
     A.qtab = (float *)ctx->qtab.p;
+    A.btab = (float *)ctx->btab.p;
     A.counters = (uint32_t *)ctx->counters.p;
     A.scan_large = (uint32_t *)ctx->scan_large.p;
     A.scan_large_cap = cap_u32(ctx->scan_large, 4);
@@ -1677,6 +1729,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         OVX_CUDA(ensure(ctx->voff, (size_t)(ctx->nv + 1) * 8));
         OVX_CUDA(ensure(ctx->emax, (size_t)(3 * nf + 1) * 4));
         OVX_CUDA(ensure(ctx->bkeys, (size_t)(3 * nf + 1) * 8));
+        OVX_CUDA(ensure(ctx->boff, (size_t)(ctx->nv + 1) * 8));
     }
     OVX_CUDA(cudaMemsetAsync(ctx->bits.p, 0, (size_t)nb * kWordsPerBrick * 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->counters.p, 0, C_WORDS * 4, st));
@@ -1724,10 +1777,16 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
             edge_fill<int><<<blocks_for(nf, kThreads), kThreads, 0, st>>>((const int *)ctx->faces, nf, ctx->nv, voff, vcnt,
                                                                          (uint32_t *)ctx->emax.p);
         OVX_CUDA(cudaGetLastError());
-        edge_find<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (uint32_t *)ctx->emax.p, ctx->nv,
-                                                                     (unsigned long long *)ctx->bkeys.p, cap_u32(ctx->bkeys, 8),
-                                                                     (uint32_t *)ctx->counters.p);
-        ctx->launches += 3;
+        // edge_fill left vcnt all zero: reuse it for the per-vertex boundary counts
+        edge_sort_count<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (uint32_t *)ctx->emax.p, ctx->nv, vcnt);
+        OVX_CUDA(cudaGetLastError());
+        unsigned long long *boff = (unsigned long long *)ctx->boff.p;
+        OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, boff, ctx->nv + 1, st));
+        edge_emit<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (const uint32_t *)ctx->emax.p, ctx->nv, boff,
+                                                                     (unsigned long long *)ctx->bkeys.p);
+        // boundary edge count -> counters[C_BOUNDARY] (low word of the u64 total; at most 3F < 2^32)
+        OVX_CUDA(cudaMemcpyAsync((uint32_t *)ctx->counters.p + C_BOUNDARY, boff + ctx->nv, 4, cudaMemcpyDeviceToDevice, st));
+        ctx->launches += 4;
         OVX_CUDA(cudaGetLastError());
     }
     stage(ctx, EV_EDGES, st);
@@ -1841,7 +1900,7 @@ int ovx_fdg_stage_times(ovx_fdg_context *ctx, float *ms, int capacity)
         return 0;
     const int pairs[kStages][2] = {{EV_BEGIN, EV_EVENTS_COUNT}, {EV_EVENTS_COUNT, EV_COMPACT}, {EV_COMPACT, EV_EDGES},
                                    {EV_EDGES, EV_RECORD_COUNT}, {EV_FINISH, EV_EVENTS_FILL}, {EV_EVENTS_FILL, EV_RECORD_FILL},
-                                   {EV_RECORD_FILL, EV_CONSUME}, {EV_CONSUME, EV_CONSTRAINED}};
+                                   {EV_RECORD_FILL, EV_CONSUME}, {EV_CONSUME, EV_SOLVE}, {EV_SOLVE, EV_CONSTRAINED}};
     if (cudaEventSynchronize(ctx->ev[EV_CONSTRAINED]) != cudaSuccess)
     {
         cudaGetLastError();
@@ -1983,7 +2042,9 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(cudaSetDevice(ctx->device));
     const long long nb = ctx->g.nbricks;
     OVX_CUDA(ensure(ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
+    OVX_CUDA(ensure(ctx->btab, (size_t)(ctx->n_boundary + 1) * 40));
     OVX_CUDA(ensure(ctx->clist, (size_t)(n + 1) * 16 * 4));
+    OVX_CUDA(ensure(ctx->vacc, (size_t)n * 64));
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONSTRAINED, 0, 4, st));
 
@@ -2012,11 +2073,13 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.roff = (const unsigned long long *)ctx->roff.p;
     SA.rec = (const Rec *)ctx->rec.p;
     SA.qtab = (const float *)ctx->qtab.p;
+    SA.btab = (const float *)ctx->btab.p;
     SA.vox = voxel_indices;
     SA.dual = dual_vertices;
     SA.flags = intersected;
     SA.counters = (uint32_t *)ctx->counters.p;
     SA.clist = (float *)ctx->clist.p;
+    SA.vacc = (float4 *)ctx->vacc.p;
     SA.clist_cap = (uint32_t)(n + 1);
     if (ctx->n_active > 0)
     {
@@ -2024,6 +2087,9 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
         ++ctx->launches;
     }
     stage(ctx, EV_CONSUME, st);
+    voxel_solve<<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
+    ++ctx->launches;
+    stage(ctx, EV_SOLVE, st);
     constrained_solve<<<ctx->sms * 8, 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
                                                     ctx->g, dual_vertices);
     ++ctx->launches;
