@@ -363,25 +363,88 @@ __device__ __forceinline__ void face_setup(const float v[3][3], const Grid &g, F
     }
 }
 
-__device__ __forceinline__ bool face_test(const FaceSetup &fs, const Grid &g, int x, int y, int z)
+// Face-test coefficients by index: 0-2 n, 3 d1, 4 d2, 5-10 nxy[k][c] (k*2+c),
+// 11-13 dxy, 14-19 nyz, 20-22 dyz, 23-28 nzx, 29-31 dzx.
+constexpr int kFaceCoef = 32;
+
+__device__ __forceinline__ void face_coefs(const FaceSetup &fs, float c[kFaceCoef])
+{
+    c[0] = fs.n[0];
+    c[1] = fs.n[1];
+    c[2] = fs.n[2];
+    c[3] = fs.d1;
+    c[4] = fs.d2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        c[5 + 2 * k] = fs.nxy[k][0];
+        c[6 + 2 * k] = fs.nxy[k][1];
+        c[11 + k] = fs.dxy[k];
+        c[14 + 2 * k] = fs.nyz[k][0];
+        c[15 + 2 * k] = fs.nyz[k][1];
+        c[20 + k] = fs.dyz[k];
+        c[23 + 2 * k] = fs.nzx[k][0];
+        c[24 + 2 * k] = fs.nzx[k][1];
+        c[29 + k] = fs.dzx[k];
+    }
+}
+
+// Box-triangle test at the voxel's min corner (flexible_dual_grid.cpp:324-409):
+// plane slab, then the 9 projected edge half-planes.  `C(i)` returns face-test
+// coefficient i (see kFaceCoef), so registers and shared memory share one code path.
+template <typename Coef>
+__device__ __forceinline__ bool face_test_c(const Coef &C, const Grid &g, int x, int y, int z)
 {
     const float p0 = g.vs[0] * (float)x, p1 = g.vs[1] * (float)y, p2 = g.vs[2] * (float)z;
-    const float nd = dot3f(fs.n[0], fs.n[1], fs.n[2], p0, p1, p2);
-    if ((nd + fs.d1) * (nd + fs.d2) > 0.0f)
+    const float nd = dot3f(C(0), C(1), C(2), p0, p1, p2);
+    if ((nd + C(3)) * (nd + C(4)) > 0.0f)
         return false;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-        if (dot2f(fs.nxy[k][0], fs.nxy[k][1], p0, p1) + fs.dxy[k] < 0.0f)
+        if (dot2f(C(5 + 2 * k), C(6 + 2 * k), p0, p1) + C(11 + k) < 0.0f)
             return false;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-        if (dot2f(fs.nyz[k][0], fs.nyz[k][1], p1, p2) + fs.dyz[k] < 0.0f)
+        if (dot2f(C(14 + 2 * k), C(15 + 2 * k), p1, p2) + C(20 + k) < 0.0f)
             return false;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-        if (dot2f(fs.nzx[k][0], fs.nzx[k][1], p2, p0) + fs.dzx[k] < 0.0f)
+        if (dot2f(C(23 + 2 * k), C(24 + 2 * k), p2, p0) + C(29 + k) < 0.0f)
             return false;
     return true;
+}
+
+struct FaceCoefRegs
+{
+    const FaceSetup &fs;
+    __device__ __forceinline__ float operator()(int i) const
+    {
+        switch (i)
+        {
+        case 0: return fs.n[0];
+        case 1: return fs.n[1];
+        case 2: return fs.n[2];
+        case 3: return fs.d1;
+        case 4: return fs.d2;
+        default: break;
+        }
+        if (i < 11)
+            return fs.nxy[(i - 5) >> 1][(i - 5) & 1];
+        if (i < 14)
+            return fs.dxy[i - 11];
+        if (i < 20)
+            return fs.nyz[(i - 14) >> 1][(i - 14) & 1];
+        if (i < 23)
+            return fs.dyz[i - 20];
+        if (i < 29)
+            return fs.nzx[(i - 23) >> 1][(i - 23) & 1];
+        return fs.dzx[i - 29];
+    }
+};
+
+__device__ __forceinline__ bool face_test(const FaceSetup &fs, const Grid &g, int x, int y, int z)
+{
+    return face_test_c(FaceCoefRegs{fs}, g, x, y, z);
 }
 
 // ---------------------------------------------------------------------------

@@ -465,53 +465,321 @@ __device__ __forceinline__ void face_bricks(const FaceSetup &fs, const Grid &g, 
     }
 }
 
-constexpr int kFaceSlots = 4; // threads per triangle in the face pass
 
-// kFaceSlots threads per triangle: thread j tests bricks j, j+kFaceSlots, ... of the face box.
-template <int M, typename IdxT>
-__global__ void __launch_bounds__(kThreads) face_records(GenArgs A)
+// Face box of a triangle restricted to the brick with origin o, as local
+// [lo, hi) per axis; false if empty.
+__device__ __forceinline__ bool brick_box(const int bmin[3], const int bmax[3], const int o[3], int lo[3], int hi[3])
 {
-    const long long tj = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tj >= (long long)kFaceSlots * A.m.nf)
-        return;
-    const long long t = tj / kFaceSlots;
-    const int j = (int)(tj - t * kFaceSlots);
-    float v[3][3];
-    if (!tri_load<IdxT>(A.m, t, v))
-        return;
-    const Grid &g = A.m.g;
-    int bmin[3], bmax[3];
-    face_box(v, g, bmin, bmax);
-    if (bmax[0] <= bmin[0] || bmax[1] <= bmin[1] || bmax[2] <= bmin[2])
-        return;
-    int b0[3], b1[3];
+    bool ok = true;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
-        b0[a] = (bmin[a] - g.gmin[a]) >> 3;
-        b1[a] = (bmax[a] - 1 - g.gmin[a]) >> 3;
+        lo[a] = (bmin[a] > o[a] ? bmin[a] : o[a]) - o[a];
+        hi[a] = (bmax[a] < o[a] + 8 ? bmax[a] : o[a] + 8) - o[a];
+        ok = ok && hi[a] > lo[a];
     }
-    const long long nx = b1[0] - b0[0] + 1, ny = b1[1] - b0[1] + 1, nz = b1[2] - b0[2] + 1;
-    const long long nbk = nx * ny * nz;
-    if (nbk > kInlineFaceBricks)
+    return ok;
+}
+
+// Word w of a brick's occupancy restricted to the local box [lo, hi).
+__device__ __forceinline__ uint32_t box_word(uint32_t word, int w, const int lo[3], const int hi[3])
+{
+    const int lz = w >> 1;
+    if (lz < lo[2] || lz >= hi[2])
+        return 0u;
+    const uint32_t xmask = ((1u << hi[0]) - 1u) & ~((1u << lo[0]) - 1u);
+    uint32_t mask = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
     {
-        if (M == COUNT && j == 0)
-        {
-            const uint32_t slot = atomicAdd(&A.counters[C_FACE_LARGE], 1u);
-            if (slot < A.face_large_cap)
-                A.face_large[slot] = (uint32_t)t;
-            else
-                atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
-        }
-        return;
+        const int ly = (w & 1) * 4 + q;
+        if (ly >= lo[1] && ly < hi[1])
+            mask |= xmask << (q * 8);
     }
-    if (j >= nbk)
-        return;
-    FaceSetup fs;
-    face_setup(v, g, fs);
+    return word & mask;
+}
+
+constexpr int kFaceThreads = 128; // face pass: one triangle per lane
+constexpr int kFaceWindow = 512; // candidates listed per step of a warp
+
+struct FaceWarp
+{
+    float coef[kFaceCoef][32];         // face-test coefficients of each lane's triangle
+    int info[11][32];                  // per lane: first brick (3), bricks along x and y, face box min (3), max (3)
+    uint32_t pass[kWordsPerBrick][32]; // face-test hits of each item of the current chunk
+    uint32_t cand[kWordsPerBrick][32]; // candidate words of the chunk's dense items
+    int org[3][32];                    // brick origin of each item
+    uint8_t own[32];                   // lane whose triangle an item belongs to
+    uint16_t cl[kFaceWindow];          // candidate list: local voxel index
+    uint8_t cs[kFaceWindow];           // candidate list: item slot
+};
+
+struct FaceCoefArr
+{
+    const float *c;
+    __device__ __forceinline__ float operator()(int i) const
+    {
+        return c[i];
+    }
+};
+
+struct FaceCoefSmem
+{
+    const float *p; // &coef[0][owner]
+    __device__ __forceinline__ float operator()(int i) const
+    {
+        return p[i * 32];
+    }
+};
+
+// Face stage (flexible_dual_grid.cpp:298-414), one triangle per lane.  The
+// warp's (triangle, brick) items are taken 32 at a time; the candidates of
+// those items (active voxels of the brick inside the triangle's face box) are
+// listed in shared memory and tested by all 32 lanes, so the face tests run on
+// full warps whatever the triangles' sizes.  COUNT adds each item's hits to its
+// brick's record count; FILL writes one record per hit.
+template <int M, typename IdxT>
+__global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
+{
+    __shared__ FaceWarp FW[kFaceThreads / 32];
+    const int lane = threadIdx.x & 31;
+    FaceWarp &W = FW[threadIdx.x >> 5];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long tbase = t - lane;
+    const Grid &g = A.m.g;
+    int nbk = 0;
+    if (t < A.m.nf)
+    {
+        float v[3][3];
+        if (tri_load<IdxT>(A.m, t, v))
+        {
+            int bmin[3], bmax[3];
+            face_box(v, g, bmin, bmax);
+            if (bmax[0] > bmin[0] && bmax[1] > bmin[1] && bmax[2] > bmin[2])
+            {
+                int b0[3], b1[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                {
+                    b0[a] = (bmin[a] - g.gmin[a]) >> 3;
+                    b1[a] = (bmax[a] - 1 - g.gmin[a]) >> 3;
+                }
+                const int nx = b1[0] - b0[0] + 1, ny = b1[1] - b0[1] + 1;
+                const long long n = (long long)nx * ny * (b1[2] - b0[2] + 1);
+                if (n > kInlineFaceBricks)
+                {
+                    if (M == COUNT)
+                    {
+                        const uint32_t slot = atomicAdd(&A.counters[C_FACE_LARGE], 1u);
+                        if (slot < A.face_large_cap)
+                            A.face_large[slot] = (uint32_t)t;
+                        else
+                            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+                    }
+                }
+                else
+                {
+                    FaceSetup fs;
+                    face_setup(v, g, fs);
+                    float c[kFaceCoef];
+                    face_coefs(fs, c);
+#pragma unroll
+                    for (int i = 0; i < kFaceCoef; ++i)
+                        W.coef[i][lane] = c[i];
+                    const int inf[11] = {b0[0], b0[1], b0[2], nx, ny, bmin[0], bmin[1], bmin[2], bmax[0], bmax[1], bmax[2]};
+#pragma unroll
+                    for (int i = 0; i < 11; ++i)
+                        W.info[i][lane] = inf[i];
+                    nbk = (int)n;
+                }
+            }
+        }
+    }
+    // items of the warp: exclusive scan of the lanes' brick counts
+    int istart = nbk;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+    {
+        const int y = __shfl_up_sync(0xffffffffu, istart, d);
+        if (lane >= d)
+            istart += y;
+    }
+    const int nitems = __shfl_sync(0xffffffffu, istart, 31);
+    istart -= nbk;
+    __syncwarp();
+    for (int ibase = 0; ibase < nitems; ibase += 32)
+    {
+        // item of this lane's slot: owner lane (last lane whose first item is at
+        // or before it) and brick rank r within the owner's face box
+        const int it = ibase + lane;
+        int lo_l = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1)
+        {
+            const int cand = lo_l + step;
+            const int sv = __shfl_sync(0xffffffffu, istart, cand & 31);
+            if (cand < 32 && sv <= it)
+                lo_l = cand;
+        }
+        const int ol = lo_l;
+        const int r = it - __shfl_sync(0xffffffffu, istart, ol);
+        uint32_t cw[kWordsPerBrick];
+        uint32_t cnt = 0;
+        long long b = 0;
+        if (it < nitems)
+        {
+            const int nx = W.info[3][ol], ny = W.info[4][ol];
+            const int bx = W.info[0][ol] + r % nx, by = W.info[1][ol] + (r / nx) % ny, bz = W.info[2][ol] + r / (nx * ny);
+            b = (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
+            const int o[3] = {g.gmin[0] + bx * kBrick, g.gmin[1] + by * kBrick, g.gmin[2] + bz * kBrick};
+            const int bmin[3] = {W.info[5][ol], W.info[6][ol], W.info[7][ol]};
+            const int bmax[3] = {W.info[8][ol], W.info[9][ol], W.info[10][ol]};
+            int lo[3], hi[3];
+            const bool any = brick_box(bmin, bmax, o, lo, hi);
+            const uint4 *bw4 = reinterpret_cast<const uint4 *>(A.bits + b * kWordsPerBrick);
+#pragma unroll
+            for (int q4 = 0; q4 < 4; ++q4)
+            {
+                const uint4 wv = any ? bw4[q4] : make_uint4(0u, 0u, 0u, 0u);
+                const uint32_t words[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                {
+                    cw[q4 * 4 + k] = any ? box_word(words[k], q4 * 4 + k, lo, hi) : 0u;
+                    cnt += __popc(cw[q4 * 4 + k]);
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                W.org[a][lane] = o[a];
+            W.own[lane] = (uint8_t)ol;
+        }
+        else
+        {
+#pragma unroll
+            for (int w = 0; w < kWordsPerBrick; ++w)
+                cw[w] = 0u;
+        }
+#pragma unroll
+        for (int w = 0; w < kWordsPerBrick; ++w)
+            W.pass[w][lane] = 0u;
+        // items with many candidates are tested by the whole warp with the
+        // triangle's coefficients in registers; the others go through the list
+        const bool dense = cnt > 32u;
+        const uint32_t dmask = __ballot_sync(0xffffffffu, dense);
+        if (dense)
+        {
+#pragma unroll
+            for (int w = 0; w < kWordsPerBrick; ++w)
+                W.cand[w][lane] = cw[w];
+        }
+        __syncwarp();
+        for (uint32_t dm = dmask; dm; dm &= dm - 1u)
+        {
+            const int sd = __ffs(dm) - 1;
+            const int so = W.own[sd];
+            float c[kFaceCoef];
+#pragma unroll
+            for (int i = 0; i < kFaceCoef; ++i)
+                c[i] = W.coef[i][so];
+            const int w = lane >> 1;
+            const uint32_t word = W.cand[w][sd];
+            uint32_t bits = (lane & 1) ? (word & 0xffff0000u) : (word & 0x0000ffffu);
+            uint32_t hit = 0;
+            const int ox = W.org[0][sd], oy = W.org[1][sd] + (w & 1) * 4, oz = W.org[2][sd] + (w >> 1);
+            while (bits)
+            {
+                const int bt = __ffs(bits) - 1;
+                bits &= bits - 1u;
+                if (face_test_c(FaceCoefArr{c}, g, ox + (bt & 7), oy + (bt >> 3), oz))
+                    hit |= 1u << bt;
+            }
+            if (hit)
+                atomicOr(&W.pass[w][sd], hit);
+        }
+        const uint32_t lcnt = dense ? 0u : cnt;
+        uint32_t off = lcnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, off, d);
+            if (lane >= d)
+                off += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
+        off -= lcnt;
+        for (uint32_t wbeg = 0; wbeg < total; wbeg += kFaceWindow)
+        {
+            // list the candidates that fall in [wbeg, wbeg + kFaceWindow)
+            const uint32_t wend = wbeg + kFaceWindow;
+            if (cnt && !dense && off < wend && off + cnt > wbeg)
+            {
+                uint32_t idx = off;
 #pragma unroll 1
-    for (long long k = j; k < nbk; k += kFaceSlots)
-        face_brick<M>(A, fs, (uint32_t)t, b0[0] + (int)(k % nx), b0[1] + (int)((k / nx) % ny), b0[2] + (int)(k / (nx * ny)));
+                for (int w = 0; w < kWordsPerBrick && idx < wend; ++w)
+                {
+                    uint32_t word = cw[w];
+                    while (word && idx < wend)
+                    {
+                        const int bt = __ffs(word) - 1;
+                        word &= word - 1u;
+                        if (idx >= wbeg)
+                        {
+                            W.cl[idx - wbeg] = (uint16_t)(w * 32 + bt);
+                            W.cs[idx - wbeg] = (uint8_t)lane;
+                        }
+                        ++idx;
+                    }
+                }
+            }
+            __syncwarp();
+            const uint32_t n = total - wbeg < (uint32_t)kFaceWindow ? total - wbeg : (uint32_t)kFaceWindow;
+            for (uint32_t k = lane; k < n; k += 32)
+            {
+                const int lv = W.cl[k], sl = W.cs[k];
+                const int x = W.org[0][sl] + (lv & 7), y = W.org[1][sl] + ((lv >> 3) & 7), z = W.org[2][sl] + (lv >> 6);
+                if (face_test_c(FaceCoefSmem{&W.coef[0][W.own[sl]]}, g, x, y, z))
+                    atomicOr(&W.pass[lv >> 5][sl], 1u << (lv & 31));
+            }
+            __syncwarp();
+        }
+        uint32_t hits = 0;
+        if (cnt)
+        {
+#pragma unroll
+            for (int w = 0; w < kWordsPerBrick; ++w)
+                hits += __popc(W.pass[w][lane]);
+        }
+        if (hits)
+        {
+            const uint32_t k0 = agg_add(A.rcnt, b, hits);
+            if (M == FILL)
+            {
+                if ((unsigned long long)k0 + hits > A.roff[b + 1] - A.roff[b])
+                    atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
+                else
+                {
+                    unsigned long long pos = A.roff[b] + k0;
+                    const uint32_t tri = (uint32_t)(tbase + ol);
+                    for (int w = 0; w < kWordsPerBrick; ++w)
+                    {
+                        uint32_t pm = W.pass[w][lane];
+                        while (pm)
+                        {
+                            const int bt = __ffs(pm) - 1;
+                            pm &= pm - 1u;
+                            Rec rr;
+                            rr.a = tri;
+                            rr.b = kRecFace | (uint32_t)(w * 32 + bt);
+                            rr.c = 0u;
+                            A.rec[pos++] = rr;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
 }
 
 // One CTA per listed triangle; threads over the bricks of its face box.
@@ -1692,7 +1960,7 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
 {
     if (ctx->fw > 0.0f && ctx->nf > 0)
     {
-        face_records<M, IdxT><<<blocks_for((long long)kFaceSlots * ctx->nf, kThreads), kThreads, 0, st>>>(A);
+        face_records<M, IdxT><<<blocks_for(ctx->nf, kFaceThreads), kFaceThreads, 0, st>>>(A);
         large_face_records<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
         ctx->launches += 2;
     }
