@@ -20,6 +20,9 @@
 //             boundary {e, 2<<30 | local voxel, 0}, e = index in the
 //                      boundary edge list, which is sorted by (v_min, v_max)
 //   qtab    plane quadric per triangle (10 floats)
+//   contrib per-voxel contribution lists, 16 B entries; brick b owns entries
+//           [4*roff[b], 4*roff[b+1]) (a record yields at most 4 contributions)
+//   vlist   per output row: first entry (40 bits) | entry count << 40
 //   btab    line quadric per boundary edge (10 floats)
 //
 // begin (ends with the one host synchronisation of a conversion):
@@ -32,10 +35,13 @@
 //   face_records<COUNT>, boundary_records<COUNT>, scan -> record offsets
 // finish (no synchronisation):
 //   *_records<FILL>     the same generators write the records
-//   brick_consume       one CTA per active brick: records -> per-voxel lists in
-//                       shared memory, ordered by the reference accumulation
-//                       order, summed sequentially in FP32 (bit-identical to
-//                       the reference CPU sums), regularised, CPQR-solved
+//   brick_lists         one CTA per active brick: records -> per-voxel
+//                       contribution lists {key, payload} in global memory
+//                       (a counting sort by voxel; records are taken in bucket
+//                       order, close to key order, so lists come out nearly sorted)
+//   voxel_accumulate    one thread per voxel: insertion-sorts its list by key,
+//                       sums it sequentially in FP32 in that order (bit-identical
+//                       to the reference CPU sums), regularises, CPQR-solves
 //   constrained_solve   box-constrained search for the few voxels whose
 //                       unconstrained solution leaves the voxel
 //
@@ -66,11 +72,6 @@ constexpr int kInlineFaceBricks = 64; // face boxes over more bricks go to the C
 constexpr int kChunk = 8;             // columns per tile for large (triangle, axis) pairs
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
-#ifndef OVX_FDG_CONSUME_WINDOW
-#define OVX_FDG_CONSUME_WINDOW 2048
-#endif
-constexpr int kWindow = OVX_FDG_CONSUME_WINDOW; // per-voxel contributions held in shared memory per pass of a brick
-constexpr int kThreadSort = 48; // lists longer than this are ranked by the whole CTA
 
 // device counter words
 enum
@@ -1034,38 +1035,22 @@ struct SolveArgs
     float *dual;
     uint8_t *flags;
     uint32_t *counters;
-    float4 *vacc; // per-voxel accumulated state, 4 float4 per output row
+    uint4 *contrib;             // per-voxel contribution lists {key lo, key hi, payload, 0}
+    unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40
     float *clist; // deferred constrained searches, 16 words each
     uint32_t clist_cap;
 };
 
-struct BrickShared
-{
-    uint32_t bits[kWordsPerBrick];
-    uint32_t wpre[kWordsPerBrick];
-    uint16_t vl[512]; // brick-local index of the i-th active voxel (i = output row - brick base)
-    uint32_t cnt[512];
-    uint32_t off[512];
-    uint32_t fill[512];
-    unsigned long long key[kWindow];
-    uint32_t pay[kWindow];
-    uint16_t perm[kWindow];
-    uint32_t scan_tmp[kConsumeThreads / 32 + 1];
-    int nvox, win_lo, win_hi, big_n, long_n;
-    uint32_t win_base, total, status;
-    uint16_t big[512];
-    uint16_t longl[512];
-};
-
-__device__ __forceinline__ int dense_index(const BrickShared &S, int lv)
+template <typename SS>
+__device__ __forceinline__ int dense_index(const SS &S, int lv)
 {
     const int w = lv >> 5, b = lv & 31;
     return (int)(S.wpre[w] + __popc(S.bits[w] & ((1u << b) - 1u)));
 }
 
 // Expand one record of the brick into (dense voxel index, order key, payload) contributions.
-template <typename Sink>
-__device__ __forceinline__ void expand(const BrickShared &S, const Rec &r, Sink &sink)
+template <typename SS, typename Sink>
+__device__ __forceinline__ void expand(const SS &S, const Rec &r, Sink &sink)
 {
     const uint32_t kind = r.b >> 30;
     if (kind == 0)
@@ -1090,33 +1075,6 @@ __device__ __forceinline__ void expand(const BrickShared &S, const Rec &r, Sink 
     else
         sink(dense_index(S, (int)(r.b & 511u)), kKeyBoundary | (unsigned long long)r.a, 0u);
 }
-
-struct CountSink
-{
-    BrickShared &S;
-    __device__ __forceinline__ void operator()(int i, unsigned long long, uint32_t) const
-    {
-        atomicAdd(&S.cnt[i], 1u);
-    }
-};
-
-struct FillSink
-{
-    BrickShared &S;
-    int lo, hi;
-    uint32_t base;
-    __device__ __forceinline__ void operator()(int i, unsigned long long key, uint32_t pay) const
-    {
-        if (i < lo || i >= hi || S.cnt[i] > (uint32_t)kWindow)
-            return;
-        const uint32_t k = atomicAdd(&S.fill[i], 1u);
-        if (k >= S.cnt[i])
-            return; // cannot happen: the count pass read the same records
-        const uint32_t pos = S.off[i] - base + k;
-        S.key[pos] = key;
-        S.pay[pos] = pay;
-    }
-};
 
 struct Acc
 {
@@ -1206,38 +1164,240 @@ __device__ __forceinline__ void acc_entry(const SolveArgs &A, const int vc[3], u
     }
 }
 
-// Accumulated state of one voxel -> its row of the voxel state array
-// (quadric, mass sum, count, flag bits: 16 words, 64-byte aligned).
-__device__ __forceinline__ void store_acc(const SolveArgs &A, long long row, const Acc &a)
+// ---------------------------------------------------------------------------
+// Contribution lists: one CTA per active brick expands the brick's records
+// and counting-sorts the contributions by voxel into global memory (brick b
+// owns entries [4*roff[b], 4*roff[b+1]): a record expands to at most four
+// contributions); then one thread per voxel orders its list by key, sums it in
+// that order (the reference CPU order) and solves.
+// ---------------------------------------------------------------------------
+struct ListShared
 {
-    float4 *d = A.vacc + row * 4;
-    d[0] = make_float4(a.q[0], a.q[1], a.q[2], a.q[3]);
-    d[1] = make_float4(a.q[4], a.q[5], a.q[6], a.q[7]);
-    d[2] = make_float4(a.q[8], a.q[9], a.mean[0], a.mean[1]);
-    d[3] = make_float4(a.mean[2], a.cnt, __uint_as_float(a.flags), 0.0f);
+    uint32_t bits[kWordsPerBrick];
+    uint32_t wpre[kWordsPerBrick];
+    uint32_t cnt[512];
+    uint32_t off[512];
+    uint32_t scan_tmp[kConsumeThreads / 32 + 1];
+    int nvox;
+    uint32_t status;
+};
+
+struct ListCount
+{
+    ListShared &S;
+    __device__ __forceinline__ void operator()(int i, unsigned long long, uint32_t) const
+    {
+        atomicAdd(&S.cnt[i], 1u);
+    }
+};
+
+struct ListFill
+{
+    ListShared &S;
+    uint4 *out;              // the brick's first entry
+    unsigned long long room; // entries the brick owns
+    __device__ __forceinline__ void operator()(int i, unsigned long long key, uint32_t pay) const
+    {
+        // off[i] counts up from the start of voxel i's list: records are taken
+        // in bucket order, which is close to key order, so lists come out nearly sorted
+        const uint32_t k = atomicAdd(&S.off[i], 1u);
+        if ((unsigned long long)k >= room)
+        {
+            atomicOr(&S.status, (uint32_t)ST_REPLAY);
+            return;
+        }
+        out[k] = make_uint4((uint32_t)key, (uint32_t)(key >> 32), pay, 0u);
+    }
+};
+
+__global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
+{
+    __shared__ ListShared S;
+    const int tid = threadIdx.x;
+    const Grid &g = A.m.g;
+    const long long b = A.active[blockIdx.x];
+    int o[3];
+    brick_origin(g, b, o);
+    const Rec *rec = A.rec + A.roff[b];
+    const unsigned long long nrec = A.roff[b + 1] - A.roff[b];
+    if (tid < 32)
+    {
+        const uint32_t w = tid < kWordsPerBrick ? A.bits[b * kWordsPerBrick + tid] : 0u;
+        const uint32_t c = __popc(w);
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (tid >= d)
+                incl += y;
+        }
+        if (tid < kWordsPerBrick)
+        {
+            S.bits[tid] = w;
+            S.wpre[tid] = incl - c;
+        }
+        if (tid == 31)
+        {
+            S.nvox = (int)incl;
+            S.status = 0;
+        }
+    }
+    for (int i = tid; i < 512; i += blockDim.x)
+        S.cnt[i] = 0;
+    __syncthreads();
+    const int nvox = S.nvox;
+    const unsigned long long vbase = A.bbase[b];
+    // voxel coordinates of the brick's rows (x-fastest local order)
+    for (int w = 0; w < kWordsPerBrick; ++w)
+    {
+        const uint32_t word = S.bits[w];
+        if (tid < 32 && ((word >> tid) & 1u))
+        {
+            const int lv = w * 32 + tid;
+            const long long row = (long long)(vbase + S.wpre[w] + __popc(word & ((1u << tid) - 1u)));
+            A.vox[row * 3 + 0] = o[0] + (lv & 7);
+            A.vox[row * 3 + 1] = o[1] + ((lv >> 3) & 7);
+            A.vox[row * 3 + 2] = o[2] + (lv >> 6);
+        }
+    }
+    {
+        ListCount cs{S};
+        for (unsigned long long r = tid; r < nrec; r += blockDim.x)
+            expand(S, rec[r], cs);
+    }
+    __syncthreads();
+    // exclusive scan of the counts: off[i] = start of voxel i's list
+    {
+        const int lane = tid & 31, warp = tid >> 5;
+        constexpr int per = 512 / kConsumeThreads;
+        uint32_t v[per], sum = 0;
+#pragma unroll
+        for (int k = 0; k < per; ++k)
+        {
+            const int j = tid * per + k;
+            v[k] = j < nvox ? S.cnt[j] : 0u;
+            sum += v[k];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d)
+                incl += y;
+        }
+        if (lane == 31)
+            S.scan_tmp[warp] = incl;
+        __syncthreads();
+        if (tid == 0)
+        {
+            uint32_t r = 0;
+            for (int k = 0; k < kConsumeThreads / 32; ++k)
+            {
+                const uint32_t x = S.scan_tmp[k];
+                S.scan_tmp[k] = r;
+                r += x;
+            }
+        }
+        __syncthreads();
+        uint32_t run = S.scan_tmp[warp] + incl - sum;
+        const unsigned long long first = 4ull * A.roff[b];
+#pragma unroll
+        for (int k = 0; k < per; ++k)
+        {
+            const int j = tid * per + k;
+            if (j < nvox)
+            {
+                if (v[k] == 0u || v[k] >= (1u << 24))
+                    atomicOr(&S.status, (uint32_t)ST_REPLAY); // every active voxel has a scanline contribution
+                A.vlist[vbase + j] = (first + run) | ((unsigned long long)v[k] << 40);
+            }
+            S.off[j] = run;
+            run += v[k];
+        }
+    }
+    __syncthreads();
+    {
+        ListFill fs{S, A.contrib + 4ull * A.roff[b], 4ull * nrec};
+        for (unsigned long long r = tid; r < nrec; r += blockDim.x)
+            expand(S, rec[r], fs);
+    }
+    __syncthreads();
+    if (tid == 0 && S.status)
+        atomicOr(&A.counters[C_STATUS], S.status);
 }
 
-// One thread per voxel row: regularise and solve (flexible_dual_grid.cpp:763-797);
-// voxels whose unconstrained solution leaves the box go to the constrained-search list.
-__global__ void __launch_bounds__(128) voxel_solve(SolveArgs A, long long n)
+constexpr int kLocalSort = 64; // lists up to this length are ordered in thread-local memory
+
+// One thread per voxel row: order the voxel's contributions by key, sum them in
+// that order, regularise and solve (flexible_dual_grid.cpp:763-797); voxels
+// whose unconstrained solution leaves the box go to the constrained-search list.
+__global__ void __launch_bounds__(128) voxel_accumulate(SolveArgs A, long long nrows)
 {
     const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= n)
+    if (row >= nrows)
         return;
-    const float4 *s = A.vacc + row * 4;
-    const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
-    const float qa[10] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w, s2.x, s2.y};
-    const float mean[3] = {s2.z, s2.w, s3.x};
-    const float cnt = s3.y;
-    const uint32_t flags = __float_as_uint(s3.z);
+    const unsigned long long d = A.vlist[row];
+    const unsigned long long first = d & ((1ull << 40) - 1ull);
+    const uint32_t n = (uint32_t)(d >> 40);
     const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
+    uint4 *lst = A.contrib + first;
+    Acc a;
+    acc_init(a);
+    if (n <= (uint32_t)kLocalSort)
+    {
+        unsigned long long key[kLocalSort];
+        uint32_t pay[kLocalSort];
+        for (uint32_t x = 0; x < n; ++x)
+        {
+            const uint4 e = lst[x];
+            const unsigned long long k = (unsigned long long)e.x | ((unsigned long long)e.y << 32);
+            uint32_t j = x;
+            while (j > 0 && key[j - 1] > k)
+            {
+                key[j] = key[j - 1];
+                pay[j] = pay[j - 1];
+                --j;
+            }
+            key[j] = k;
+            pay[j] = e.z;
+        }
+        for (uint32_t x = 0; x < n; ++x)
+            acc_entry(A, vc, key[x], pay[x], a);
+    }
+    else
+    {
+        // long list (rare): insertion sort in place, then sum
+        for (uint32_t x = 1; x < n; ++x)
+        {
+            const uint4 e = lst[x];
+            const unsigned long long k = (unsigned long long)e.x | ((unsigned long long)e.y << 32);
+            uint32_t j = x;
+            while (j > 0)
+            {
+                const uint4 pe = lst[j - 1];
+                const unsigned long long pk = (unsigned long long)pe.x | ((unsigned long long)pe.y << 32);
+                if (pk <= k)
+                    break;
+                lst[j] = pe;
+                --j;
+            }
+            lst[j] = e;
+        }
+        for (uint32_t x = 0; x < n; ++x)
+        {
+            const uint4 e = lst[x];
+            acc_entry(A, vc, (unsigned long long)e.x | ((unsigned long long)e.y << 32), e.z, a);
+        }
+    }
     float q[10];
-    regularize(qa, mean, cnt, A.rw, q);
+    regularize(a.q, a.mean, a.cnt, A.rw, q);
     float v[3];
     const bool inside = solve_unconstrained(vc, A.m.g, q, v);
-    A.flags[row * 3 + 0] = (uint8_t)(flags & 1u);
-    A.flags[row * 3 + 1] = (uint8_t)((flags >> 1) & 1u);
-    A.flags[row * 3 + 2] = (uint8_t)((flags >> 2) & 1u);
+    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
+    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
+    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
     if (inside)
     {
         A.dual[row * 3 + 0] = v[0];
@@ -1259,278 +1419,6 @@ __global__ void __launch_bounds__(128) voxel_solve(SolveArgs A, long long n)
 #pragma unroll
     for (int i = 0; i < 10; ++i)
         c[4 + i] = q[i];
-}
-
-// block-wide exclusive scan of S.cnt[0..nvox) (lists longer than the window count 0) into S.off
-__device__ __forceinline__ void scan_counts(BrickShared &S, int nvox)
-{
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int per = 512 / kConsumeThreads;
-    uint32_t v[per], sum = 0;
-#pragma unroll
-    for (int i = 0; i < per; ++i)
-    {
-        const int j = tid * per + i;
-        const uint32_t c = j < nvox ? S.cnt[j] : 0u;
-        v[i] = c > (uint32_t)kWindow ? 0u : c;
-        sum += v[i];
-    }
-    uint32_t incl = sum;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1)
-    {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d)
-            incl += y;
-    }
-    if (lane == 31)
-        S.scan_tmp[warp] = incl;
-    __syncthreads();
-    if (tid == 0)
-    {
-        uint32_t r = 0;
-        for (int i = 0; i < kConsumeThreads / 32; ++i)
-        {
-            const uint32_t x = S.scan_tmp[i];
-            S.scan_tmp[i] = r;
-            r += x;
-        }
-        S.total = r;
-    }
-    __syncthreads();
-    uint32_t run = S.scan_tmp[warp] + incl - sum;
-#pragma unroll
-    for (int i = 0; i < per; ++i)
-    {
-        S.off[tid * per + i] = run;
-        run += v[i];
-    }
-}
-
-struct SelectSink
-{
-    int target;
-    unsigned long long last;
-    bool any;
-    unsigned long long best;
-    uint32_t pay;
-    __device__ __forceinline__ void operator()(int j, unsigned long long key, uint32_t p)
-    {
-        if (j != target || (any && key <= last))
-            return;
-        if (key < best)
-        {
-            best = key;
-            pay = p;
-        }
-    }
-};
-
-// A voxel whose list exceeds the window: its contributions in key order by
-// repeated selection over the brick's records (one thread; rare).
-__device__ __noinline__ void select_voxel(const SolveArgs &A, const BrickShared &S, int i, const Rec *rec, unsigned long long nrec,
-                                          long long row, const int vc[3])
-{
-    Acc a;
-    acc_init(a);
-    const uint32_t n = S.cnt[i];
-    unsigned long long last = 0;
-    for (uint32_t step = 0; step < n; ++step)
-    {
-        SelectSink sel{i, last, step > 0, ~0ull, 0u};
-        for (unsigned long long r = 0; r < nrec; ++r)
-            expand(S, rec[r], sel);
-        acc_entry(A, vc, sel.best, sel.pay, a);
-        last = sel.best;
-    }
-    store_acc(A, row, a);
-}
-
-__global__ void __launch_bounds__(kConsumeThreads, 8) brick_consume(SolveArgs A)
-{
-    __shared__ BrickShared S;
-    const int tid = threadIdx.x;
-    const uint32_t slot = blockIdx.x;
-    const Grid &g = A.m.g;
-    const long long b = A.active[slot];
-    int o[3];
-    brick_origin(g, b, o);
-    const Rec *rec = A.rec + A.roff[b];
-    const unsigned long long nrec = A.roff[b + 1] - A.roff[b];
-
-    // occupancy words, their prefix counts and the dense list of active voxels
-    if (tid < 32)
-    {
-        const uint32_t w = tid < kWordsPerBrick ? A.bits[b * kWordsPerBrick + tid] : 0u;
-        const uint32_t c = __popc(w);
-        uint32_t incl = c;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1)
-        {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-            if (tid >= d)
-                incl += y;
-        }
-        if (tid < kWordsPerBrick)
-        {
-            S.bits[tid] = w;
-            S.wpre[tid] = incl - c;
-            uint32_t x = w, k = incl - c;
-            while (x)
-            {
-                const int bt = __ffs(x) - 1;
-                x &= x - 1u;
-                S.vl[k++] = (uint16_t)(tid * 32 + bt);
-            }
-        }
-        if (tid == 31)
-        {
-            S.nvox = (int)incl;
-            S.big_n = 0;
-            S.status = 0;
-        }
-    }
-    for (int i = tid; i < 512; i += blockDim.x)
-    {
-        S.cnt[i] = 0;
-        S.fill[i] = 0;
-    }
-    __syncthreads();
-    const int nvox = S.nvox;
-    const unsigned long long vbase = A.bbase[b];
-
-    for (int i = tid; i < nvox; i += blockDim.x)
-    {
-        const int lv = S.vl[i];
-        const long long row = (long long)(vbase + i);
-        A.vox[row * 3 + 0] = o[0] + (lv & 7);
-        A.vox[row * 3 + 1] = o[1] + ((lv >> 3) & 7);
-        A.vox[row * 3 + 2] = o[2] + (lv >> 6);
-    }
-
-    {
-        CountSink cs{S};
-        for (unsigned long long r = tid; r < nrec; r += blockDim.x)
-            expand(S, rec[r], cs);
-    }
-    __syncthreads();
-    for (int i = tid; i < nvox; i += blockDim.x)
-    {
-        const uint32_t c = S.cnt[i];
-        if (c > (uint32_t)kWindow)
-            S.big[atomicAdd(&S.big_n, 1)] = (uint16_t)i;
-        else if (c == 0)
-            S.status = ST_REPLAY; // every active voxel receives at least one scanline contribution
-    }
-    scan_counts(S, nvox);
-    __syncthreads();
-    if (tid == 0 && S.status)
-        atomicOr(&A.counters[C_STATUS], S.status);
-
-    // windows of consecutive voxels whose contributions fit in shared memory
-    int lo = 0;
-    while (lo < nvox)
-    {
-        if (tid == 0)
-        {
-            int hi = lo;
-            const uint32_t base = S.off[lo];
-            if (S.total - base <= (uint32_t)kWindow)
-                hi = nvox;
-            else
-                while (hi < nvox && S.off[hi] + (S.cnt[hi] > (uint32_t)kWindow ? 0u : S.cnt[hi]) - base <= (uint32_t)kWindow)
-                    ++hi;
-            S.win_lo = lo;
-            S.win_hi = hi;
-            S.win_base = base;
-            S.long_n = 0;
-        }
-        __syncthreads();
-        const int wlo = S.win_lo, whi = S.win_hi;
-        const uint32_t wbase = S.win_base;
-        {
-            FillSink fs{S, wlo, whi, wbase};
-            for (unsigned long long r = tid; r < nrec; r += blockDim.x)
-                expand(S, rec[r], fs);
-        }
-        __syncthreads();
-        for (int i = wlo + tid; i < whi; i += blockDim.x)
-        {
-            const uint32_t n = S.cnt[i];
-            if (n == 0 || n > (uint32_t)kWindow)
-                continue;
-            if (n > (uint32_t)kThreadSort)
-            {
-                S.longl[atomicAdd(&S.long_n, 1)] = (uint16_t)i;
-                continue;
-            }
-            const uint32_t s0 = S.off[i] - wbase;
-            for (uint32_t x = 1; x < n; ++x)
-            {
-                const unsigned long long k = S.key[s0 + x];
-                const uint32_t p = S.pay[s0 + x];
-                uint32_t j = x;
-                while (j > 0 && S.key[s0 + j - 1] > k)
-                {
-                    S.key[s0 + j] = S.key[s0 + j - 1];
-                    S.pay[s0 + j] = S.pay[s0 + j - 1];
-                    --j;
-                }
-                S.key[s0 + j] = k;
-                S.pay[s0 + j] = p;
-            }
-            for (uint32_t x = 0; x < n; ++x)
-                S.perm[s0 + x] = (uint16_t)x;
-        }
-        __syncthreads();
-        const int nlong = S.long_n;
-        for (int li = 0; li < nlong; ++li)
-        {
-            const int i = S.longl[li];
-            const uint32_t n = S.cnt[i];
-            const uint32_t s0 = S.off[i] - wbase;
-            for (uint32_t x = tid; x < n; x += blockDim.x)
-            {
-                const unsigned long long kx = S.key[s0 + x];
-                uint32_t r = 0;
-                for (uint32_t j = 0; j < n; ++j)
-                {
-                    const unsigned long long kj = S.key[s0 + j];
-                    r += (kj < kx) || (kj == kx && j < x);
-                }
-                S.perm[s0 + r] = (uint16_t)x;
-            }
-        }
-        __syncthreads();
-        for (int i = wlo + tid; i < whi; i += blockDim.x)
-        {
-            const uint32_t n = S.cnt[i];
-            if (n == 0 || n > (uint32_t)kWindow)
-                continue;
-            const uint32_t s0 = S.off[i] - wbase;
-            const int lv = S.vl[i];
-            const int vc[3] = {o[0] + (lv & 7), o[1] + ((lv >> 3) & 7), o[2] + (lv >> 6)};
-            Acc a;
-            acc_init(a);
-            for (uint32_t x = 0; x < n; ++x)
-            {
-                const uint32_t j = s0 + S.perm[s0 + x];
-                acc_entry(A, vc, S.key[j], S.pay[j], a);
-            }
-            store_acc(A, (long long)(vbase + i), a);
-        }
-        __syncthreads();
-        lo = whi;
-    }
-
-    const int nbig = S.big_n;
-    for (int k = tid; k < nbig; k += blockDim.x)
-    {
-        const int i = S.big[k];
-        const int lv = S.vl[i];
-        const int vc[3] = {o[0] + (lv & 7), o[1] + ((lv >> 3) & 7), o[2] + (lv >> 6)};
-        select_voxel(A, S, i, rec, nrec, (long long)(vbase + i), vc);
-    }
 }
 
 // Constrained search (faces, edges, corners of the voxel box) for the voxels
@@ -1737,7 +1625,7 @@ enum
     kStageEvents
 };
 const char *const kStageNames[] = {"scanline_mark_count", "compaction", "boundary_edges", "face_boundary_count",
-                                   "scanline_fill", "face_boundary_fill", "brick_consume", "voxel_solve",
+                                   "scanline_fill", "face_boundary_fill", "brick_lists", "voxel_accumulate",
                                    "constrained_solve"};
 constexpr int kStages = 9;
 
@@ -1755,7 +1643,7 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
     Buf vcnt, voff, emax, bkeys, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, vacc;
+    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist;
     unsigned long long *host = nullptr; // pinned readback words
     std::string err;
     // state between begin and finish
@@ -1783,7 +1671,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
                 &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->vacc};
+                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
@@ -2312,7 +2200,8 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(ensure(ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
     OVX_CUDA(ensure(ctx->btab, (size_t)(ctx->n_boundary + 1) * 40));
     OVX_CUDA(ensure(ctx->clist, (size_t)(n + 1) * 16 * 4));
-    OVX_CUDA(ensure(ctx->vacc, (size_t)n * 64));
+    OVX_CUDA(ensure(ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
+    OVX_CUDA(ensure(ctx->vlist, (size_t)n * 8));
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONSTRAINED, 0, 4, st));
 
@@ -2347,15 +2236,16 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.flags = intersected;
     SA.counters = (uint32_t *)ctx->counters.p;
     SA.clist = (float *)ctx->clist.p;
-    SA.vacc = (float4 *)ctx->vacc.p;
+    SA.contrib = (uint4 *)ctx->contrib.p;
+    SA.vlist = (unsigned long long *)ctx->vlist.p;
     SA.clist_cap = (uint32_t)(n + 1);
     if (ctx->n_active > 0)
     {
-        brick_consume<<<(unsigned)ctx->n_active, kConsumeThreads, 0, st>>>(SA);
+        brick_lists<<<(unsigned)ctx->n_active, kConsumeThreads, 0, st>>>(SA);
         ++ctx->launches;
     }
     stage(ctx, EV_CONSUME, st);
-    voxel_solve<<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
+    voxel_accumulate<<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
     ++ctx->launches;
     stage(ctx, EV_SOLVE, st);
     constrained_solve<<<ctx->sms * 8, 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
