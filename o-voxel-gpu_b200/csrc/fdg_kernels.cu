@@ -56,6 +56,7 @@
 #include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <mutex>
@@ -81,6 +82,7 @@ enum
     C_BOUNDARY = 2,
     C_STATUS = 3,
     C_CONSTRAINED = 4,
+    C_FSTAGED = 5,
     C_WORDS = 8
 };
 enum
@@ -159,6 +161,8 @@ struct GenArgs
     Rec *rec;                       // FILL
     float *qtab;                    // COUNT of the intersection pass
     float *btab;                    // FILL of the boundary pass
+    uint4 *fstage;                  // COUNT of the face pass: face records {brick, t, code, 0} (NULL: off)
+    uint32_t fstage_cap;
     uint32_t *counters;
     uint32_t *scan_large;
     uint32_t scan_large_cap;
@@ -751,6 +755,38 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
             for (int w = 0; w < kWordsPerBrick; ++w)
                 hits += __popc(W.pass[w][lane]);
         }
+        if (M == COUNT && A.fstage)
+        {
+            // stage the records now (one reservation per warp) so that the
+            // fill pass need not repeat the tests; past the capacity they are
+            // only counted and the fill pass runs instead
+            uint32_t incl = hits;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1)
+            {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d)
+                    incl += y;
+            }
+            uint32_t base = 0;
+            if (lane == 31 && incl)
+                base = atomicAdd(&A.counters[C_FSTAGED], incl);
+            base = __shfl_sync(0xffffffffu, base, 31);
+            unsigned long long pos = (unsigned long long)base + incl - hits;
+            const uint32_t tri = (uint32_t)(tbase + ol);
+            for (int w = 0; w < kWordsPerBrick && hits; ++w)
+            {
+                uint32_t pm = W.pass[w][lane];
+                while (pm)
+                {
+                    const int bt = __ffs(pm) - 1;
+                    pm &= pm - 1u;
+                    if (pos < A.fstage_cap)
+                        A.fstage[pos] = make_uint4((uint32_t)b, tri, kRecFace | (uint32_t)(w * 32 + bt), 0u);
+                    ++pos;
+                }
+            }
+        }
         if (hits)
         {
             const uint32_t k0 = agg_add(A.rcnt, b, hits);
@@ -781,6 +817,30 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
         }
         __syncwarp();
     }
+}
+
+// Staged face records -> their bricks' buckets (after the scanline records).
+__global__ void __launch_bounds__(kThreads) bucket_records(const uint4 *__restrict__ stage, uint32_t n, uint32_t *__restrict__ cursor,
+                                                           const unsigned long long *__restrict__ roff, Rec *__restrict__ rec,
+                                                           uint32_t *__restrict__ counters)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint4 r = stage[i];
+    const long long b = (long long)r.x;
+    const uint32_t k = agg_add(cursor, b, 1u);
+    const unsigned long long base = roff[b];
+    if (k >= roff[b + 1] - base)
+    {
+        atomicOr(&counters[C_STATUS], (uint32_t)ST_REPLAY);
+        return;
+    }
+    Rec o;
+    o.a = r.y;
+    o.b = r.z;
+    o.c = r.w;
+    rec[base + k] = o;
 }
 
 // One CTA per listed triangle; threads over the bricks of its face box.
@@ -1643,7 +1703,7 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
     Buf vcnt, voff, emax, bkeys, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist;
+    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage;
     unsigned long long *host = nullptr; // pinned readback words
     std::string err;
     // state between begin and finish
@@ -1657,6 +1717,8 @@ struct ovx_fdg_context
     float origin[3] = {0, 0, 0};
     float fw = 0, bw = 0, rw = 0;
     long long n_vox = 0, n_active = 0, n_rec = 0, n_boundary = 0;
+    unsigned long long n_fstaged = 0, fstage_want = 0; // face records staged by the count pass (and the most seen)
+    bool face_staged = false;                         // all of them fitted: the fill pass need not redo the tests
     int finished = 0;
     long long launches = 0; // kernels this library launched (its own, not CUB's)
     bool profiling = false;
@@ -1671,7 +1733,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
                 &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist};
+                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
@@ -1821,6 +1883,8 @@ GenArgs make_gen(ovx_fdg_context *ctx)
     A.rec = (Rec *)ctx->rec.p;
     A.qtab = (float *)ctx->qtab.p;
     A.btab = (float *)ctx->btab.p;
+    A.fstage = (uint4 *)ctx->fstage.p;
+    A.fstage_cap = cap_u32(ctx->fstage, sizeof(uint4));
     A.counters = (uint32_t *)ctx->counters.p;
     A.scan_large = (uint32_t *)ctx->scan_large.p;
     A.scan_large_cap = cap_u32(ctx->scan_large, 4);
@@ -1848,9 +1912,22 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
 {
     if (ctx->fw > 0.0f && ctx->nf > 0)
     {
-        face_records<M, IdxT><<<blocks_for(ctx->nf, kFaceThreads), kFaceThreads, 0, st>>>(A);
+        if (M == FILL && ctx->face_staged)
+        {
+            if (ctx->n_fstaged > 0)
+            {
+                bucket_records<<<blocks_for((long long)ctx->n_fstaged, kThreads), kThreads, 0, st>>>(
+                    A.fstage, (uint32_t)ctx->n_fstaged, A.rcnt, A.roff, A.rec, A.counters);
+                ++ctx->launches;
+            }
+        }
+        else
+        {
+            face_records<M, IdxT><<<blocks_for(ctx->nf, kFaceThreads), kFaceThreads, 0, st>>>(A);
+            ++ctx->launches;
+        }
         large_face_records<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
-        ctx->launches += 2;
+        ++ctx->launches;
     }
     if (ctx->bw > 0.0f && ctx->nf > 0)
     {
@@ -1879,6 +1956,13 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(ensure(ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
         OVX_CUDA(ensure(ctx->qtab, (size_t)(nf + 1) * 40));
+    if (full && ctx->fw > 0.0f)
+    {
+        // staging room for the face records: the most seen so far, else a guess
+        const unsigned long long guess = std::min(24ull * (unsigned long long)nf, 4ull * (unsigned long long)nf + (16ull << 20));
+        const unsigned long long want = std::max(ctx->fstage_want, guess);
+        OVX_CUDA(ensure(ctx->fstage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
+    }
     if (boundary)
     {
         OVX_CUDA(ensure(ctx->vcnt, (size_t)(ctx->nv + 1) * 4));
@@ -1975,6 +2059,9 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     ctx->n_active = (long long)ctx->host[1];
     ctx->n_rec = full ? (long long)ctx->host[2] : 0;
     ctx->n_boundary = hc[C_BOUNDARY];
+    ctx->n_fstaged = full ? hc[C_FSTAGED] : 0u;
+    ctx->face_staged = full && ctx->n_fstaged <= (unsigned long long)cap_u32(ctx->fstage, sizeof(uint4));
+    ctx->fstage_want = std::max(ctx->fstage_want, ctx->n_fstaged);
     *num_voxels = (int64_t)n;
     return OVX_FDG_OK;
 }
