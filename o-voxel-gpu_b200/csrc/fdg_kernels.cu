@@ -1388,8 +1388,6 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
         atomicOr(&A.counters[C_STATUS], S.status);
 }
 
-constexpr int kLocalSort = 64; // lists up to this length are ordered in thread-local memory
-
 // One thread per voxel row: order the voxel's contributions by key, sum them in
 // that order, regularise and solve (flexible_dual_grid.cpp:763-797); voxels
 // whose unconstrained solution leaves the box go to the constrained-search list.
@@ -1405,51 +1403,29 @@ __global__ void __launch_bounds__(128) voxel_accumulate(SolveArgs A, long long n
     uint4 *lst = A.contrib + first;
     Acc a;
     acc_init(a);
-    if (n <= (uint32_t)kLocalSort)
+    // insertion sort in place: the list is nearly sorted already (brick_lists
+    // fills it in bucket order), so this is close to one pass over it
+    for (uint32_t x = 1; x < n; ++x)
     {
-        unsigned long long key[kLocalSort];
-        uint32_t pay[kLocalSort];
-        for (uint32_t x = 0; x < n; ++x)
+        const uint4 e = lst[x];
+        const unsigned long long k = (unsigned long long)e.x | ((unsigned long long)e.y << 32);
+        uint32_t j = x;
+        while (j > 0)
         {
-            const uint4 e = lst[x];
-            const unsigned long long k = (unsigned long long)e.x | ((unsigned long long)e.y << 32);
-            uint32_t j = x;
-            while (j > 0 && key[j - 1] > k)
-            {
-                key[j] = key[j - 1];
-                pay[j] = pay[j - 1];
-                --j;
-            }
-            key[j] = k;
-            pay[j] = e.z;
+            const uint4 pe = lst[j - 1];
+            const unsigned long long pk = (unsigned long long)pe.x | ((unsigned long long)pe.y << 32);
+            if (pk <= k)
+                break;
+            lst[j] = pe;
+            --j;
         }
-        for (uint32_t x = 0; x < n; ++x)
-            acc_entry(A, vc, key[x], pay[x], a);
-    }
-    else
-    {
-        // long list (rare): insertion sort in place, then sum
-        for (uint32_t x = 1; x < n; ++x)
-        {
-            const uint4 e = lst[x];
-            const unsigned long long k = (unsigned long long)e.x | ((unsigned long long)e.y << 32);
-            uint32_t j = x;
-            while (j > 0)
-            {
-                const uint4 pe = lst[j - 1];
-                const unsigned long long pk = (unsigned long long)pe.x | ((unsigned long long)pe.y << 32);
-                if (pk <= k)
-                    break;
-                lst[j] = pe;
-                --j;
-            }
+        if (j != x)
             lst[j] = e;
-        }
-        for (uint32_t x = 0; x < n; ++x)
-        {
-            const uint4 e = lst[x];
-            acc_entry(A, vc, (unsigned long long)e.x | ((unsigned long long)e.y << 32), e.z, a);
-        }
+    }
+    for (uint32_t x = 0; x < n; ++x)
+    {
+        const uint4 e = lst[x];
+        acc_entry(A, vc, (unsigned long long)e.x | ((unsigned long long)e.y << 32), e.z, a);
     }
     float q[10];
     regularize(a.q, a.mean, a.cnt, A.rw, q);

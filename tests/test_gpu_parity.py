@@ -120,3 +120,45 @@ def test_bad_face_index_raises(cuda):
     # the context stays usable afterwards
     w = SMALL["dyadic_tilted"]
     assert_fdg_equal(_gpu_api(w, cuda), _oracle(w), "after error")
+
+
+def _face_heavy_workload():
+    """Eight medium, slightly tilted triangles at grid 128: each hits hundreds of
+    voxels in the face stage, far more than the library's first guess of face
+    records per triangle, while each face box spans at most 64 bricks."""
+    rng = np.random.default_rng(11)
+    verts, faces = [], []
+    for k in range(8):
+        c = rng.uniform(-0.25, 0.25, size=3)
+        a = np.array([0.0, 0.0, 0.0])
+        b = np.array([0.22, 0.01, 0.004])
+        d = np.array([0.02, 0.21, 0.008])
+        tri = np.stack([a, b, d]) - (a + b + d) / 3.0 + c
+        verts.append(tri)
+        faces.append(np.arange(3) + 3 * k)
+    return W.Workload("face_heavy", np.concatenate(verts).astype(np.float32), np.stack(faces).astype(np.int64),
+                      128, W.UNIT_AABB)
+
+
+@pytest.mark.gpu
+def test_face_record_staging_and_fallback(cuda):
+    """The first conversion on a fresh context overflows the staging array for
+    face records and re-runs the face tests in the fill pass; the second one
+    fits and buckets the staged records.  Both are bit-exact."""
+    import torch
+    import ovx_fdg_abi as abi
+
+    w = _face_heavy_workload()
+    want = _oracle(w)
+    _, _, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
+    ab = np.asarray(w.aabb, np.float32).reshape(2, 3)
+    ctx = abi.Context(cuda.index or 0)
+    try:
+        vt = torch.from_numpy(w.vertices).to(cuda)
+        ft = torch.from_numpy(w.faces).to(cuda)
+        for step in ("fill pass", "staged"):
+            out = ctx.mesh_to_fdg(vt, ft, ab[0], vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+            torch.cuda.synchronize()
+            assert_fdg_equal(tuple(t.cpu().numpy() for t in out), want, f"face_heavy ({step})")
+    finally:
+        ctx.close()
