@@ -1156,12 +1156,21 @@ __device__ __forceinline__ void acc_init(Acc &a)
     a.first = true;
 }
 
-// Add one contribution in reference order (flexible_dual_grid.cpp:251-271, :409, :521).
-__device__ __forceinline__ void acc_entry(const SolveArgs &A, const int vc[3], unsigned long long key, uint32_t pay, Acc &a)
+// One contribution decoded and loaded, ready to be added (flexible_dual_grid.cpp:251-271, :409, :521).
+struct Contrib
 {
-    const unsigned stage = (unsigned)(key >> 62);
-    float qt[10];
-    if (stage == 0)
+    float q[10];
+    float p[3];
+    uint32_t flag;
+    unsigned stage;
+};
+
+__device__ __forceinline__ void contrib_load(const SolveArgs &A, const int vc[3], unsigned long long key, uint32_t pay, Contrib &c)
+{
+    c.stage = (unsigned)(key >> 62);
+    c.flag = 0u;
+    c.p[0] = c.p[1] = c.p[2] = 0.0f;
+    if (c.stage == 0)
     {
         const unsigned long long ta = key >> 2;
         const long long t = (long long)(ta / 3ull);
@@ -1176,51 +1185,65 @@ __device__ __forceinline__ void acc_entry(const SolveArgs &A, const int vc[3], u
         const float pu = (float)(c0 - dx + 1) * vs0;
         const float pv = (float)(c1 - dy + 1) * vs1;
         const float pw = __uint_as_float(pay);
-        float p[3];
-        p[0] = ax2 == 0 ? pw : (ax2 == 1 ? pv : pu);
-        p[1] = ax2 == 0 ? pu : (ax2 == 1 ? pw : pv);
-        p[2] = ax2 == 0 ? pv : (ax2 == 1 ? pu : pw);
+        c.p[0] = ax2 == 0 ? pw : (ax2 == 1 ? pv : pu);
+        c.p[1] = ax2 == 0 ? pu : (ax2 == 1 ? pw : pv);
+        c.p[2] = ax2 == 0 ? pv : (ax2 == 1 ? pu : pw);
 #pragma unroll
         for (int i = 0; i < 10; ++i)
-            qt[i] = A.qtab[t * 10 + i];
-        if (a.first)
-        {
-            a.mean[0] = p[0];
-            a.mean[1] = p[1];
-            a.mean[2] = p[2];
-            a.cnt = 1.0f;
-#pragma unroll
-            for (int i = 0; i < 10; ++i)
-                a.q[i] = qt[i];
-            a.first = false;
-        }
-        else
-        {
-            a.mean[0] = a.mean[0] + p[0];
-            a.mean[1] = a.mean[1] + p[1];
-            a.mean[2] = a.mean[2] + p[2];
-            a.cnt = a.cnt + 1.0f;
-#pragma unroll
-            for (int i = 0; i < 10; ++i)
-                a.q[i] = a.q[i] + qt[i];
-        }
+            c.q[i] = A.qtab[t * 10 + i];
         if (dx == 0 && dy == 0)
-            a.flags |= 1u << ax2;
+            c.flag = 1u << ax2;
     }
-    else if (stage == 1)
+    else if (c.stage == 1)
     {
         const long long t = (long long)(key & ((1ull << 62) - 1ull));
 #pragma unroll
         for (int i = 0; i < 10; ++i)
-            a.q[i] = a.q[i] + A.qtab[t * 10 + i];
+            c.q[i] = A.qtab[t * 10 + i];
     }
     else
     {
-        // line quadric of boundary edge e, computed once by the boundary pass
+        // line quadric of boundary edge e (computed once by the boundary pass), weighted
         const float *bq = A.btab + (size_t)(key & 0xffffffffull) * 10;
 #pragma unroll
         for (int i = 0; i < 10; ++i)
-            a.q[i] = a.q[i] + A.bw * bq[i];
+            c.q[i] = A.bw * bq[i];
+    }
+}
+
+// Adds one contribution in reference order; the first one is copied (keeps signed zeros).
+__device__ __forceinline__ void contrib_apply(const Contrib &c, Acc &a)
+{
+    if (c.stage == 0)
+    {
+        if (a.first)
+        {
+            a.mean[0] = c.p[0];
+            a.mean[1] = c.p[1];
+            a.mean[2] = c.p[2];
+            a.cnt = 1.0f;
+#pragma unroll
+            for (int i = 0; i < 10; ++i)
+                a.q[i] = c.q[i];
+            a.first = false;
+        }
+        else
+        {
+            a.mean[0] = a.mean[0] + c.p[0];
+            a.mean[1] = a.mean[1] + c.p[1];
+            a.mean[2] = a.mean[2] + c.p[2];
+            a.cnt = a.cnt + 1.0f;
+#pragma unroll
+            for (int i = 0; i < 10; ++i)
+                a.q[i] = a.q[i] + c.q[i];
+        }
+        a.flags |= c.flag;
+    }
+    else
+    {
+#pragma unroll
+        for (int i = 0; i < 10; ++i)
+            a.q[i] = a.q[i] + c.q[i];
     }
 }
 
@@ -1391,41 +1414,100 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
 // One thread per voxel row: order the voxel's contributions by key, sum them in
 // that order, regularise and solve (flexible_dual_grid.cpp:763-797); voxels
 // whose unconstrained solution leaves the box go to the constrained-search list.
+__device__ __forceinline__ unsigned long long entry_key(const uint4 &e)
+{
+    return (unsigned long long)e.x | ((unsigned long long)e.y << 32);
+}
+
+__device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src)
+{
+    const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src);
+    const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src);
+    return (unsigned long long)lo | ((unsigned long long)hi << 32);
+}
+
+#ifndef OVX_FDG_WARP_SORT_MIN
+#define OVX_FDG_WARP_SORT_MIN 16
+#endif
+constexpr int kWarpSortMin = OVX_FDG_WARP_SORT_MIN; // lists this long or longer are ordered by the whole warp
+
 __global__ void __launch_bounds__(128) voxel_accumulate(SolveArgs A, long long nrows)
 {
     const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= nrows)
-        return;
-    const unsigned long long d = A.vlist[row];
+    const int lane = threadIdx.x & 31;
+    const bool valid = row < nrows;
+    const unsigned long long d = valid ? A.vlist[row] : 0ull;
     const unsigned long long first = d & ((1ull << 40) - 1ull);
     const uint32_t n = (uint32_t)(d >> 40);
+    // The warp orders the longer lists of its 32 voxels one after another: each
+    // lane holds up to two entries of the list and finds its rank among the
+    // list's (unique) keys, then stores the entry at that rank.
+    for (int v = 0; v < 32; ++v)
+    {
+        const uint32_t nv = __shfl_sync(0xffffffffu, n, v);
+        const unsigned long long fv = __shfl_sync(0xffffffffu, first, v);
+        if (nv < (uint32_t)kWarpSortMin || nv > 64u)
+            continue;
+        uint4 *L = A.contrib + fv;
+        const uint4 pad = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+        const uint4 e0 = (uint32_t)lane < nv ? L[lane] : pad;
+        const uint4 e1 = (uint32_t)lane + 32u < nv ? L[lane + 32] : pad;
+        const unsigned long long k0 = entry_key(e0), k1 = entry_key(e1);
+        uint32_t r0 = 0, r1 = 0;
+        const uint32_t n0 = nv < 32u ? nv : 32u;
+        // (keys are unique per voxel; ties, which cannot occur, would keep list order)
+        for (uint32_t j = 0; j < n0; ++j)
+        {
+            const unsigned long long kj = shfl_u64(k0, (int)j);
+            r0 += kj < k0 || (kj == k0 && j < (uint32_t)lane);
+            r1 += kj <= k1;
+        }
+        for (uint32_t j = 32; j < nv; ++j)
+        {
+            const unsigned long long kj = shfl_u64(k1, (int)(j - 32));
+            r0 += kj < k0;
+            r1 += kj < k1 || (kj == k1 && j < (uint32_t)lane + 32u);
+        }
+        __syncwarp();
+        if ((uint32_t)lane < nv)
+            L[r0] = e0;
+        if ((uint32_t)lane + 32u < nv)
+            L[r1] = e1;
+    }
+    __syncwarp();
+    if (!valid)
+        return;
     const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
     uint4 *lst = A.contrib + first;
+    if (n < (uint32_t)kWarpSortMin || n > 64u)
+    {
+        // short lists (nearly sorted already: brick_lists fills them in bucket
+        // order) and very long ones (rare): insertion sort in place
+        for (uint32_t x = 1; x < n; ++x)
+        {
+            const uint4 e = lst[x];
+            const unsigned long long k = entry_key(e);
+            uint32_t j = x;
+            while (j > 0)
+            {
+                const uint4 pe = lst[j - 1];
+                if (entry_key(pe) <= k)
+                    break;
+                lst[j] = pe;
+                --j;
+            }
+            if (j != x)
+                lst[j] = e;
+        }
+    }
     Acc a;
     acc_init(a);
-    // insertion sort in place: the list is nearly sorted already (brick_lists
-    // fills it in bucket order), so this is close to one pass over it
-    for (uint32_t x = 1; x < n; ++x)
-    {
-        const uint4 e = lst[x];
-        const unsigned long long k = (unsigned long long)e.x | ((unsigned long long)e.y << 32);
-        uint32_t j = x;
-        while (j > 0)
-        {
-            const uint4 pe = lst[j - 1];
-            const unsigned long long pk = (unsigned long long)pe.x | ((unsigned long long)pe.y << 32);
-            if (pk <= k)
-                break;
-            lst[j] = pe;
-            --j;
-        }
-        if (j != x)
-            lst[j] = e;
-    }
     for (uint32_t x = 0; x < n; ++x)
     {
         const uint4 e = lst[x];
-        acc_entry(A, vc, (unsigned long long)e.x | ((unsigned long long)e.y << 32), e.z, a);
+        Contrib c;
+        contrib_load(A, vc, entry_key(e), e.z, c);
+        contrib_apply(c, a);
     }
     float q[10];
     regularize(a.q, a.mean, a.cnt, A.rw, q);
