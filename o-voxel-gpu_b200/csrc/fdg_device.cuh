@@ -226,8 +226,15 @@ __device__ __forceinline__ void axis_col_bounds(const AxisScan &s, const Grid &g
 
 // Events of one scan row, columns restricted to [col_lo, col_hi).
 // emit(xi, yi, zi, x_float, y_float, z_double) in (ax0, ax1, ax2) order.
-template <typename Emit>
-__device__ __forceinline__ void scan_row(const AxisScan &s, int yi, int col_lo, int col_hi, const Grid &g, Emit &emit)
+// One scanline row yi of a projection axis (flexible_dual_grid.cpp:219-236):
+// the two edge crossings (t3, t4), sorted along x, and the column range.
+struct RowSetup
+{
+    double t3x, t3z, t4x, t4z;
+    int x0, x1; // columns xi in [x0, x1)
+};
+
+__device__ __forceinline__ void row_setup(const AxisScan &s, int yi, int col_lo, int col_hi, const Grid &g, RowSetup &r)
 {
     const bool first = yi < s.mid;
     const double *T0 = first ? s.t[0] : s.t[2];
@@ -273,25 +280,43 @@ __device__ __forceinline__ void scan_row(const AxisScan &s, int yi, int col_lo, 
     const double rx = g.rv[s.ax0];
     const int ls = clampi(trunc_div(t3x, vx, rx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
     const int le = clampi(trunc_div(t4x, vx, rx), g.gmin[s.ax0], g.gmax[s.ax0] - 1);
-    const int x0 = ls > col_lo ? ls : col_lo;
-    const int x1 = le < col_hi ? le : col_hi;
-    const double vz = (double)g.vs[s.ax2];
-    const double rz = g.rv[s.ax2];
-    for (int xi = x0; xi < x1; ++xi)
+    r.t3x = t3x;
+    r.t3z = t3z;
+    r.t4x = t4x;
+    r.t4z = t4z;
+    r.x0 = ls > col_lo ? ls : col_lo;
+    r.x1 = le < col_hi ? le : col_hi;
+}
+
+// Crossing of column xi with a row (flexible_dual_grid.cpp:238-250): its z and
+// voxel index zi along the projection axis.
+__device__ __forceinline__ void col_event(const RowSetup &r, int xi, int ax0, int ax2, const Grid &g, double &z, int &zi)
+{
+    const float xf = (float)(xi + 1) * g.vs[ax0];
+    const double x = (double)xf;
+    if (r.t3x == r.t4x)
+        z = r.t3z;
+    else
     {
-        const float xf = (float)(xi + 1) * g.vs[s.ax0];
-        const double x = (double)xf;
+        const double al = (x - r.t3x) / (r.t4x - r.t3x);
+        z = (1.0 - al) * r.t3z + al * r.t4z;
+    }
+    zi = trunc_div(z, (double)g.vs[ax2], g.rv[ax2]);
+}
+
+template <typename Emit>
+__device__ __forceinline__ void scan_row(const AxisScan &s, int yi, int col_lo, int col_hi, const Grid &g, Emit &emit)
+{
+    RowSetup r;
+    row_setup(s, yi, col_lo, col_hi, g, r);
+    const float yf = (float)(yi + 1) * g.vs[s.ax1];
+    for (int xi = r.x0; xi < r.x1; ++xi)
+    {
         double z;
-        if (t3x == t4x)
-            z = t3z;
-        else
-        {
-            const double al = (x - t3x) / (t4x - t3x);
-            z = (1.0 - al) * t3z + al * t4z;
-        }
-        const int zi = trunc_div(z, vz, rz);
+        int zi;
+        col_event(r, xi, s.ax0, s.ax2, g, z, zi);
         if (zi >= g.gmin[s.ax2] && zi < g.gmax[s.ax2])
-            emit(xi, yi, zi, xf, yf, z);
+            emit(xi, yi, zi, (float)(xi + 1) * g.vs[s.ax0], yf, z);
     }
 }
 

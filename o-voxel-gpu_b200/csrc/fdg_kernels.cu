@@ -68,7 +68,6 @@ using namespace ovx;
 namespace
 {
 
-constexpr int kInlineScanWork = 256;  // rows x column span of one (triangle, axis) rasterised by one thread
 constexpr int kInlineFaceBricks = 64; // face boxes over more bricks go to the CTA-per-triangle path
 constexpr int kChunk = 8;             // columns per tile for large (triangle, axis) pairs
 constexpr int kThreads = 256;
@@ -292,53 +291,178 @@ struct EventSink
     }
 };
 
-template <int M, typename IdxT>
-__global__ void __launch_bounds__(kThreads) tri_events(GenArgs A)
+constexpr int kEventThreads = 128;   // scanline pass: one (triangle, axis) per lane
+constexpr int kWarpScanWork = 4096;  // (triangle, axis) pairs with more row x column work go to large_events
+
+struct EventWarp
 {
-    // one thread per (triangle, projection axis)
-    const long long ta = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ta >= 3 * A.m.nf)
-        return;
-    const long long t = ta / 3;
-    const int ax2 = (int)(ta - 3 * t);
-    float v[3][3];
-    if (!tri_load<IdxT>(A.m, t, v))
-    {
-        if (M == COUNT)
-            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_BAD_INDEX);
-        return;
-    }
-    if (M == COUNT && ax2 == 0 && A.qtab)
-    {
-        float q[10];
-        tri_quadric(v, q);
+    double t[3][3][32]; // sorted vertices (projection coordinates) of each lane's (triangle, axis)
+    int start[32], mid[32];
+};
+
+// Largest lane l with v(l) <= x, for v non-decreasing over the lanes (x >= v(0)).
+__device__ __forceinline__ int owner_lane(uint32_t v, uint32_t x)
+{
+    int l = 0;
 #pragma unroll
-        for (int i = 0; i < 10; ++i)
-            A.qtab[t * 10 + i] = q[i];
-    }
-    AxisScan s;
-    axis_setup(v, ax2, A.m.g, s);
-    const int rows = s.end - s.start;
-    if (rows <= 0)
-        return;
-    int clo, chi;
-    axis_col_bounds(s, A.m.g, clo, chi);
-    if ((long long)rows * (long long)(chi - clo + 1) > kInlineScanWork)
+    for (int step = 16; step >= 1; step >>= 1)
     {
-        if (M == COUNT)
-        {
-            const uint32_t slot = atomicAdd(&A.counters[C_SCAN_LARGE], 1u);
-            if (slot < A.scan_large_cap)
-                A.scan_large[slot] = (uint32_t)ta;
-            else
-                atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
-        }
-        return;
+        const int c = l + step;
+        const uint32_t vc = __shfl_sync(0xffffffffu, v, c & 31);
+        if (c < 32 && vc <= x)
+            l = c;
     }
-    EventSink<M> sink{A, (uint32_t)t, ax2};
-#pragma unroll 1
-    for (int yi = s.start; yi < s.end; ++yi)
-        scan_row(s, yi, INT_MIN, INT_MAX, A.m.g, sink);
+    return l;
+}
+
+__device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t x, uint32_t &total)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t incl = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d)
+            incl += y;
+    }
+    total = __shfl_sync(0xffffffffu, incl, 31);
+    return incl - x;
+}
+
+// Scanline events (flexible_dual_grid.cpp:195-283), one (triangle, axis) per
+// lane.  The rows of the warp's 32 pairs are spread over the lanes 32 at a
+// time, and the column crossings of those rows again 32 at a time, so the FP64
+// event arithmetic runs on full warps whatever the triangles' sizes.  COUNT
+// marks the occupancy bits and counts event records per brick (and writes the
+// quadric table); FILL writes the records.
+template <int M, typename IdxT>
+__global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
+{
+    __shared__ EventWarp EW[kEventThreads / 32];
+    const int lane = threadIdx.x & 31;
+    EventWarp &E = EW[threadIdx.x >> 5];
+    const long long ta = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long tabase = ta - lane;
+    const Grid &g = A.m.g;
+    uint32_t nrows = 0;
+    if (ta < 3 * A.m.nf)
+    {
+        const long long t = ta / 3;
+        const int ax2 = (int)(ta - 3 * t);
+        float v[3][3];
+        if (!tri_load<IdxT>(A.m, t, v))
+        {
+            if (M == COUNT)
+                atomicOr(&A.counters[C_STATUS], (uint32_t)ST_BAD_INDEX);
+        }
+        else
+        {
+            if (M == COUNT && ax2 == 0 && A.qtab)
+            {
+                float q[10];
+                tri_quadric(v, q);
+#pragma unroll
+                for (int i = 0; i < 10; ++i)
+                    A.qtab[t * 10 + i] = q[i];
+            }
+            AxisScan s;
+            axis_setup(v, ax2, g, s);
+            const int rows = s.end - s.start;
+            if (rows > 0)
+            {
+                int clo, chi;
+                axis_col_bounds(s, g, clo, chi);
+                if ((long long)rows * (long long)(chi - clo + 1) > kWarpScanWork)
+                {
+                    if (M == COUNT)
+                    {
+                        const uint32_t slot = atomicAdd(&A.counters[C_SCAN_LARGE], 1u);
+                        if (slot < A.scan_large_cap)
+                            A.scan_large[slot] = (uint32_t)ta;
+                        else
+                            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            E.t[k][c][lane] = s.t[k][c];
+                    E.start[lane] = s.start;
+                    E.mid[lane] = s.mid;
+                    nrows = (uint32_t)rows;
+                }
+            }
+        }
+    }
+    uint32_t nrow_all;
+    const uint32_t rstart = warp_exclusive_scan(nrows, nrow_all);
+    __syncwarp();
+    for (uint32_t rb = 0; rb < nrow_all; rb += 32)
+    {
+        // this lane's row: owner pair ol, row yi
+        const uint32_t r = rb + (uint32_t)lane;
+        const int ol = owner_lane(rstart, r);
+        const uint32_t ors = __shfl_sync(0xffffffffu, rstart, ol);
+        const int oax2 = (int)((tabase + ol) % 3);
+        RowSetup rs;
+        rs.t3x = rs.t3z = rs.t4x = rs.t4z = 0.0;
+        rs.x0 = rs.x1 = 0;
+        int yi = 0;
+        if (r < nrow_all)
+        {
+            AxisScan s;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    s.t[k][c] = E.t[k][c][ol];
+            s.start = E.start[ol];
+            s.mid = E.mid[ol];
+            s.end = 0;
+            s.ax2 = oax2;
+            s.ax0 = (oax2 + 1) % 3;
+            s.ax1 = (oax2 + 2) % 3;
+            yi = s.start + (int)(r - ors);
+            row_setup(s, yi, INT_MIN, INT_MAX, g, rs);
+        }
+        const uint32_t ncol = rs.x1 > rs.x0 ? (uint32_t)(rs.x1 - rs.x0) : 0u;
+        uint32_t ncol_all;
+        const uint32_t cstart = warp_exclusive_scan(ncol, ncol_all);
+        for (uint32_t cb = 0; cb < ncol_all; cb += 32)
+        {
+            // this lane's column crossing: owner row lane rl
+            const uint32_t c = cb + (uint32_t)lane;
+            const int rl = owner_lane(cstart, c);
+            RowSetup cr;
+            cr.t3x = __shfl_sync(0xffffffffu, rs.t3x, rl);
+            cr.t3z = __shfl_sync(0xffffffffu, rs.t3z, rl);
+            cr.t4x = __shfl_sync(0xffffffffu, rs.t4x, rl);
+            cr.t4z = __shfl_sync(0xffffffffu, rs.t4z, rl);
+            cr.x0 = __shfl_sync(0xffffffffu, rs.x0, rl);
+            cr.x1 = 0;
+            const int cyi = __shfl_sync(0xffffffffu, yi, rl);
+            const int col = __shfl_sync(0xffffffffu, ol, rl);
+            const uint32_t ccs = __shfl_sync(0xffffffffu, cstart, rl);
+            if (c < ncol_all)
+            {
+                const long long cta = tabase + col;
+                const int cax2 = (int)(cta % 3);
+                const int xi = cr.x0 + (int)(c - ccs);
+                double z;
+                int zi;
+                col_event(cr, xi, (cax2 + 1) % 3, cax2, g, z, zi);
+                if (zi >= g.gmin[cax2] && zi < g.gmax[cax2])
+                {
+                    EventSink<M> sink{A, (uint32_t)(cta / 3), cax2};
+                    sink(xi, cyi, zi, 0.0f, 0.0f, z);
+                }
+            }
+        }
+    }
 }
 
 // One CTA per listed (triangle, axis); threads over (row, column chunk) tiles.
@@ -1958,7 +2082,7 @@ void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
 {
     if (ctx->nf > 0)
     {
-        tri_events<M, IdxT><<<blocks_for(3 * ctx->nf, kThreads), kThreads, 0, st>>>(A);
+        tri_events<M, IdxT><<<blocks_for(3 * ctx->nf, kEventThreads), kEventThreads, 0, st>>>(A);
         ++ctx->launches;
     }
     large_events<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
