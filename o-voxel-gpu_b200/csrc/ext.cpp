@@ -10,7 +10,11 @@
 //
 // plus `mesh_to_flexible_dual_grid_cuda_ex`, which takes unshifted vertices,
 // the aabb origin and int32 or int64 faces so the wrapper does not need the
-// extra cast and shift passes over the inputs.
+// extra cast and shift passes over the inputs, and
+// `mesh_to_flexible_dual_grid_cuda_batch`, which converts a list of meshes
+// (each with its own grid) with a pool of host worker threads, each owning a
+// library context and a CUDA stream, so that one mesh's host synchronisation,
+// output allocation and small launches overlap the other meshes' GPU work.
 //
 // All compute goes through the C ABI in include/ovx_fdg.h (libovx_fdg.so).
 // Setting OVX_FDG_CHECK in the environment makes every call wait for its
@@ -22,10 +26,16 @@
 #include <ATen/cuda/CUDAContext.h>
 #include <c10/cuda/CUDAGuard.h>
 
+#include <c10/cuda/CUDAStream.h>
+
+#include <atomic>
 #include <cstdlib>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "ovx_fdg.h"
 
@@ -115,6 +125,23 @@ std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Ten
     return std::make_tuple(vox, dual, inter);
 }
 
+// Worker contexts of the batched path: one per (device, worker slot), kept for
+// the life of the process like the single-mesh context.
+DeviceContext &worker_context(int device, int slot)
+{
+    static std::mutex map_mu;
+    static std::map<std::pair<int, int>, std::unique_ptr<DeviceContext>> contexts;
+    std::lock_guard<std::mutex> lock(map_mu);
+    auto &ptr = contexts[{device, slot}];
+    if (!ptr)
+    {
+        ptr = std::make_unique<DeviceContext>();
+        const int rc = ovx_fdg_context_create(device, &ptr->ctx);
+        TORCH_CHECK(rc == OVX_FDG_OK, "ovx_fdg_context_create failed: ", ovx_fdg_status_string(rc));
+    }
+    return *ptr;
+}
+
 } // namespace
 
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> mesh_to_flexible_dual_grid_cuda(
@@ -155,9 +182,118 @@ torch::Tensor intersect_occ_cuda(const torch::Tensor &triangles, const std::vect
     return vox;
 }
 
+std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_flexible_dual_grid_cuda_batch(
+    const std::vector<torch::Tensor> &vertices, const std::vector<torch::Tensor> &faces,
+    const std::vector<std::vector<float>> &origins, const std::vector<std::vector<float>> &voxel_sizes,
+    const std::vector<std::vector<int64_t>> &grid_ranges, float face_weight, float boundary_weight,
+    float regularization_weight, int64_t workers)
+{
+    const size_t n = vertices.size();
+    TORCH_CHECK(faces.size() == n && origins.size() == n && voxel_sizes.size() == n && grid_ranges.size() == n,
+                "mesh_to_flexible_dual_grid_batch: per-mesh argument lists differ in length");
+    std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> out(n);
+    if (n == 0)
+        return out;
+    const c10::Device dev = vertices[0].device();
+    for (size_t i = 0; i < n; ++i)
+    {
+        TORCH_CHECK(vertices[i].is_cuda() && faces[i].is_cuda(), "mesh ", i, ": vertices and faces must be CUDA tensors");
+        TORCH_CHECK(vertices[i].device() == dev && faces[i].device() == dev, "mesh ", i, ": all meshes must be on one device");
+        TORCH_CHECK(vertices[i].scalar_type() == torch::kFloat32, "mesh ", i, ": vertices must be float32");
+        TORCH_CHECK(faces[i].scalar_type() == torch::kInt32 || faces[i].scalar_type() == torch::kInt64,
+                    "mesh ", i, ": faces must be int32 or int64");
+        TORCH_CHECK(vertices[i].dim() == 2 && vertices[i].size(1) == 3, "mesh ", i, ": vertices must be [V,3]");
+        TORCH_CHECK(faces[i].dim() == 2 && faces[i].size(1) == 3, "mesh ", i, ": faces must be [F,3]");
+        TORCH_CHECK(origins[i].size() == 3, "mesh ", i, ": origin must have 3 elements");
+    }
+    const c10::cuda::CUDAGuard guard(dev);
+    const int device = dev.index();
+    const int nw = (int)std::max<int64_t>(1, std::min<int64_t>(workers, (int64_t)n));
+    c10::cuda::CUDAStream caller = at::cuda::getCurrentCUDAStream(device);
+    // the workers' streams first wait for the work already queued on the caller's stream
+    cudaEvent_t ready;
+    TORCH_CHECK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) == cudaSuccess, "cudaEventCreate failed");
+    cudaEventRecord(ready, caller.stream());
+    std::atomic<size_t> next{0};
+    std::atomic<bool> failed{false};
+    std::mutex err_mu;
+    std::string err;
+    std::vector<c10::cuda::CUDAStream> streams;
+    for (int w = 0; w < nw; ++w)
+        streams.push_back(c10::cuda::getStreamFromPool(false, device));
+    auto work = [&](int w) {
+        try
+        {
+            const c10::cuda::CUDAGuard g(dev);
+            const c10::cuda::CUDAStreamGuard sg(streams[w]);
+            cudaStream_t st = streams[w].stream();
+            cudaStreamWaitEvent(st, ready, 0);
+            DeviceContext &dc = worker_context(device, w);
+            std::lock_guard<std::mutex> lock(dc.mu);
+            for (;;)
+            {
+                const size_t i = next.fetch_add(1);
+                if (i >= n || failed.load())
+                    break;
+                const ovx_fdg_grid grid = make_grid(voxel_sizes[i], grid_ranges[i]);
+                auto v = vertices[i].contiguous();
+                auto f = faces[i].contiguous();
+                const float o[3] = {origins[i][0], origins[i][1], origins[i][2]};
+                int64_t nv = 0;
+                check(ovx_fdg_begin(dc.ctx, st, v.data_ptr<float>(), v.size(0), f.numel() ? f.data_ptr() : nullptr,
+                                    f.scalar_type() == torch::kInt64 ? 8 : 4, f.size(0), o, &grid, face_weight,
+                                    boundary_weight, regularization_weight, &nv),
+                      dc.ctx, "mesh_to_flexible_dual_grid_batch (occupancy)");
+                auto opts = torch::TensorOptions().device(dev);
+                auto vox = torch::empty({nv, 3}, opts.dtype(torch::kInt32));
+                auto dual = torch::empty({nv, 3}, opts.dtype(torch::kFloat32));
+                auto inter = torch::empty({nv, 3}, opts.dtype(torch::kBool));
+                check(ovx_fdg_finish(dc.ctx, st, nv ? vox.data_ptr<int32_t>() : nullptr, nv ? dual.data_ptr<float>() : nullptr,
+                                     nv ? reinterpret_cast<uint8_t *>(inter.data_ptr<bool>()) : nullptr),
+                      dc.ctx, "mesh_to_flexible_dual_grid_batch (quadrics)");
+                // the outputs are handed to the caller's stream
+                vox.record_stream(caller);
+                dual.record_stream(caller);
+                inter.record_stream(caller);
+                out[i] = std::make_tuple(vox, dual, inter);
+            }
+            static const bool sync_check = std::getenv("OVX_FDG_CHECK") != nullptr;
+            if (sync_check)
+                check(ovx_fdg_sync_status(dc.ctx, st), dc.ctx, "mesh_to_flexible_dual_grid_batch (device checks)");
+        }
+        catch (const std::exception &e)
+        {
+            failed.store(true);
+            std::lock_guard<std::mutex> lock(err_mu);
+            if (err.empty())
+                err = e.what();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < nw; ++w)
+        pool.emplace_back(work, w);
+    work(0);
+    for (auto &t : pool)
+        t.join();
+    // the caller's stream waits for every worker's queued work
+    for (int w = 0; w < nw; ++w)
+    {
+        cudaEvent_t done;
+        cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+        cudaEventRecord(done, streams[w].stream());
+        cudaStreamWaitEvent(caller.stream(), done, 0);
+        cudaEventDestroy(done);
+    }
+    cudaEventDestroy(ready);
+    TORCH_CHECK(!failed.load(), err);
+    return out;
+}
+
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
 {
     m.def("mesh_to_flexible_dual_grid_cuda", &mesh_to_flexible_dual_grid_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("mesh_to_flexible_dual_grid_cuda_ex", &mesh_to_flexible_dual_grid_cuda_ex, py::call_guard<py::gil_scoped_release>());
     m.def("intersect_occ_cuda", &intersect_occ_cuda, py::call_guard<py::gil_scoped_release>());
+    m.def("mesh_to_flexible_dual_grid_cuda_batch", &mesh_to_flexible_dual_grid_cuda_batch,
+          py::call_guard<py::gil_scoped_release>());
 }

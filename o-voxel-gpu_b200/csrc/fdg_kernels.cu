@@ -82,6 +82,8 @@ enum
     C_STATUS = 3,
     C_CONSTRAINED = 4,
     C_FSTAGED = 5,
+    C_LONG = 6,
+    C_HUGE = 7,
     C_WORDS = 8
 };
 enum
@@ -1220,6 +1222,9 @@ struct SolveArgs
     uint8_t *flags;
     uint32_t *counters;
     uint4 *contrib;             // per-voxel contribution lists {key lo, key hi, payload, 0}
+    uint32_t *longv;            // rows whose lists are too long for voxel_accumulate: up to kLongMidMax
+                                // entries from the front (counter C_LONG), longer ones from the back (C_HUGE)
+    uint32_t longv_cap;
     unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40
     float *clist; // deferred constrained searches, 16 words each
     uint32_t clist_cap;
@@ -1550,89 +1555,10 @@ __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int
     return (unsigned long long)lo | ((unsigned long long)hi << 32);
 }
 
-#ifndef OVX_FDG_WARP_SORT_MIN
-#define OVX_FDG_WARP_SORT_MIN 16
-#endif
-constexpr int kWarpSortMin = OVX_FDG_WARP_SORT_MIN; // lists this long or longer are ordered by the whole warp
-
-__global__ void __launch_bounds__(128) voxel_accumulate(SolveArgs A, long long nrows)
+// Regularise and solve one voxel (flexible_dual_grid.cpp:763-797); a voxel whose
+// unconstrained solution leaves its box goes to the constrained-search list.
+__device__ __forceinline__ void voxel_finish(const SolveArgs &A, long long row, const int vc[3], const Acc &a)
 {
-    const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    const bool valid = row < nrows;
-    const unsigned long long d = valid ? A.vlist[row] : 0ull;
-    const unsigned long long first = d & ((1ull << 40) - 1ull);
-    const uint32_t n = (uint32_t)(d >> 40);
-    // The warp orders the longer lists of its 32 voxels one after another: each
-    // lane holds up to two entries of the list and finds its rank among the
-    // list's (unique) keys, then stores the entry at that rank.
-    for (int v = 0; v < 32; ++v)
-    {
-        const uint32_t nv = __shfl_sync(0xffffffffu, n, v);
-        const unsigned long long fv = __shfl_sync(0xffffffffu, first, v);
-        if (nv < (uint32_t)kWarpSortMin || nv > 64u)
-            continue;
-        uint4 *L = A.contrib + fv;
-        const uint4 pad = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
-        const uint4 e0 = (uint32_t)lane < nv ? L[lane] : pad;
-        const uint4 e1 = (uint32_t)lane + 32u < nv ? L[lane + 32] : pad;
-        const unsigned long long k0 = entry_key(e0), k1 = entry_key(e1);
-        uint32_t r0 = 0, r1 = 0;
-        const uint32_t n0 = nv < 32u ? nv : 32u;
-        // (keys are unique per voxel; ties, which cannot occur, would keep list order)
-        for (uint32_t j = 0; j < n0; ++j)
-        {
-            const unsigned long long kj = shfl_u64(k0, (int)j);
-            r0 += kj < k0 || (kj == k0 && j < (uint32_t)lane);
-            r1 += kj <= k1;
-        }
-        for (uint32_t j = 32; j < nv; ++j)
-        {
-            const unsigned long long kj = shfl_u64(k1, (int)(j - 32));
-            r0 += kj < k0;
-            r1 += kj < k1 || (kj == k1 && j < (uint32_t)lane + 32u);
-        }
-        __syncwarp();
-        if ((uint32_t)lane < nv)
-            L[r0] = e0;
-        if ((uint32_t)lane + 32u < nv)
-            L[r1] = e1;
-    }
-    __syncwarp();
-    if (!valid)
-        return;
-    const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
-    uint4 *lst = A.contrib + first;
-    if (n < (uint32_t)kWarpSortMin || n > 64u)
-    {
-        // short lists (nearly sorted already: brick_lists fills them in bucket
-        // order) and very long ones (rare): insertion sort in place
-        for (uint32_t x = 1; x < n; ++x)
-        {
-            const uint4 e = lst[x];
-            const unsigned long long k = entry_key(e);
-            uint32_t j = x;
-            while (j > 0)
-            {
-                const uint4 pe = lst[j - 1];
-                if (entry_key(pe) <= k)
-                    break;
-                lst[j] = pe;
-                --j;
-            }
-            if (j != x)
-                lst[j] = e;
-        }
-    }
-    Acc a;
-    acc_init(a);
-    for (uint32_t x = 0; x < n; ++x)
-    {
-        const uint4 e = lst[x];
-        Contrib c;
-        contrib_load(A, vc, entry_key(e), e.z, c);
-        contrib_apply(c, a);
-    }
     float q[10];
     regularize(a.q, a.mean, a.cnt, A.rw, q);
     float v[3];
@@ -1661,6 +1587,237 @@ __global__ void __launch_bounds__(128) voxel_accumulate(SolveArgs A, long long n
 #pragma unroll
     for (int i = 0; i < 10; ++i)
         c[4 + i] = q[i];
+}
+
+#ifndef OVX_FDG_WARP_SORT_MIN
+#define OVX_FDG_WARP_SORT_MIN 16
+#endif
+constexpr int kWarpSortMin = OVX_FDG_WARP_SORT_MIN; // lists this long or longer are ordered by the whole warp
+constexpr int kWarpSortPer = 2;                      // ... up to 2 entries per lane
+constexpr int kWarpSortMax = 32 * kWarpSortPer;      // longer lists go to voxel_accumulate_long
+constexpr int kLongMidMax = 1024;                    // ... one CTA of 128 threads, shared-memory sort
+constexpr int kLongHugeMax = 8192;                   // ... one CTA of 256 threads; longer: in-place insertion sort
+
+__global__ void __launch_bounds__(128) voxel_accumulate(SolveArgs A, long long nrows)
+{
+    const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = row < nrows;
+    const unsigned long long d = valid ? A.vlist[row] : 0ull;
+    const unsigned long long first = d & ((1ull << 40) - 1ull);
+    const uint32_t n = (uint32_t)(d >> 40);
+    // The warp orders the longer lists of its 32 voxels one after another: each
+    // lane holds up to kWarpSortPer entries of the list and finds their ranks
+    // among the list's (unique) keys, then stores the entries at those ranks.
+    for (int v = 0; v < 32; ++v)
+    {
+        const uint32_t nv = __shfl_sync(0xffffffffu, n, v);
+        const unsigned long long fv = __shfl_sync(0xffffffffu, first, v);
+        if (nv < (uint32_t)kWarpSortMin || nv > (uint32_t)kWarpSortMax)
+            continue;
+        uint4 *L = A.contrib + fv;
+        const uint4 pad = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
+        uint4 e[kWarpSortPer];
+        unsigned long long k[kWarpSortPer];
+        uint32_t r[kWarpSortPer];
+#pragma unroll
+        for (int q = 0; q < kWarpSortPer; ++q)
+        {
+            const uint32_t idx = (uint32_t)(lane + 32 * q);
+            e[q] = idx < nv ? L[idx] : pad;
+            k[q] = entry_key(e[q]);
+            r[q] = 0;
+        }
+        // rank = number of smaller keys (keys are unique per voxel; ties, which
+        // cannot occur, would keep list order)
+#pragma unroll
+        for (int sq = 0; sq < kWarpSortPer; ++sq)
+        {
+            if ((uint32_t)(32 * sq) >= nv)
+                break;
+            const uint32_t jn = nv - 32u * sq < 32u ? nv - 32u * sq : 32u;
+            for (uint32_t j = 0; j < jn; ++j)
+            {
+                const unsigned long long kj = shfl_u64(k[sq], (int)j);
+                const uint32_t jj = 32u * sq + j;
+#pragma unroll
+                for (int q = 0; q < kWarpSortPer; ++q)
+                    r[q] += kj < k[q] || (kj == k[q] && jj < (uint32_t)(lane + 32 * q));
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < kWarpSortPer; ++q)
+            if ((uint32_t)(lane + 32 * q) < nv)
+                L[r[q]] = e[q];
+    }
+    __syncwarp();
+    if (!valid)
+        return;
+    if (n > (uint32_t)kWarpSortMax)
+    {
+        // long list: left to voxel_accumulate_long (one CTA per voxel)
+        const bool huge = n > (uint32_t)kLongMidMax;
+        const uint32_t slot = atomicAdd(&A.counters[huge ? C_HUGE : C_LONG], 1u);
+        if (slot < A.longv_cap)
+        {
+            A.longv[huge ? A.longv_cap - 1u - slot : slot] = (uint32_t)row;
+            return;
+        }
+        atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+        return;
+    }
+    const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
+    uint4 *lst = A.contrib + first;
+    if (n < (uint32_t)kWarpSortMin)
+    {
+        // short lists (nearly sorted already: brick_lists fills them in bucket
+        // order): insertion sort in place
+        for (uint32_t x = 1; x < n; ++x)
+        {
+            const uint4 e = lst[x];
+            const unsigned long long k = entry_key(e);
+            uint32_t j = x;
+            while (j > 0)
+            {
+                const uint4 pe = lst[j - 1];
+                if (entry_key(pe) <= k)
+                    break;
+                lst[j] = pe;
+                --j;
+            }
+            if (j != x)
+                lst[j] = e;
+        }
+    }
+    Acc a;
+    acc_init(a);
+    for (uint32_t x = 0; x < n; ++x)
+    {
+        const uint4 e = lst[x];
+        Contrib c;
+        contrib_load(A, vc, entry_key(e), e.z, c);
+        contrib_apply(c, a);
+    }
+    voxel_finish(A, row, vc, a);
+}
+
+constexpr int kLongChunk = 256; // contributions staged per step of the sequential sum
+template <int kMax>
+constexpr size_t long_smem()
+{
+    return (size_t)kMax * 12 + (size_t)kLongChunk * sizeof(Contrib);
+}
+
+// One CTA per voxel with a long contribution list (coarse grids over dense
+// meshes): bitonic sort of the keys in shared memory, then the contributions
+// are loaded by all threads a chunk at a time and summed in order by one
+// thread.  Lists longer than kMax are insertion-sorted in place (slow,
+// correct).
+// kHuge = false: lists of up to kLongMidMax entries (front of longv); true: longer lists (back of longv).
+template <int kMax, int kThreadsT, bool kHuge>
+__global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
+{
+    extern __shared__ unsigned long long lsm[];
+    unsigned long long *key = lsm;
+    uint32_t *pay = reinterpret_cast<uint32_t *>(key + kMax);
+    Contrib *cb = reinterpret_cast<Contrib *>(pay + kMax);
+    const int tid = threadIdx.x;
+    const uint32_t nlong = min(A.counters[kHuge ? C_HUGE : C_LONG], A.longv_cap);
+    for (uint32_t li = blockIdx.x; li < nlong; li += gridDim.x)
+    {
+        const long long row = A.longv[kHuge ? A.longv_cap - 1u - li : li];
+        const unsigned long long d = A.vlist[row];
+        const unsigned long long first = d & ((1ull << 40) - 1ull);
+        const uint32_t n = (uint32_t)(d >> 40);
+        const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
+        uint4 *lst = A.contrib + first;
+        Acc a;
+        acc_init(a);
+        if (n <= (uint32_t)kMax)
+        {
+            uint32_t p2 = 1;
+            while (p2 < n)
+                p2 <<= 1;
+            for (uint32_t i = tid; i < p2; i += blockDim.x)
+            {
+                if (i < n)
+                {
+                    const uint4 e = lst[i];
+                    key[i] = entry_key(e);
+                    pay[i] = e.z;
+                }
+                else
+                {
+                    key[i] = ~0ull;
+                    pay[i] = 0u;
+                }
+            }
+            __syncthreads();
+            for (uint32_t k = 2; k <= p2; k <<= 1)
+                for (uint32_t j = k >> 1; j > 0; j >>= 1)
+                {
+                    for (uint32_t i = tid; i < p2; i += blockDim.x)
+                    {
+                        const uint32_t l = i ^ j;
+                        if (l > i)
+                        {
+                            const bool up = (i & k) == 0;
+                            const unsigned long long ki = key[i], kl = key[l];
+                            if ((ki > kl) == up)
+                            {
+                                key[i] = kl;
+                                key[l] = ki;
+                                const uint32_t t = pay[i];
+                                pay[i] = pay[l];
+                                pay[l] = t;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            for (uint32_t c0 = 0; c0 < n; c0 += kLongChunk)
+            {
+                const uint32_t cn = min((uint32_t)kLongChunk, n - c0);
+                for (uint32_t i = tid; i < cn; i += blockDim.x)
+                    contrib_load(A, vc, key[c0 + i], pay[c0 + i], cb[i]);
+                __syncthreads();
+                if (tid == 0)
+                    for (uint32_t i = 0; i < cn; ++i)
+                        contrib_apply(cb[i], a);
+                __syncthreads();
+            }
+        }
+        else if (tid == 0)
+        {
+            for (uint32_t x = 1; x < n; ++x)
+            {
+                const uint4 e = lst[x];
+                const unsigned long long k = entry_key(e);
+                uint32_t j = x;
+                while (j > 0)
+                {
+                    const uint4 pe = lst[j - 1];
+                    if (entry_key(pe) <= k)
+                        break;
+                    lst[j] = pe;
+                    --j;
+                }
+                if (j != x)
+                    lst[j] = e;
+            }
+            for (uint32_t x = 0; x < n; ++x)
+            {
+                const uint4 e = lst[x];
+                Contrib c;
+                contrib_load(A, vc, entry_key(e), e.z, c);
+                contrib_apply(c, a);
+            }
+        }
+        if (tid == 0)
+            voxel_finish(A, row, vc, a);
+        __syncthreads();
+    }
 }
 
 // Constrained search (faces, edges, corners of the voxel box) for the voxels
@@ -1885,7 +2042,7 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
     Buf vcnt, voff, emax, bkeys, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage;
+    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, longv;
     unsigned long long *host = nullptr; // pinned readback words
     std::string err;
     // state between begin and finish
@@ -1915,7 +2072,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
                 &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage};
+                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage, &c->longv};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
@@ -2471,6 +2628,8 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(ensure(ctx->clist, (size_t)(n + 1) * 16 * 4));
     OVX_CUDA(ensure(ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
     OVX_CUDA(ensure(ctx->vlist, (size_t)n * 8));
+    OVX_CUDA(ensure(ctx->longv, (size_t)(n + 1) * 4));
+    OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_LONG, 0, 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONSTRAINED, 0, 4, st));
 
@@ -2507,6 +2666,8 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.clist = (float *)ctx->clist.p;
     SA.contrib = (uint4 *)ctx->contrib.p;
     SA.vlist = (unsigned long long *)ctx->vlist.p;
+    SA.longv = (uint32_t *)ctx->longv.p;
+    SA.longv_cap = (uint32_t)(n + 1);
     SA.clist_cap = (uint32_t)(n + 1);
     if (ctx->n_active > 0)
     {
@@ -2515,7 +2676,11 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     }
     stage(ctx, EV_CONSUME, st);
     voxel_accumulate<<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
-    ++ctx->launches;
+    voxel_accumulate_long<kLongMidMax, 128, false><<<ctx->sms * 8, 128, long_smem<kLongMidMax>(), st>>>(SA);
+    OVX_CUDA(cudaFuncSetAttribute(voxel_accumulate_long<kLongHugeMax, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)long_smem<kLongHugeMax>()));
+    voxel_accumulate_long<kLongHugeMax, 256, true><<<ctx->sms * 2, 256, long_smem<kLongHugeMax>(), st>>>(SA);
+    ctx->launches += 3;
     stage(ctx, EV_SOLVE, st);
     constrained_solve<<<ctx->sms * 8, 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
                                                     ctx->g, dual_vertices);

@@ -16,7 +16,7 @@ Differences, all deliberate:
   * Output rows are in a deterministic brick order (8x8x8 bricks, x fastest),
     not in an arbitrary order.  Values are bit-identical to the reference CPU path.
 """
-from typing import Any, List, Optional, Tuple, Union
+from typing import Any, List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 import torch
@@ -27,6 +27,7 @@ ArrayLike = Union[List[Any], Tuple[Any, ...], np.ndarray, torch.Tensor]
 
 __all__ = [
     "mesh_to_flexible_dual_grid",
+    "mesh_to_flexible_dual_grid_batch",
     "intersect_occ",
 ]
 
@@ -213,3 +214,65 @@ def intersect_occ(
     vertices = vertices - aabb[0].reshape(1, 3)
     triangles = vertices[faces.to(dtype=torch.long)].contiguous()
     return _ext().intersect_occ_cuda(triangles, voxel_size_arg, grid_range_arg)
+
+
+@torch.no_grad()
+def mesh_to_flexible_dual_grid_batch(
+    meshes: Sequence[Tuple[torch.Tensor, torch.Tensor]],
+    voxel_size=None,
+    grid_size=None,
+    aabb=None,
+    face_weight: float = 1.0,
+    boundary_weight: float = 1.0,
+    regularization_weight: float = 0.1,
+    workers: int = 4,
+) -> List[Tuple[torch.Tensor, torch.Tensor, torch.Tensor]]:
+    """
+    Convert many meshes at once; returns one (voxel_indices, dual_vertices,
+    intersected) tuple per mesh, each exactly what mesh_to_flexible_dual_grid
+    returns for that mesh.
+
+    Args:
+        meshes: sequence of (vertices [V,3], faces [F,3]) CUDA tensors, all on one device.
+        voxel_size, grid_size, aabb: as in mesh_to_flexible_dual_grid, either one value
+            for every mesh or a list with one value per mesh (with exactly three
+            meshes a list of three numbers is one per-axis value: give per-mesh
+            sizes as three 3-element lists).
+        face_weight, boundary_weight, regularization_weight: shared by all meshes.
+        workers: host threads converting meshes concurrently, each with its own
+            CUDA stream; the results are ordered on the caller's current stream.
+
+    The reference has no batched form; this one exists so that many small and
+    mid-sized meshes keep the GPU busy while each mesh's single host
+    synchronisation (to learn its voxel count) happens.
+    """
+    n = len(meshes)
+
+    def per_mesh_list(x, shape_one):
+        # one value per mesh: a list/tuple of n values, unless it already has the
+        # shape of a single value (one 3-vector, one [[x0,y0,z0],[x1,y1,z1]] box)
+        if x is None or isinstance(x, (torch.Tensor, np.ndarray)) or not isinstance(x, (list, tuple)) or len(x) != n:
+            return False
+        return np.asarray(x, dtype=np.float64).shape != shape_one
+
+    def per_mesh(x, i, is_list):
+        return x[i] if is_list else x
+
+    vs_list = per_mesh_list(voxel_size, (3,)) if not isinstance(voxel_size, float) else False
+    gs_list = per_mesh_list(grid_size, (3,)) if not isinstance(grid_size, int) else False
+    ab_list = per_mesh_list(aabb, (2, 3))
+    verts, fcs, origins, vsizes, granges = [], [], [], [], []
+    for i, (v, f) in enumerate(meshes):
+        v, f, ab, ab_cpu, vs_arg, gr_arg = _grid_setup(v, f, per_mesh(voxel_size, i, vs_list),
+                                                      per_mesh(grid_size, i, gs_list), per_mesh(aabb, i, ab_list))
+        _require_cuda(v, "mesh_to_flexible_dual_grid_batch")
+        if ab_cpu is None:
+            ab_cpu = ab.detach().cpu()
+        verts.append(v)
+        fcs.append(f)
+        origins.append([float(x) for x in ab_cpu[0].tolist()])
+        vsizes.append(vs_arg)
+        granges.append(gr_arg)
+    return _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
+                                                        float(boundary_weight), float(regularization_weight),
+                                                        int(workers))

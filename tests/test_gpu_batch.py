@@ -1,0 +1,80 @@
+"""Batched conversion (mesh_to_flexible_dual_grid_batch): every mesh's result
+must equal the single-mesh API's (same rows, same order) and the oracle's."""
+import numpy as np
+import pytest
+
+import fdg_workloads as W
+from fdg_check import assert_fdg_equal
+from oracle import oracle as O
+
+
+_ORACLE = {}
+
+
+def _oracle(w, key):
+    if key not in _ORACLE:
+        r = O.run_workload(w)
+        _ORACLE[key] = (r.voxels, r.dual, r.intersected)
+    return _ORACLE[key]
+
+
+def _upload(ws, device):
+    import torch
+
+    return [(torch.from_numpy(w.vertices).to(device), torch.from_numpy(w.faces).to(device)) for w in ws]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("workers", [1, 4])
+def test_batch_matches_oracle_and_single(cuda, workers):
+    import torch
+    import o_voxel
+
+    ws = W.batch(seed=7, n_meshes=12, f_lo=500, f_hi=20_000, grids=(64, 128, 256))
+    meshes = _upload(ws, cuda)
+    kw = dict(face_weight=1.0, boundary_weight=0.2, regularization_weight=1e-2)
+    outs = o_voxel.convert.mesh_to_flexible_dual_grid_batch(
+        meshes, grid_size=[w.grid_size for w in ws], aabb=[w.aabb for w in ws], workers=workers, **kw)
+    torch.cuda.synchronize()
+    assert len(outs) == len(ws)
+    for w, (v, f), out in zip(ws, meshes, outs):
+        got = tuple(t.cpu().numpy() for t in out)
+        single = o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=w.grid_size, aabb=w.aabb, **kw)
+        for a, b in zip(got, single):
+            assert np.array_equal(a, b.cpu().numpy()), w.name
+        assert_fdg_equal(got, _oracle(w, ("batch7", w.name)), w.name)
+
+
+@pytest.mark.gpu
+def test_batch_shared_grid_and_empty(cuda):
+    import torch
+    import o_voxel
+
+    ws = [W.ico_cap(0), W.ico_cap(1), W.ico_cap(2)]
+    meshes = _upload(ws, cuda)
+    meshes.append((torch.zeros((0, 3), device=cuda), torch.zeros((0, 3), dtype=torch.int64, device=cuda)))
+    outs = o_voxel.convert.mesh_to_flexible_dual_grid_batch(meshes, grid_size=64, aabb=W.UNIT_AABB,
+                                                            boundary_weight=0.2, regularization_weight=1e-2)
+    torch.cuda.synchronize()
+    for w, out in zip(ws, outs[:3]):
+        r = O.run_workload(w)
+        assert_fdg_equal(tuple(t.cpu().numpy() for t in out), (r.voxels, r.dual, r.intersected), w.name)
+    assert all(t.shape[0] == 0 for t in outs[3])
+    assert o_voxel.convert.mesh_to_flexible_dual_grid_batch([], grid_size=64, aabb=W.UNIT_AABB) == []
+
+
+@pytest.mark.gpu
+def test_batch_error_is_raised(cuda):
+    import torch
+    import o_voxel
+
+    good = _upload([W.ico_cap(0)], cuda)[0]
+    bad = (torch.rand(4, 3, device=cuda) - 0.5, torch.tensor([[0, 1, 2], [1, 2, 9]], device=cuda))
+    with pytest.raises(RuntimeError, match="face index"):
+        o_voxel.convert.mesh_to_flexible_dual_grid_batch([good, bad, good], grid_size=32, aabb=W.UNIT_AABB, workers=2)
+    # the pool stays usable
+    outs = o_voxel.convert.mesh_to_flexible_dual_grid_batch([good], grid_size=64, aabb=W.UNIT_AABB,
+                                                            boundary_weight=0.2, regularization_weight=1e-2)
+    w = W.ico_cap(0)
+    r = O.run_workload(w)
+    assert_fdg_equal(tuple(t.cpu().numpy() for t in outs[0]), (r.voxels, r.dual, r.intersected), "after error")
