@@ -12,6 +12,8 @@ size is used).  Prints one JSON line on rank 0.
   roofline   compulsory bytes of a conversion (12V + 8*3F + 27N) over the
              conversion time against the measured HBM copy bandwidth
   cpu_baseline  the reference's CPU implementation on the host cores
+  batched    256 mixed meshes (grids 64-512): the batched API against one
+             call per mesh, meshes/s of each (single GPU only)
 
 --impl reference times the reference CPU implementation alone.
 Multi-GPU: replicas only (each rank converts its own copy; no collective).
@@ -163,6 +165,56 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- batched workload
+BATCH_WORKERS = 8
+
+
+def run_batched(dev, steps=2):
+    """256 seeded meshes built like the 282k-face one, face counts log-uniform in
+    [1k, 500k] (about 21M faces in all), grid 64/128/256/512 per mesh, per-mesh
+    aabb: the batched API against the same meshes converted one call at a time."""
+    import torch
+
+    import fdg_workloads as W
+    import o_voxel
+
+    ws = W.batch(4)
+    meshes = [(torch.from_numpy(w.vertices).to(dev), torch.from_numpy(w.faces).to(dev)) for w in ws]
+    F = sum(w.num_faces for w in ws)
+    kw = dict(face_weight=1.0, boundary_weight=0.2, regularization_weight=1e-2)
+    grids = [w.grid_size for w in ws]
+    aabbs = [w.aabb for w in ws]
+
+    def plain():
+        for (v, f), w in zip(meshes, ws):
+            o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=w.grid_size, aabb=w.aabb, **kw)
+
+    def batched():
+        o_voxel.convert.mesh_to_flexible_dual_grid_batch(meshes, grid_size=grids, aabb=aabbs, workers=BATCH_WORKERS, **kw)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return sum(ms) / len(ms)
+
+    t_plain = timed(plain)
+    t_batch = timed(batched)
+    return {"workload": "256 meshes, faces log-uniform 1k-500k, grids 64-512, per-mesh aabb",
+            "meshes": len(ws), "faces": int(F), "workers": BATCH_WORKERS, "steps": steps,
+            "plain_ms": t_plain, "plain_meshes_per_s": len(ws) / (t_plain / 1e3),
+            "batched_ms": t_batch, "batched_meshes_per_s": len(ws) / (t_batch / 1e3),
+            "batched_mfaces_per_s": F / (t_batch / 1e3) / 1e6, "speedup": t_plain / t_batch,
+            "api": "o_voxel.convert.mesh_to_flexible_dual_grid_batch vs one mesh_to_flexible_dual_grid call per mesh"}
+
+
 # ----------------------------------------------------------------------------- our arm
 def run_ours(args, rank, world):
     import numpy as np
@@ -285,6 +337,9 @@ def run_ours(args, rank, world):
         cpu_t = statistics.median([cb.step() for _ in range(2)])
         cb.close()
         cpu = cb.describe(cb.cores * cb.faces / cpu_t / 1e6)
+    batched = None
+    if not args.no_batch and world == 1:
+        batched = run_batched(dev)
     line = {
         "metric": METRIC, "value": value, "unit": "Mfaces/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -294,6 +349,7 @@ def run_ours(args, rank, world):
                    "weights": [w.face_weight, w.boundary_weight, w.regularization_weight], "faces_dtype": "int64",
                    "l2": "flushed between steps (256 MB write outside the timed events)", "parallelism": f"replicas x{world}"},
         "meshes_per_s": world / (ms_per_step / 1e3),
+        "batched": batched,
         "e2e": {"value": e2e_value, "unit": "Mfaces/s", "ms_per_step": e2e_ms, "h2d_bytes_per_step": 12 * V + 8 * 3 * F,
                 "d2h_bytes_per_step": 27 * N, "api": "o_voxel.convert.mesh_to_flexible_dual_grid"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -316,6 +372,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 256-mesh batched measurement")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
