@@ -86,6 +86,32 @@ int ovx_fdg_set_profiling(ovx_fdg_context *ctx, int enable);
 int ovx_fdg_stage_times(ovx_fdg_context *ctx, float *ms, int capacity);
 const char *ovx_fdg_stage_name(int stage);
 int64_t ovx_fdg_kernel_launches(const ovx_fdg_context *ctx);
+/*
+ * Output row order of the following conversions (full and occupancy-only):
+ * OVX_FDG_ORDER_BRICK (default) -- 8x8x8 bricks in x-fastest order, voxels in
+ * x-fastest order inside a brick; OVX_FDG_ORDER_Z -- ascending z-order code
+ * (ovx_z_order_encode of the voxel coordinates), i.e. the order the
+ * reference's examples produce by sorting on o_voxel.serialize.encode_seq
+ * (examples/mesh2ovox.py:31-35).  Z-order needs grid_min >= 0 and a multiple
+ * of 8 on every axis.  No counterpart in the reference operator.
+ */
+enum ovx_fdg_order
+{
+    OVX_FDG_ORDER_BRICK = 0,
+    OVX_FDG_ORDER_Z = 1
+};
+int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order);
+
+/*
+ * z-order (Morton) codes, o_voxel.serialize.encode_seq / decode_seq with
+ * mode='z_order' (serialize.py:7-36, src/serialize/z_order.cu:33-97,
+ * src/ext.cpp:28-29): code = interleave of the low 10 bits of x, y, z with x
+ * the most significant of each triple; device int32 arrays of length n,
+ * enqueued on `stream`.  Coordinates must lie in [0, 1024).
+ */
+int ovx_z_order_encode(void *stream, const int32_t *x, const int32_t *y, const int32_t *z, int64_t n, int32_t *codes);
+int ovx_z_order_decode(void *stream, const int32_t *codes, int64_t n, int32_t *x, int32_t *y, int32_t *z);
+
 /* Sizes of the last conversion, known after ovx_fdg_begin: out[0] voxel rows,
  * out[1] occupied 8^3 bricks, out[2] quadric records bucketed by brick,
  * out[3] boundary edges, out[4] bricks of the grid.  Writes min(capacity, 5)

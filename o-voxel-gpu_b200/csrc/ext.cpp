@@ -90,7 +90,7 @@ ovx_fdg_grid make_grid(const std::vector<float> &voxel_size, const std::vector<i
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Tensor &vertices, const torch::Tensor &faces,
                                                                  const float *origin, const std::vector<float> &voxel_size,
                                                                  const std::vector<int64_t> &grid_range, float face_weight,
-                                                                 float boundary_weight, float regularization_weight)
+                                                                 float boundary_weight, float regularization_weight, int64_t order)
 {
     TORCH_CHECK(vertices.is_cuda(), "vertices must be a CUDA tensor");
     TORCH_CHECK(faces.is_cuda(), "faces must be a CUDA tensor");
@@ -107,6 +107,7 @@ std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Ten
     cudaStream_t stream = at::cuda::getCurrentCUDAStream(device).stream();
     DeviceContext &dc = context_for(device);
     std::lock_guard<std::mutex> lock(dc.mu);
+    check(ovx_fdg_set_output_order(dc.ctx, (int)order), dc.ctx, "mesh_to_flexible_dual_grid (order)");
     int64_t n = 0;
     check(ovx_fdg_begin(dc.ctx, stream, v.data_ptr<float>(), v.size(0), f.numel() ? f.data_ptr() : nullptr,
                         f.scalar_type() == torch::kInt64 ? 8 : 4, f.size(0), origin, &grid, face_weight, boundary_weight,
@@ -146,23 +147,24 @@ DeviceContext &worker_context(int device, int slot)
 
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> mesh_to_flexible_dual_grid_cuda(
     const torch::Tensor &vertices, const torch::Tensor &faces, const std::vector<float> &voxel_size,
-    const std::vector<int64_t> &grid_range, float face_weight, float boundary_weight, float regularization_weight)
+    const std::vector<int64_t> &grid_range, float face_weight, float boundary_weight, float regularization_weight,
+    int64_t order)
 {
-    return run_fdg(vertices, faces, nullptr, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight);
+    return run_fdg(vertices, faces, nullptr, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight, order);
 }
 
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> mesh_to_flexible_dual_grid_cuda_ex(
     const torch::Tensor &vertices, const torch::Tensor &faces, const std::vector<float> &origin,
     const std::vector<float> &voxel_size, const std::vector<int64_t> &grid_range, float face_weight, float boundary_weight,
-    float regularization_weight)
+    float regularization_weight, int64_t order)
 {
     TORCH_CHECK(origin.size() == 3, "origin must have 3 elements");
     const float o[3] = {origin[0], origin[1], origin[2]};
-    return run_fdg(vertices, faces, o, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight);
+    return run_fdg(vertices, faces, o, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight, order);
 }
 
 torch::Tensor intersect_occ_cuda(const torch::Tensor &triangles, const std::vector<float> &voxel_size,
-                                 const std::vector<int64_t> &grid_range)
+                                 const std::vector<int64_t> &grid_range, int64_t order)
 {
     TORCH_CHECK(triangles.is_cuda(), "triangles must be a CUDA tensor");
     TORCH_CHECK(triangles.scalar_type() == torch::kFloat32, "triangles must be float32");
@@ -174,6 +176,7 @@ torch::Tensor intersect_occ_cuda(const torch::Tensor &triangles, const std::vect
     cudaStream_t stream = at::cuda::getCurrentCUDAStream(device).stream();
     DeviceContext &dc = context_for(device);
     std::lock_guard<std::mutex> lock(dc.mu);
+    check(ovx_fdg_set_output_order(dc.ctx, (int)order), dc.ctx, "intersect_occ (order)");
     int64_t n = 0;
     check(ovx_fdg_occupancy_begin(dc.ctx, stream, t.numel() ? t.data_ptr<float>() : nullptr, t.size(0), &grid, &n), dc.ctx,
           "intersect_occ");
@@ -186,7 +189,7 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     const std::vector<torch::Tensor> &vertices, const std::vector<torch::Tensor> &faces,
     const std::vector<std::vector<float>> &origins, const std::vector<std::vector<float>> &voxel_sizes,
     const std::vector<std::vector<int64_t>> &grid_ranges, float face_weight, float boundary_weight,
-    float regularization_weight, int64_t workers)
+    float regularization_weight, int64_t workers, int64_t order)
 {
     const size_t n = vertices.size();
     TORCH_CHECK(faces.size() == n && origins.size() == n && voxel_sizes.size() == n && grid_ranges.size() == n,
@@ -230,6 +233,7 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
             cudaStreamWaitEvent(st, ready, 0);
             DeviceContext &dc = worker_context(device, w);
             std::lock_guard<std::mutex> lock(dc.mu);
+            check(ovx_fdg_set_output_order(dc.ctx, (int)order), dc.ctx, "mesh_to_flexible_dual_grid_batch (order)");
             for (;;)
             {
                 const size_t i = next.fetch_add(1);
@@ -289,11 +293,49 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     return out;
 }
 
+// o_voxel.serialize z-order codes (reference: src/ext.cpp:28-29, src/serialize/api.cu)
+torch::Tensor z_order_encode_cuda(const torch::Tensor &x, const torch::Tensor &y, const torch::Tensor &z)
+{
+    TORCH_CHECK(x.is_cuda() && y.is_cuda() && z.is_cuda(), "z_order_encode_cuda: CUDA tensors expected");
+    TORCH_CHECK(x.numel() == y.numel() && x.numel() == z.numel(), "z_order_encode_cuda: x, y, z differ in length");
+    const c10::cuda::CUDAGuard guard(x.device());
+    auto xi = x.to(torch::kInt32).contiguous(), yi = y.to(torch::kInt32).contiguous(), zi = z.to(torch::kInt32).contiguous();
+    auto codes = torch::empty_like(xi);
+    const int rc = ovx_z_order_encode(at::cuda::getCurrentCUDAStream(x.get_device()).stream(), xi.data_ptr<int32_t>(),
+                                      yi.data_ptr<int32_t>(), zi.data_ptr<int32_t>(), xi.numel(), codes.data_ptr<int32_t>());
+    TORCH_CHECK(rc == OVX_FDG_OK, "z_order_encode_cuda failed: ", ovx_fdg_status_string(rc));
+    return codes;
+}
+
+std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> z_order_decode_cuda(const torch::Tensor &codes)
+{
+    TORCH_CHECK(codes.is_cuda(), "z_order_decode_cuda: CUDA tensor expected");
+    const c10::cuda::CUDAGuard guard(codes.device());
+    auto c = codes.to(torch::kInt32).contiguous();
+    auto x = torch::empty_like(c), y = torch::empty_like(c), z = torch::empty_like(c);
+    const int rc = ovx_z_order_decode(at::cuda::getCurrentCUDAStream(codes.get_device()).stream(), c.data_ptr<int32_t>(),
+                                      c.numel(), x.data_ptr<int32_t>(), y.data_ptr<int32_t>(), z.data_ptr<int32_t>());
+    TORCH_CHECK(rc == OVX_FDG_OK, "z_order_decode_cuda failed: ", ovx_fdg_status_string(rc));
+    return std::make_tuple(x, y, z);
+}
+
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
 {
-    m.def("mesh_to_flexible_dual_grid_cuda", &mesh_to_flexible_dual_grid_cuda, py::call_guard<py::gil_scoped_release>());
-    m.def("mesh_to_flexible_dual_grid_cuda_ex", &mesh_to_flexible_dual_grid_cuda_ex, py::call_guard<py::gil_scoped_release>());
-    m.def("intersect_occ_cuda", &intersect_occ_cuda, py::call_guard<py::gil_scoped_release>());
-    m.def("mesh_to_flexible_dual_grid_cuda_batch", &mesh_to_flexible_dual_grid_cuda_batch,
+    // `order` (0: brick order, 1: z-order) is this library's addition; the
+    // first seven arguments are the reference operator's
+    m.def("mesh_to_flexible_dual_grid_cuda", &mesh_to_flexible_dual_grid_cuda, py::arg("vertices"), py::arg("faces"),
+          py::arg("voxel_size"), py::arg("grid_range"), py::arg("face_weight"), py::arg("boundary_weight"),
+          py::arg("regularization_weight"), py::arg("order") = 0, py::call_guard<py::gil_scoped_release>());
+    m.def("mesh_to_flexible_dual_grid_cuda_ex", &mesh_to_flexible_dual_grid_cuda_ex, py::arg("vertices"), py::arg("faces"),
+          py::arg("origin"), py::arg("voxel_size"), py::arg("grid_range"), py::arg("face_weight"),
+          py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("order") = 0,
           py::call_guard<py::gil_scoped_release>());
+    m.def("intersect_occ_cuda", &intersect_occ_cuda, py::arg("triangles"), py::arg("voxel_size"), py::arg("grid_range"),
+          py::arg("order") = 0, py::call_guard<py::gil_scoped_release>());
+    m.def("mesh_to_flexible_dual_grid_cuda_batch", &mesh_to_flexible_dual_grid_cuda_batch, py::arg("vertices"),
+          py::arg("faces"), py::arg("origins"), py::arg("voxel_sizes"), py::arg("grid_ranges"), py::arg("face_weight"),
+          py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("workers"), py::arg("order") = 0,
+          py::call_guard<py::gil_scoped_release>());
+    m.def("z_order_encode_cuda", &z_order_encode_cuda, py::call_guard<py::gil_scoped_release>());
+    m.def("z_order_decode_cuda", &z_order_decode_cuda, py::call_guard<py::gil_scoped_release>());
 }

@@ -53,6 +53,7 @@
 #include "ovx_fdg.h"
 #include "fdg_device.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
@@ -141,6 +142,42 @@ __device__ __forceinline__ void vertex_load(const Mesh &M, long long i, float p[
     p[0] = M.verts[i * 3 + 0] - M.ox;
     p[1] = M.verts[i * 3 + 1] - M.oy;
     p[2] = M.verts[i * 3 + 2] - M.oz;
+}
+
+// z-order (Morton) codes with x as the most significant coordinate of each bit
+// triple, as o_voxel.serialize.encode_seq builds them (serialize/z_order.cu:33-97).
+__host__ __device__ __forceinline__ uint32_t spread3_10(uint32_t v)
+{
+    uint32_t r = 0;
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        r |= ((v >> i) & 1u) << (3 * i);
+    return r;
+}
+
+__host__ __device__ __forceinline__ uint32_t compact3_10(uint32_t c)
+{
+    uint32_t r = 0;
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        r |= ((c >> (3 * i)) & 1u) << i;
+    return r;
+}
+
+// Local index lx + 8ly + 64lz of an 8^3 brick -> its 9-bit z-order rank.
+__device__ __forceinline__ int local_morton(int lv)
+{
+    const uint32_t lx = (uint32_t)lv & 7u, ly = ((uint32_t)lv >> 3) & 7u, lz = (uint32_t)lv >> 6;
+    return (int)((spread3_10(lx) << 2) | (spread3_10(ly) << 1) | spread3_10(lz));
+}
+
+__device__ __forceinline__ unsigned long long brick_morton(unsigned long long bx, unsigned long long by, unsigned long long bz)
+{
+    unsigned long long r = 0;
+#pragma unroll
+    for (int i = 0; i < 21; ++i)
+        r |= (((bx >> i) & 1ull) << (3 * i + 2)) | (((by >> i) & 1ull) << (3 * i + 1)) | (((bz >> i) & 1ull) << (3 * i));
+    return r;
 }
 
 __device__ __forceinline__ void brick_origin(const Grid &g, long long b, int o[3])
@@ -1222,6 +1259,7 @@ struct SolveArgs
     uint8_t *flags;
     uint32_t *counters;
     uint4 *contrib;             // per-voxel contribution lists {key lo, key hi, payload, 0}
+    bool zorder;                // output rows in z-order (bbase then holds z-order row bases)
     uint32_t *longv;            // rows whose lists are too long for voxel_accumulate: up to kLongMidMax
                                 // entries from the front (counter C_LONG), longer ones from the back (C_HUGE)
     uint32_t longv_cap;
@@ -1230,11 +1268,58 @@ struct SolveArgs
     uint32_t clist_cap;
 };
 
+// Rank of active voxel lv among the brick's voxels in output order.
 template <typename SS>
 __device__ __forceinline__ int dense_index(const SS &S, int lv)
 {
-    const int w = lv >> 5, b = lv & 31;
+    const int r = S.zorder ? local_morton(lv) : lv;
+    const int w = r >> 5, b = r & 31;
     return (int)(S.wpre[w] + __popc(S.bits[w] & ((1u << b) - 1u)));
+}
+
+// Loads a brick's occupancy into S (obits, bits in output-rank order, wpre,
+// nvox); the calling CTA must not use S before the final barrier.
+template <typename SS>
+__device__ __forceinline__ void load_brick_ranks(SS &S, const uint32_t *__restrict__ bits, long long b, bool zorder)
+{
+    const int tid = threadIdx.x;
+    if (tid < kWordsPerBrick)
+    {
+        const uint32_t w = bits[b * kWordsPerBrick + tid];
+        S.obits[tid] = w;
+        S.bits[tid] = zorder ? 0u : w;
+    }
+    if (tid == 0)
+        S.zorder = zorder ? 1 : 0;
+    __syncthreads();
+    if (zorder)
+    {
+        for (int lv = tid; lv < 512; lv += blockDim.x)
+            if ((S.obits[lv >> 5] >> (lv & 31)) & 1u)
+            {
+                const int m = local_morton(lv);
+                atomicOr(&S.bits[m >> 5], 1u << (m & 31));
+            }
+        __syncthreads();
+    }
+    if (tid < 32)
+    {
+        const uint32_t w = tid < kWordsPerBrick ? S.bits[tid] : 0u;
+        const uint32_t c = __popc(w);
+        uint32_t incl = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (tid >= d)
+                incl += y;
+        }
+        if (tid < kWordsPerBrick)
+            S.wpre[tid] = incl - c;
+        if (tid == 31)
+            S.nvox = (int)incl;
+    }
+    __syncthreads();
 }
 
 // Expand one record of the brick into (dense voxel index, order key, payload) contributions.
@@ -1385,8 +1470,10 @@ __device__ __forceinline__ void contrib_apply(const Contrib &c, Acc &a)
 // ---------------------------------------------------------------------------
 struct ListShared
 {
-    uint32_t bits[kWordsPerBrick];
-    uint32_t wpre[kWordsPerBrick];
+    uint32_t obits[kWordsPerBrick]; // occupancy words (bit = local index)
+    uint32_t bits[kWordsPerBrick];  // the same voxels in output-rank order (z-order: bit = local z-order rank)
+    uint32_t wpre[kWordsPerBrick];  // prefix counts of bits
+    int zorder;
     uint32_t cnt[512];
     uint32_t off[512];
     uint32_t scan_tmp[kConsumeThreads / 32 + 1];
@@ -1432,42 +1519,21 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     brick_origin(g, b, o);
     const Rec *rec = A.rec + A.roff[b];
     const unsigned long long nrec = A.roff[b + 1] - A.roff[b];
-    if (tid < 32)
-    {
-        const uint32_t w = tid < kWordsPerBrick ? A.bits[b * kWordsPerBrick + tid] : 0u;
-        const uint32_t c = __popc(w);
-        uint32_t incl = c;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1)
-        {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-            if (tid >= d)
-                incl += y;
-        }
-        if (tid < kWordsPerBrick)
-        {
-            S.bits[tid] = w;
-            S.wpre[tid] = incl - c;
-        }
-        if (tid == 31)
-        {
-            S.nvox = (int)incl;
-            S.status = 0;
-        }
-    }
     for (int i = tid; i < 512; i += blockDim.x)
         S.cnt[i] = 0;
-    __syncthreads();
+    if (tid == 0)
+        S.status = 0;
+    load_brick_ranks(S, A.bits, b, A.zorder);
     const int nvox = S.nvox;
     const unsigned long long vbase = A.bbase[b];
-    // voxel coordinates of the brick's rows (x-fastest local order)
+    // voxel coordinates of the brick's rows
     for (int w = 0; w < kWordsPerBrick; ++w)
     {
-        const uint32_t word = S.bits[w];
+        const uint32_t word = S.obits[w];
         if (tid < 32 && ((word >> tid) & 1u))
         {
             const int lv = w * 32 + tid;
-            const long long row = (long long)(vbase + S.wpre[w] + __popc(word & ((1u << tid) - 1u)));
+            const long long row = (long long)(vbase + dense_index(S, lv));
             A.vox[row * 3 + 0] = o[0] + (lv & 7);
             A.vox[row * 3 + 1] = o[1] + ((lv >> 3) & 7);
             A.vox[row * 3 + 2] = o[2] + (lv >> 6);
@@ -1844,37 +1910,93 @@ __global__ void __launch_bounds__(128) constrained_solve(const float *__restrict
 }
 
 // Occupancy only: coordinates of every active voxel, one CTA per active brick.
-__global__ void __launch_bounds__(128) brick_coords(const uint32_t *__restrict__ bits, const unsigned long long *__restrict__ bbase,
-                                                    const uint32_t *__restrict__ active, Grid g, int32_t *__restrict__ vox)
+struct CoordShared
 {
-    __shared__ uint32_t sb[kWordsPerBrick], sp[kWordsPerBrick];
+    uint32_t obits[kWordsPerBrick];
+    uint32_t bits[kWordsPerBrick];
+    uint32_t wpre[kWordsPerBrick];
+    int zorder;
+    int nvox;
+};
+
+// Coordinates of the active voxels (intersect_occ output), one CTA per active brick.
+__global__ void __launch_bounds__(128) brick_coords(const uint32_t *__restrict__ bits, const unsigned long long *__restrict__ bbase,
+                                                    const uint32_t *__restrict__ active, Grid g, bool zorder, int32_t *__restrict__ vox)
+{
+    __shared__ CoordShared S;
     const long long b = active[blockIdx.x];
-    if (threadIdx.x < kWordsPerBrick)
-        sb[threadIdx.x] = bits[b * kWordsPerBrick + threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        uint32_t r = 0;
-        for (int w = 0; w < kWordsPerBrick; ++w)
-        {
-            sp[w] = r;
-            r += __popc(sb[w]);
-        }
-    }
-    __syncthreads();
+    load_brick_ranks(S, bits, b, zorder);
     int o[3];
     brick_origin(g, b, o);
     const unsigned long long base = bbase[b];
     for (int lv = threadIdx.x; lv < 512; lv += blockDim.x)
     {
-        const int w = lv >> 5, bt = lv & 31;
-        if (!((sb[w] >> bt) & 1u))
+        if (!((S.obits[lv >> 5] >> (lv & 31)) & 1u))
             continue;
-        const long long row = (long long)(base + sp[w] + __popc(sb[w] & ((1u << bt) - 1u)));
+        const long long row = (long long)(base + dense_index(S, lv));
         vox[row * 3 + 0] = o[0] + (lv & 7);
         vox[row * 3 + 1] = o[1] + ((lv >> 3) & 7);
         vox[row * 3 + 2] = o[2] + (lv >> 6);
     }
+}
+
+// z-order row bases: sort key of each active brick (its z-order code) ...
+__global__ void zorder_brick_keys(const uint32_t *__restrict__ active, long long n_active, Grid g,
+                                  unsigned long long *__restrict__ keys, uint32_t *__restrict__ slots)
+{
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_active)
+        return;
+    const long long b = active[s];
+    const unsigned long long bx = (unsigned long long)(g.gmin[0] / kBrick) + (unsigned long long)(b % g.nb[0]);
+    const unsigned long long by = (unsigned long long)(g.gmin[1] / kBrick) + (unsigned long long)((b / g.nb[0]) % g.nb[1]);
+    const unsigned long long bz = (unsigned long long)(g.gmin[2] / kBrick) + (unsigned long long)(b / ((long long)g.nb[0] * g.nb[1]));
+    keys[s] = brick_morton(bx, by, bz);
+    slots[s] = (uint32_t)s;
+}
+
+// ... voxel counts in that order ...
+__global__ void zorder_counts(const uint32_t *__restrict__ sorted_slots, long long n_active, const uint32_t *__restrict__ active,
+                              const uint32_t *__restrict__ bcount, uint32_t *__restrict__ cnt)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n_active)
+        cnt[j] = bcount[active[sorted_slots[j]]];
+    else if (j == n_active)
+        cnt[j] = 0u;
+}
+
+// ... and their exclusive scan scattered back to the bricks.
+__global__ void zorder_bases(const uint32_t *__restrict__ sorted_slots, long long n_active, const uint32_t *__restrict__ active,
+                             const unsigned long long *__restrict__ base_sorted, unsigned long long *__restrict__ zbase)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n_active)
+        zbase[active[sorted_slots[j]]] = base_sorted[j];
+}
+
+// o_voxel.serialize z-order codes (serialize/z_order.cu:33-97): 10 bits per coordinate.
+__global__ void z_order_encode_kernel(const int32_t *__restrict__ x, const int32_t *__restrict__ y, const int32_t *__restrict__ z,
+                                      long long n, int32_t *__restrict__ codes)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t c = (spread3_10((uint32_t)x[i] & 1023u) << 2) | (spread3_10((uint32_t)y[i] & 1023u) << 1) |
+                       spread3_10((uint32_t)z[i] & 1023u);
+    codes[i] = (int32_t)c;
+}
+
+__global__ void z_order_decode_kernel(const int32_t *__restrict__ codes, long long n, int32_t *__restrict__ x,
+                                      int32_t *__restrict__ y, int32_t *__restrict__ z)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t c = (uint32_t)codes[i];
+    x[i] = (int32_t)compact3_10(c >> 2);
+    y[i] = (int32_t)compact3_10(c >> 1);
+    z[i] = (int32_t)compact3_10(c);
 }
 
 // ===========================================================================
@@ -2043,6 +2165,7 @@ struct ovx_fdg_context
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
     Buf vcnt, voff, emax, bkeys, boff, btab;
     Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, longv;
+    Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     unsigned long long *host = nullptr; // pinned readback words
     std::string err;
     // state between begin and finish
@@ -2058,6 +2181,7 @@ struct ovx_fdg_context
     long long n_vox = 0, n_active = 0, n_rec = 0, n_boundary = 0;
     unsigned long long n_fstaged = 0, fstage_want = 0; // face records staged by the count pass (and the most seen)
     bool face_staged = false;                         // all of them fitted: the fill pass need not redo the tests
+    int order = 0;                                    // output row order: 0 brick-linear, 1 z-order
     int finished = 0;
     long long launches = 0; // kernels this library launched (its own, not CUB's)
     bool profiling = false;
@@ -2072,7 +2196,8 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
                 &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage, &c->longv};
+                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage, &c->longv,
+                &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
@@ -2152,6 +2277,46 @@ inline unsigned blocks_for(long long n, int threads)
     return (unsigned)((n + threads - 1) / threads);
 }
 
+// z-order row bases of the active bricks (ctx->zbase, indexed by brick): the
+// bricks' z-order codes sorted, their voxel counts scanned in that order.
+int zorder_row_bases(ovx_fdg_context *ctx, cudaStream_t st)
+{
+    const long long na = ctx->n_active, nb = ctx->g.nbricks;
+    OVX_CUDA(ensure(ctx->zkeys, (size_t)(na + 1) * 16));
+    OVX_CUDA(ensure(ctx->zslots, (size_t)(na + 1) * 8));
+    OVX_CUDA(ensure(ctx->zcnt, (size_t)(na + 1) * 4));
+    OVX_CUDA(ensure(ctx->zsbase, (size_t)(na + 1) * 8));
+    OVX_CUDA(ensure(ctx->zbase, (size_t)(nb + 1) * 8));
+    if (na == 0)
+        return OVX_FDG_OK;
+    unsigned long long *kin = (unsigned long long *)ctx->zkeys.p, *kout = kin + (na + 1);
+    uint32_t *vin = (uint32_t *)ctx->zslots.p, *vout = vin + (na + 1);
+    const uint32_t *active = (const uint32_t *)ctx->active.p;
+    zorder_brick_keys<<<blocks_for(na, 256), 256, 0, st>>>(active, na, ctx->g, kin, vin);
+    // key bits: 3 x (bits of the largest brick coordinate)
+    int cb = 1;
+    for (int a = 0; a < 3; ++a)
+    {
+        const long long mx = ctx->g.gmin[a] / kBrick + ctx->g.nb[a];
+        while ((1ll << cb) <= mx)
+            ++cb;
+    }
+    const int end_bit = std::min(63, 3 * cb);
+    size_t bytes = 0;
+    OVX_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, (int)na, 0, end_bit, st));
+    OVX_CUDA(ensure(ctx->cub_tmp, bytes));
+    OVX_CUDA(cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, bytes, kin, kout, vin, vout, (int)na, 0, end_bit, st));
+    zorder_counts<<<blocks_for(na + 1, 256), 256, 0, st>>>(vout, na, active, (const uint32_t *)ctx->bcount.p,
+                                                          (uint32_t *)ctx->zcnt.p);
+    OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->zcnt.p, (unsigned long long *)ctx->zsbase.p, na + 1, st));
+    zorder_bases<<<blocks_for(na, 256), 256, 0, st>>>(vout, na, active, (const unsigned long long *)ctx->zsbase.p,
+                                                     (unsigned long long *)ctx->zbase.p);
+    ctx->launches += 3;
+    OVX_CUDA(cudaGetLastError());
+    return OVX_FDG_OK;
+}
+
+
 int check_grid(ovx_fdg_context *ctx, const ovx_fdg_grid *grid, Grid &g)
 {
     if (!grid)
@@ -2173,6 +2338,10 @@ int check_grid(ovx_fdg_context *ctx, const ovx_fdg_grid *grid, Grid &g)
         g.nb[a] = (int)((sz + kBrick - 1) / kBrick);
         nb *= g.nb[a];
     }
+    if (ctx->order == 1)
+        for (int a = 0; a < 3; ++a)
+            if (g.gmin[a] < 0 || g.gmin[a] % kBrick != 0)
+                return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "z-order output needs grid_min >= 0 and a multiple of 8 on every axis");
     if (nb * kWordsPerBrick * 4ll > (64ll << 30) || nb >= (1ll << 31))
         return fail(ctx, OVX_FDG_CAPACITY, "grid too large for the dense brick bitmap (64 GiB limit)");
     g.nbricks = nb;
@@ -2461,6 +2630,36 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
     delete ctx;
 }
 
+int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order)
+{
+    if (!ctx)
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (order != OVX_FDG_ORDER_BRICK && order != OVX_FDG_ORDER_Z)
+        return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "unknown output order");
+    ctx->order = order;
+    return OVX_FDG_OK;
+}
+
+int ovx_z_order_encode(void *stream, const int32_t *x, const int32_t *y, const int32_t *z, int64_t n, int32_t *codes)
+{
+    if (n < 0 || (n > 0 && (!x || !y || !z || !codes)))
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (n == 0)
+        return OVX_FDG_OK;
+    z_order_encode_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(x, y, z, n, codes);
+    return cudaGetLastError() == cudaSuccess ? OVX_FDG_OK : OVX_FDG_CUDA_ERROR;
+}
+
+int ovx_z_order_decode(void *stream, const int32_t *codes, int64_t n, int32_t *x, int32_t *y, int32_t *z)
+{
+    if (n < 0 || (n > 0 && (!x || !y || !z || !codes)))
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (n == 0)
+        return OVX_FDG_OK;
+    z_order_decode_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(codes, n, x, y, z);
+    return cudaGetLastError() == cudaSuccess ? OVX_FDG_OK : OVX_FDG_CUDA_ERROR;
+}
+
 int ovx_fdg_set_profiling(ovx_fdg_context *ctx, int enable)
 {
     if (!ctx)
@@ -2654,6 +2853,14 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.rw = ctx->rw;
     SA.bits = (const uint32_t *)ctx->bits.p;
     SA.bbase = (const unsigned long long *)ctx->bbase.p;
+    SA.zorder = ctx->order == 1;
+    if (SA.zorder)
+    {
+        const int zr = zorder_row_bases(ctx, st);
+        if (zr != OVX_FDG_OK)
+            return zr;
+        SA.bbase = (const unsigned long long *)ctx->zbase.p;
+    }
     SA.active = (const uint32_t *)ctx->active.p;
     SA.roff = (const unsigned long long *)ctx->roff.p;
     SA.rec = (const Rec *)ctx->rec.p;
@@ -2753,8 +2960,16 @@ int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "NULL output buffer");
     cudaStream_t st = (cudaStream_t)stream;
     OVX_CUDA(cudaSetDevice(ctx->device));
-    brick_coords<<<(unsigned)ctx->n_active, 128, 0, st>>>((const uint32_t *)ctx->bits.p, (const unsigned long long *)ctx->bbase.p,
-                                                          (const uint32_t *)ctx->active.p, ctx->g, voxel_indices);
+    const unsigned long long *base = (const unsigned long long *)ctx->bbase.p;
+    if (ctx->order == 1)
+    {
+        const int zr = zorder_row_bases(ctx, st);
+        if (zr != OVX_FDG_OK)
+            return zr;
+        base = (const unsigned long long *)ctx->zbase.p;
+    }
+    brick_coords<<<(unsigned)ctx->n_active, 128, 0, st>>>((const uint32_t *)ctx->bits.p, base, (const uint32_t *)ctx->active.p,
+                                                          ctx->g, ctx->order == 1, voxel_indices);
     ++ctx->launches;
     OVX_CUDA(cudaGetLastError());
     return OVX_FDG_OK;

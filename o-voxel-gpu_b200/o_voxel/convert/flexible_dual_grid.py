@@ -144,6 +144,14 @@ def _grid_setup(vertices, faces, voxel_size, grid_size, aabb):
     return vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg
 
 
+def _order_code(order: Optional[str]) -> int:
+    if order is None or order == "brick":
+        return 0
+    if order == "z_order":
+        return 1
+    raise ValueError(f"order must be None, 'brick' or 'z_order', got {order!r}")
+
+
 def _require_cuda(t: torch.Tensor, name: str):
     if not t.is_cuda:
         raise RuntimeError(f"{name}: this implementation runs on CUDA tensors only (got a {t.device} tensor)")
@@ -160,6 +168,7 @@ def mesh_to_flexible_dual_grid(
     boundary_weight: float = 1.0,
     regularization_weight: float = 0.1,
     timing: bool = False,
+    order: Optional[str] = None,
 ) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
     """
     Convert a triangle mesh into a sparse flexible dual grid.
@@ -174,6 +183,10 @@ def mesh_to_flexible_dual_grid(
         boundary_weight (float): weight of the boundary-edge term of the QEF (> 0 adds it).
         regularization_weight (float): weight pulling each dual vertex toward the mean intersection point.
         timing (bool): accepted for compatibility; ignored (as on the reference CUDA path).
+        order (str): row order of the outputs (not in the reference, whose GPU order is
+            arbitrary): None or 'brick' -- 8x8x8 bricks then voxels, x-fastest;
+            'z_order' -- ascending o_voxel.serialize.encode_seq code, the order the
+            reference's examples obtain by sorting on it.
 
     Returns:
         voxel_indices (torch.Tensor): [N, 3] int32 occupied voxel coordinates.
@@ -182,17 +195,18 @@ def mesh_to_flexible_dual_grid(
         intersected (torch.Tensor): [N, 3] bool; axis a is set when the voxel's edge along a
             starting at its min corner crosses the surface.
     """
+    oc = _order_code(order)
     vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg = _grid_setup(vertices, faces, voxel_size, grid_size, aabb)
     _require_cuda(vertices, "mesh_to_flexible_dual_grid")
     if aabb_cpu is not None:
         origin = [float(x) for x in aabb_cpu[0].tolist()]
         return _ext().mesh_to_flexible_dual_grid_cuda_ex(vertices, faces, origin, voxel_size_arg, grid_range_arg,
                                                          float(face_weight), float(boundary_weight),
-                                                         float(regularization_weight))
+                                                         float(regularization_weight), oc)
     # aabb derived on the device: shift with torch, exactly like the reference wrapper
     vertices = vertices - aabb[0].reshape(1, 3)
     return _ext().mesh_to_flexible_dual_grid_cuda(vertices, faces, voxel_size_arg, grid_range_arg, float(face_weight),
-                                                  float(boundary_weight), float(regularization_weight))
+                                                  float(boundary_weight), float(regularization_weight), oc)
 
 
 @torch.no_grad()
@@ -202,18 +216,19 @@ def intersect_occ(
     voxel_size: Optional[FloatArrayLike] = None,
     grid_size: Optional[IntArrayLike] = None,
     aabb: Optional[ArrayLike] = None,
+    order: Optional[str] = None,
 ) -> torch.Tensor:
     """
     Return only the voxel coordinates intersected by a triangle mesh ([N, 3] int32).
 
-    Same grid setup and occupancy rules as mesh_to_flexible_dual_grid, without
-    quadrics or dual vertices.
+    Same grid setup, occupancy rules and `order` option as
+    mesh_to_flexible_dual_grid, without quadrics or dual vertices.
     """
     vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg = _grid_setup(vertices, faces, voxel_size, grid_size, aabb)
     _require_cuda(vertices, "intersect_occ")
     vertices = vertices - aabb[0].reshape(1, 3)
     triangles = vertices[faces.to(dtype=torch.long)].contiguous()
-    return _ext().intersect_occ_cuda(triangles, voxel_size_arg, grid_range_arg)
+    return _ext().intersect_occ_cuda(triangles, voxel_size_arg, grid_range_arg, _order_code(order))
 
 
 @torch.no_grad()
@@ -226,6 +241,7 @@ def mesh_to_flexible_dual_grid_batch(
     boundary_weight: float = 1.0,
     regularization_weight: float = 0.1,
     workers: int = 4,
+    order: Optional[str] = None,
 ) -> List[Tuple[torch.Tensor, torch.Tensor, torch.Tensor]]:
     """
     Convert many meshes at once; returns one (voxel_indices, dual_vertices,
@@ -241,6 +257,7 @@ def mesh_to_flexible_dual_grid_batch(
         face_weight, boundary_weight, regularization_weight: shared by all meshes.
         workers: host threads converting meshes concurrently, each with its own
             CUDA stream; the results are ordered on the caller's current stream.
+        order: output row order, as in mesh_to_flexible_dual_grid.
 
     The reference has no batched form; this one exists so that many small and
     mid-sized meshes keep the GPU busy while each mesh's single host
@@ -275,4 +292,4 @@ def mesh_to_flexible_dual_grid_batch(
         granges.append(gr_arg)
     return _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
                                                         float(boundary_weight), float(regularization_weight),
-                                                        int(workers))
+                                                        int(workers), _order_code(order))

@@ -32,6 +32,9 @@ PROTOTYPES = [
     ("ovx_fdg_stage_name", ctypes.c_char_p, [ctypes.c_int]),
     ("ovx_fdg_kernel_launches", _I64, [_P]),
     ("ovx_fdg_last_counts", ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.c_int]),
+    ("ovx_fdg_set_output_order", ctypes.c_int, [_P, ctypes.c_int]),
+    ("ovx_z_order_encode", ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
+    ("ovx_z_order_decode", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
     ("ovx_fdg_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.c_int32, _I64, _P, _P, _F, _F, _F, ctypes.POINTER(_I64)]),
     ("ovx_fdg_finish", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("ovx_fdg_sync_status", ctypes.c_int, [_P, _P]),
@@ -120,6 +123,10 @@ class Context:
 
     def kernel_launches(self) -> int:
         return int(self._lib.ovx_fdg_kernel_launches(self.handle))
+
+    def set_output_order(self, order: int):
+        """0: brick order (default), 1: ascending z-order code."""
+        self._check(self._lib.ovx_fdg_set_output_order(self.handle, int(order)), "ovx_fdg_set_output_order")
 
     def last_counts(self) -> dict:
         """Sizes of the last conversion (voxels, occupied bricks, records, boundary edges, grid bricks)."""

@@ -68,6 +68,28 @@ def build_ref(force=False):
     return REF_SO
 
 
+REF_ZORDER_SO = os.path.join(REF_DIR, "zorder_ref.so")
+
+
+def build_ref_zorder(force=False):
+    """Compile the reference's z-order source (src/serialize/z_order.cu; its
+    CPU functions are what the binding calls) into oracle/_ref; returns the .so
+    path or None if the source is absent."""
+    src = os.path.join(REFERENCE_ROOT, "src", "serialize", "z_order.cu")
+    if not os.path.exists(src):
+        return REF_ZORDER_SO if os.path.exists(REF_ZORDER_SO) else None
+    binding = os.path.join(HERE, "ref_zorder_binding.cu")
+    if not (force or _newer(REF_ZORDER_SO, [src, binding])):
+        return REF_ZORDER_SO
+    os.makedirs(REF_DIR, exist_ok=True)
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    cmd = [nvcc, "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC", "-shared",
+           "-I", os.path.dirname(src), src, binding, "-o", REF_ZORDER_SO]
+    subprocess.check_call(cmd)
+    return REF_ZORDER_SO
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
+    print(build_ref_zorder(force="--force" in sys.argv))

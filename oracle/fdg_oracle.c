@@ -650,3 +650,42 @@ void fdg_oracle_free_ptr(void *p)
 {
     free(p);
 }
+
+/*
+ * z-order codes of o_voxel.serialize.encode_seq / decode_seq, mode 'z_order'
+ * (serialize/z_order.cu:33-97 and serialize.py:7-36): bit i of x, y and z goes
+ * to bits 3i+2, 3i+1 and 3i of a 30-bit code (x the most significant of each
+ * triple), for coordinates in [0, 1024).
+ */
+void fdg_oracle_z_order_encode(int64_t n, const int32_t *x, const int32_t *y, const int32_t *z, int32_t *codes)
+{
+    for (int64_t k = 0; k < n; ++k)
+    {
+        uint32_t c = 0;
+        for (int i = 0; i < 10; ++i)
+        {
+            c |= (((uint32_t)x[k] >> i) & 1u) << (3 * i + 2);
+            c |= (((uint32_t)y[k] >> i) & 1u) << (3 * i + 1);
+            c |= (((uint32_t)z[k] >> i) & 1u) << (3 * i);
+        }
+        codes[k] = (int32_t)c;
+    }
+}
+
+void fdg_oracle_z_order_decode(int64_t n, const int32_t *codes, int32_t *x, int32_t *y, int32_t *z)
+{
+    for (int64_t k = 0; k < n; ++k)
+    {
+        const uint32_t c = (uint32_t)codes[k];
+        uint32_t a = 0, b = 0, d = 0;
+        for (int i = 0; i < 10; ++i)
+        {
+            a |= ((c >> (3 * i + 2)) & 1u) << i;
+            b |= ((c >> (3 * i + 1)) & 1u) << i;
+            d |= ((c >> (3 * i)) & 1u) << i;
+        }
+        x[k] = (int32_t)a;
+        y[k] = (int32_t)b;
+        z[k] = (int32_t)d;
+    }
+}

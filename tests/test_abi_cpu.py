@@ -15,7 +15,7 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 def declared():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(ovx_fdg_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(ovx_\w+)\s*\(", text)))
 
 
 def test_header_declares_functions():

@@ -55,7 +55,24 @@ def test_signature_matches_reference():
     import inspect
 
     sig = inspect.signature(o_voxel.convert.mesh_to_flexible_dual_grid)
+    # the reference's parameters, in order, then this implementation's optional `order`
     assert list(sig.parameters) == ["vertices", "faces", "voxel_size", "grid_size", "aabb", "face_weight",
-                                    "boundary_weight", "regularization_weight", "timing"]
+                                    "boundary_weight", "regularization_weight", "timing", "order"]
     d = {k: p.default for k, p in sig.parameters.items()}
     assert d["face_weight"] == 1.0 and d["boundary_weight"] == 1.0 and d["regularization_weight"] == 0.1
+    assert d["order"] is None
+
+
+def test_order_and_serialize_argument_checks():
+    import torch
+
+    v = torch.zeros(3, 3)
+    f = torch.tensor([[0, 1, 2]])
+    with pytest.raises(ValueError, match="order"):
+        o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=8, aabb=[[0, 0, 0], [1, 1, 1]], order="hilbert")
+    with pytest.raises(RuntimeError, match="CUDA tensors only"):
+        o_voxel.serialize.encode_seq(torch.zeros(4, 3, dtype=torch.int32))
+    with pytest.raises(NotImplementedError):
+        o_voxel.serialize.encode_seq(torch.zeros(4, 3, dtype=torch.int32), mode="hilbert")
+    with pytest.raises(ValueError):
+        o_voxel.serialize.decode_seq(torch.zeros(4, dtype=torch.int32), mode="peano")
