@@ -161,6 +161,29 @@ int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *tri
 int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices);
 
 /*
+ * Flexible dual grid -> triangle mesh (reference
+ * o_voxel.convert.flexible_dual_grid_to_mesh, o_voxel/convert/flexible_dual_grid.py:332-477,
+ * with its hashmap src/hash/hash.cu:269-420).  Inputs (device): coords int32
+ * [N,3], dual_vertices float32 [N,3] (voxel-relative offsets, as that function
+ * takes them), intersected uint8 [N,3], split_weight float32 [N] or NULL;
+ * grid_size, voxel_size and aabb_min on the host.  begin finds the quads (one
+ * stream synchronisation) and returns the output sizes: num_vertices = N (N +
+ * quads in training mode), num_triangles = 2 * quads (4 * quads in training
+ * mode, which needs split_weight).  finish writes vertices float32
+ * [num_vertices,3] and triangles int32 [num_triangles,3].  A mesh context holds
+ * the lookup table and is not safe to use from two threads at once.
+ */
+typedef struct ovx_fdg_mesh_context ovx_fdg_mesh_context;
+int ovx_fdg_mesh_context_create(int device, ovx_fdg_mesh_context **out);
+void ovx_fdg_mesh_context_destroy(ovx_fdg_mesh_context *ctx);
+const char *ovx_fdg_mesh_last_error(const ovx_fdg_mesh_context *ctx);
+int ovx_fdg_to_mesh_begin(ovx_fdg_mesh_context *ctx, void *stream, const int32_t *coords, const float *dual_vertices,
+                          const uint8_t *intersected, const float *split_weight, int64_t num_voxels, const int32_t grid_size[3],
+                          const float voxel_size[3], const float aabb_min[3], int32_t train, int64_t *num_vertices,
+                          int64_t *num_triangles);
+int ovx_fdg_to_mesh_finish(ovx_fdg_mesh_context *ctx, void *stream, float *vertices, int32_t *triangles);
+
+/*
  * Occupancy without any allocation (no counterpart in the reference; its
  * operators always allocate).  For hosts that cannot let a library allocate
  * device memory: an application that hands all device memory to its own pool

@@ -293,6 +293,65 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     return out;
 }
 
+// flexible dual grid -> mesh (reference o_voxel/convert/flexible_dual_grid.py:332-477)
+std::tuple<torch::Tensor, torch::Tensor> flexible_dual_grid_to_mesh_cuda(
+    const torch::Tensor &coords, const torch::Tensor &dual_vertices, const torch::Tensor &intersected,
+    const c10::optional<torch::Tensor> &split_weight, const std::vector<int64_t> &grid_size,
+    const std::vector<float> &voxel_size, const std::vector<float> &aabb_min, bool train)
+{
+    TORCH_CHECK(coords.is_cuda() && dual_vertices.is_cuda() && intersected.is_cuda(), "flexible_dual_grid_to_mesh: CUDA tensors expected");
+    TORCH_CHECK(coords.dim() == 2 && coords.size(1) == 3, "coords must be [N,3]");
+    const int64_t n = coords.size(0);
+    TORCH_CHECK(dual_vertices.dim() == 2 && dual_vertices.size(0) == n && dual_vertices.size(1) == 3, "dual_vertices must be [N,3]");
+    TORCH_CHECK(intersected.numel() == 3 * n, "intersected must have N x 3 entries");
+    TORCH_CHECK(grid_size.size() == 3 && voxel_size.size() == 3 && aabb_min.size() == 3, "grid_size, voxel_size, aabb_min need 3 values");
+    const c10::cuda::CUDAGuard guard(coords.device());
+    const int device = coords.get_device();
+    auto c = coords.to(torch::kInt32).contiguous();
+    auto d = dual_vertices.to(torch::kFloat32).contiguous();
+    auto f = intersected.to(torch::kUInt8).contiguous();
+    torch::Tensor w;
+    if (split_weight.has_value() && split_weight->defined())
+    {
+        w = split_weight->to(torch::kFloat32).contiguous();
+        TORCH_CHECK(w.numel() == n, "split_weight must have one value per voxel");
+    }
+    TORCH_CHECK(!train || w.defined(), "split_weight must be provided in training mode");
+    static std::mutex map_mu;
+    static std::map<int, ovx_fdg_mesh_context *> contexts;
+    static std::map<int, std::unique_ptr<std::mutex>> locks;
+    ovx_fdg_mesh_context *ctx = nullptr;
+    std::mutex *mu = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(map_mu);
+        auto &slot = contexts[device];
+        if (!slot)
+        {
+            const int rc = ovx_fdg_mesh_context_create(device, &slot);
+            TORCH_CHECK(rc == OVX_FDG_OK, "ovx_fdg_mesh_context_create failed: ", ovx_fdg_status_string(rc));
+            locks[device] = std::make_unique<std::mutex>();
+        }
+        ctx = slot;
+        mu = locks[device].get();
+    }
+    std::lock_guard<std::mutex> lock(*mu);
+    cudaStream_t stream = at::cuda::getCurrentCUDAStream(device).stream();
+    const int32_t gs[3] = {(int32_t)grid_size[0], (int32_t)grid_size[1], (int32_t)grid_size[2]};
+    const float vs[3] = {voxel_size[0], voxel_size[1], voxel_size[2]};
+    const float am[3] = {aabb_min[0], aabb_min[1], aabb_min[2]};
+    int64_t nv = 0, nt = 0;
+    int rc = ovx_fdg_to_mesh_begin(ctx, stream, n ? c.data_ptr<int32_t>() : nullptr, n ? d.data_ptr<float>() : nullptr,
+                                   n ? f.data_ptr<uint8_t>() : nullptr, w.defined() ? w.data_ptr<float>() : nullptr, n, gs, vs,
+                                   am, train ? 1 : 0, &nv, &nt);
+    TORCH_CHECK(rc == OVX_FDG_OK, "flexible_dual_grid_to_mesh failed (", ovx_fdg_status_string(rc), "): ", ovx_fdg_mesh_last_error(ctx));
+    auto opts = torch::TensorOptions().device(coords.device());
+    auto verts = torch::empty({nv, 3}, opts.dtype(torch::kFloat32));
+    auto tris = torch::empty({nt, 3}, opts.dtype(torch::kInt32));
+    rc = ovx_fdg_to_mesh_finish(ctx, stream, nv ? verts.data_ptr<float>() : nullptr, nt ? tris.data_ptr<int32_t>() : nullptr);
+    TORCH_CHECK(rc == OVX_FDG_OK, "flexible_dual_grid_to_mesh failed (", ovx_fdg_status_string(rc), "): ", ovx_fdg_mesh_last_error(ctx));
+    return std::make_tuple(verts, tris);
+}
+
 // o_voxel.serialize z-order codes (reference: src/ext.cpp:28-29, src/serialize/api.cu)
 torch::Tensor z_order_encode_cuda(const torch::Tensor &x, const torch::Tensor &y, const torch::Tensor &z)
 {
@@ -337,5 +396,6 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
           py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("workers"), py::arg("order") = 0,
           py::call_guard<py::gil_scoped_release>());
     m.def("z_order_encode_cuda", &z_order_encode_cuda, py::call_guard<py::gil_scoped_release>());
+    m.def("flexible_dual_grid_to_mesh_cuda", &flexible_dual_grid_to_mesh_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("z_order_decode_cuda", &z_order_decode_cuda, py::call_guard<py::gil_scoped_release>());
 }

@@ -29,6 +29,7 @@ __all__ = [
     "mesh_to_flexible_dual_grid",
     "mesh_to_flexible_dual_grid_batch",
     "intersect_occ",
+    "flexible_dual_grid_to_mesh",
 ]
 
 _C = None
@@ -293,3 +294,66 @@ def mesh_to_flexible_dual_grid_batch(
     return _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
                                                         float(boundary_weight), float(regularization_weight),
                                                         int(workers), _order_code(order))
+
+
+@torch.no_grad()
+def flexible_dual_grid_to_mesh(
+    coords: torch.Tensor,
+    dual_vertices: torch.Tensor,
+    intersected_flag: torch.Tensor,
+    split_weight: Optional[torch.Tensor],
+    aabb: ArrayLike,
+    voxel_size: Optional[FloatArrayLike] = None,
+    grid_size: Optional[IntArrayLike] = None,
+    train: bool = False,
+):
+    """
+    Extract a triangle mesh from a sparse flexible dual grid (the inverse path of
+    mesh_to_flexible_dual_grid; reference o_voxel/convert/flexible_dual_grid.py:332-477).
+
+    Every intersected voxel edge whose four surrounding voxels are active gives
+    one quad of their dual vertices, split into two triangles (by the larger
+    normal alignment, or by split_weight), or into four around a weighted middle
+    vertex in training mode.
+
+    Args:
+        coords: [N, 3] voxel coordinates (CUDA).
+        dual_vertices: [N, 3] dual vertices as offsets inside their voxels (voxel units).
+        intersected_flag: [N, 3] bool edge flags.
+        split_weight: [N] or [N, 1] split weights, or None.
+        aabb: [[x0, y0, z0], [x1, y1, z1]].
+        voxel_size / grid_size: one of them is required.
+        train: training-mode split (needs split_weight).
+
+    Returns:
+        vertices ([N (+ quads in training mode), 3] float32, world coordinates),
+        faces ([2 * quads (4 * quads in training mode), 3] int32).
+    """
+    _require_cuda(coords, "flexible_dual_grid_to_mesh")
+    if isinstance(aabb, (list, tuple)):
+        aabb = np.array(aabb)
+    if isinstance(aabb, np.ndarray):
+        aabb = torch.tensor(aabb, dtype=torch.float32)
+    assert isinstance(aabb, torch.Tensor), f"aabb must be a list, tuple, np.ndarray, or torch.Tensor, but got {type(aabb)}"
+    aabb = aabb.detach().to("cpu", torch.float32)
+    assert aabb.dim() == 2 and aabb.size(0) == 2 and aabb.size(1) == 3, f"aabb must be [2, 3], got {tuple(aabb.shape)}"
+    if voxel_size is not None:
+        if isinstance(voxel_size, float):
+            voxel_size = [voxel_size, voxel_size, voxel_size]
+        vs_t = torch.as_tensor(np.asarray(voxel_size) if not isinstance(voxel_size, torch.Tensor) else voxel_size,
+                               dtype=torch.float32).cpu()
+        gs_t = ((aabb[1] - aabb[0]) / vs_t).round().int()
+    else:
+        assert grid_size is not None, "Either voxel_size or grid_size must be provided"
+        if isinstance(grid_size, int):
+            grid_size = [grid_size, grid_size, grid_size]
+        gs_t = torch.as_tensor(np.asarray(grid_size) if not isinstance(grid_size, torch.Tensor) else grid_size,
+                               dtype=torch.int32).cpu()
+        vs_t = (aabb[1] - aabb[0]) / gs_t
+    assert vs_t.numel() == 3 and gs_t.numel() == 3, "voxel_size and grid_size must have 3 elements"
+    sw = None
+    if split_weight is not None:
+        sw = split_weight.reshape(-1)
+    return _ext().flexible_dual_grid_to_mesh_cuda(coords, dual_vertices, intersected_flag, sw,
+                                                  [int(x) for x in gs_t.tolist()], [float(x) for x in vs_t.tolist()],
+                                                  [float(x) for x in aabb[0].tolist()], bool(train))

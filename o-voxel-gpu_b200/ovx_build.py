@@ -35,11 +35,11 @@ def _sources(*names):
 
 
 def build_lib(force=False, verbose=False):
-    srcs = _sources("fdg_kernels.cu", "fdg_device.cuh")
+    srcs = _sources("fdg_kernels.cu", "fdg_mesh.cu", "fdg_device.cuh")
     if not (force or _newer(LIB, srcs)):
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [NVCC, *ARCH, *NVCC_FLAGS, "-shared", "-I", INCLUDE, srcs[0], "-o", LIB]
+    cmd = [NVCC, *ARCH, *NVCC_FLAGS, "-shared", "-I", INCLUDE, srcs[0], srcs[1], "-o", LIB]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     subprocess.check_call(cmd)

@@ -35,6 +35,12 @@ PROTOTYPES = [
     ("ovx_fdg_set_output_order", ctypes.c_int, [_P, ctypes.c_int]),
     ("ovx_z_order_encode", ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
     ("ovx_z_order_decode", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
+    ("ovx_fdg_mesh_context_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    ("ovx_fdg_mesh_context_destroy", None, [_P]),
+    ("ovx_fdg_mesh_last_error", ctypes.c_char_p, [_P]),
+    ("ovx_fdg_to_mesh_begin", ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _P, _P, _P, ctypes.c_int32,
+                                             ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
+    ("ovx_fdg_to_mesh_finish", ctypes.c_int, [_P, _P, _P, _P]),
     ("ovx_fdg_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.c_int32, _I64, _P, _P, _F, _F, _F, ctypes.POINTER(_I64)]),
     ("ovx_fdg_finish", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("ovx_fdg_sync_status", ctypes.c_int, [_P, _P]),
