@@ -112,6 +112,16 @@ int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order);
 int ovx_z_order_encode(void *stream, const int32_t *x, const int32_t *y, const int32_t *z, int64_t n, int32_t *codes);
 int ovx_z_order_decode(void *stream, const int32_t *codes, int64_t n, int32_t *x, int32_t *y, int32_t *z);
 
+/*
+ * .vxz attribute packing of a conversion's outputs, as the reference's example
+ * does before writing (examples/mesh2ovox.py:51-54): dual_u8[i][a] =
+ * uint8(clamp(dual[i][a] * resolution[a] - voxel[i][a], 0, 1) * 255) (float32,
+ * truncating), intersected_u8[i] = x + 2y + 4z of the three flags.  Device
+ * arrays of n rows, enqueued on `stream`.
+ */
+int ovx_fdg_pack(void *stream, const int32_t *voxel_indices, const float *dual_vertices, const uint8_t *intersected,
+                 int64_t n, const float resolution[3], uint8_t *dual_u8, uint8_t *intersected_u8);
+
 /* Sizes of the last conversion, known after ovx_fdg_begin: out[0] voxel rows,
  * out[1] occupied 8^3 bricks, out[2] quadric records bucketed by brick,
  * out[3] boundary edges, out[4] bricks of the grid.  Writes min(capacity, 5)

@@ -352,6 +352,29 @@ std::tuple<torch::Tensor, torch::Tensor> flexible_dual_grid_to_mesh_cuda(
     return std::make_tuple(verts, tris);
 }
 
+// .vxz attribute packing (reference examples/mesh2ovox.py:51-54)
+std::tuple<torch::Tensor, torch::Tensor> pack_flexible_dual_grid_cuda(const torch::Tensor &voxels, const torch::Tensor &dual,
+                                                                     const torch::Tensor &intersected, const std::vector<float> &resolution)
+{
+    TORCH_CHECK(voxels.is_cuda() && dual.is_cuda() && intersected.is_cuda(), "pack_flexible_dual_grid: CUDA tensors expected");
+    TORCH_CHECK(resolution.size() == 3, "resolution must have 3 values");
+    const int64_t n = voxels.size(0);
+    TORCH_CHECK(dual.numel() == 3 * n && intersected.numel() == 3 * n, "inputs must all have N x 3 entries");
+    const c10::cuda::CUDAGuard guard(voxels.device());
+    auto v = voxels.to(torch::kInt32).contiguous();
+    auto d = dual.to(torch::kFloat32).contiguous();
+    auto f = intersected.to(torch::kUInt8).contiguous();
+    auto opts = torch::TensorOptions().device(voxels.device()).dtype(torch::kUInt8);
+    auto du = torch::empty({n, 3}, opts);
+    auto fu = torch::empty({n, 1}, opts);
+    const float r[3] = {resolution[0], resolution[1], resolution[2]};
+    const int rc = ovx_fdg_pack(at::cuda::getCurrentCUDAStream(voxels.get_device()).stream(), n ? v.data_ptr<int32_t>() : nullptr,
+                                n ? d.data_ptr<float>() : nullptr, n ? f.data_ptr<uint8_t>() : nullptr, n, r,
+                                n ? du.data_ptr<uint8_t>() : nullptr, n ? fu.data_ptr<uint8_t>() : nullptr);
+    TORCH_CHECK(rc == OVX_FDG_OK, "pack_flexible_dual_grid failed: ", ovx_fdg_status_string(rc));
+    return std::make_tuple(du, fu);
+}
+
 // o_voxel.serialize z-order codes (reference: src/ext.cpp:28-29, src/serialize/api.cu)
 torch::Tensor z_order_encode_cuda(const torch::Tensor &x, const torch::Tensor &y, const torch::Tensor &z)
 {
@@ -397,5 +420,6 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
           py::call_guard<py::gil_scoped_release>());
     m.def("z_order_encode_cuda", &z_order_encode_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("flexible_dual_grid_to_mesh_cuda", &flexible_dual_grid_to_mesh_cuda, py::call_guard<py::gil_scoped_release>());
+    m.def("pack_flexible_dual_grid_cuda", &pack_flexible_dual_grid_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("z_order_decode_cuda", &z_order_decode_cuda, py::call_guard<py::gil_scoped_release>());
 }

@@ -844,6 +844,8 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
         __syncwarp();
         for (uint32_t dm = dmask; dm; dm &= dm - 1u)
         {
+            // one dense item: its candidates are compacted into the shared list,
+            // then tested by all lanes with the triangle's coefficients in registers
             const int sd = __ffs(dm) - 1;
             const int so = W.own[sd];
             float c[kFaceCoef];
@@ -853,17 +855,23 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
             const int w = lane >> 1;
             const uint32_t word = W.cand[w][sd];
             uint32_t bits = (lane & 1) ? (word & 0xffff0000u) : (word & 0x0000ffffu);
-            uint32_t hit = 0;
-            const int ox = W.org[0][sd], oy = W.org[1][sd] + (w & 1) * 4, oz = W.org[2][sd] + (w >> 1);
+            uint32_t ntot;
+            uint32_t pos = warp_exclusive_scan((uint32_t)__popc(bits), ntot);
             while (bits)
             {
                 const int bt = __ffs(bits) - 1;
                 bits &= bits - 1u;
-                if (face_test_c(FaceCoefArr{c}, g, ox + (bt & 7), oy + (bt >> 3), oz))
-                    hit |= 1u << bt;
+                W.cl[pos++] = (uint16_t)(w * 32 + bt);
             }
-            if (hit)
-                atomicOr(&W.pass[w][sd], hit);
+            __syncwarp();
+            const int ox = W.org[0][sd], oy = W.org[1][sd], oz = W.org[2][sd];
+            for (uint32_t k = lane; k < ntot; k += 32)
+            {
+                const int lv = W.cl[k];
+                if (face_test_c(FaceCoefArr{c}, g, ox + (lv & 7), oy + ((lv >> 3) & 7), oz + (lv >> 6)))
+                    atomicOr(&W.pass[lv >> 5][sd], 1u << (lv & 31));
+            }
+            __syncwarp();
         }
         const uint32_t lcnt = dense ? 0u : cnt;
         uint32_t off = lcnt;
@@ -1975,6 +1983,26 @@ __global__ void zorder_bases(const uint32_t *__restrict__ sorted_slots, long lon
         zbase[active[sorted_slots[j]]] = base_sorted[j];
 }
 
+// .vxz attribute packing of a conversion's outputs (examples/mesh2ovox.py:51-54):
+// dual vertex -> clamp(dual * res - coord, 0, 1) * 255 truncated to uint8, one
+// operation at a time in float32 as there; flags -> x + 2y + 4z in one byte.
+__global__ void fdg_pack_kernel(const int32_t *__restrict__ vox, const float *__restrict__ dual, const uint8_t *__restrict__ inter,
+                                long long n, float r0, float r1, float r2, uint8_t *__restrict__ dual_u8, uint8_t *__restrict__ inter_u8)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float r[3] = {r0, r1, r2};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        float d = __fsub_rn(__fmul_rn(dual[i * 3 + a], r[a]), (float)vox[i * 3 + a]);
+        d = fminf(fmaxf(d, 0.0f), 1.0f);
+        dual_u8[i * 3 + a] = (uint8_t)(int)__fmul_rn(d, 255.0f);
+    }
+    inter_u8[i] = (uint8_t)((inter[i * 3 + 0] ? 1 : 0) + 2 * (inter[i * 3 + 1] ? 1 : 0) + 4 * (inter[i * 3 + 2] ? 1 : 0));
+}
+
 // o_voxel.serialize z-order codes (serialize/z_order.cu:33-97): 10 bits per coordinate.
 __global__ void z_order_encode_kernel(const int32_t *__restrict__ x, const int32_t *__restrict__ y, const int32_t *__restrict__ z,
                                       long long n, int32_t *__restrict__ codes)
@@ -2638,6 +2666,18 @@ int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order)
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "unknown output order");
     ctx->order = order;
     return OVX_FDG_OK;
+}
+
+int ovx_fdg_pack(void *stream, const int32_t *voxel_indices, const float *dual_vertices, const uint8_t *intersected,
+                 int64_t n, const float resolution[3], uint8_t *dual_u8, uint8_t *intersected_u8)
+{
+    if (n < 0 || !resolution || (n > 0 && (!voxel_indices || !dual_vertices || !intersected || !dual_u8 || !intersected_u8)))
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (n == 0)
+        return OVX_FDG_OK;
+    fdg_pack_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(voxel_indices, dual_vertices, intersected, n, resolution[0],
+                                                                          resolution[1], resolution[2], dual_u8, intersected_u8);
+    return cudaGetLastError() == cudaSuccess ? OVX_FDG_OK : OVX_FDG_CUDA_ERROR;
 }
 
 int ovx_z_order_encode(void *stream, const int32_t *x, const int32_t *y, const int32_t *z, int64_t n, int32_t *codes)

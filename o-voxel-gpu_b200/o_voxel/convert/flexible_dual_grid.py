@@ -30,6 +30,7 @@ __all__ = [
     "mesh_to_flexible_dual_grid_batch",
     "intersect_occ",
     "flexible_dual_grid_to_mesh",
+    "pack_flexible_dual_grid",
 ]
 
 _C = None
@@ -357,3 +358,24 @@ def flexible_dual_grid_to_mesh(
     return _ext().flexible_dual_grid_to_mesh_cuda(coords, dual_vertices, intersected_flag, sw,
                                                   [int(x) for x in gs_t.tolist()], [float(x) for x in vs_t.tolist()],
                                                   [float(x) for x in aabb[0].tolist()], bool(train))
+
+
+@torch.no_grad()
+def pack_flexible_dual_grid(voxel_indices: torch.Tensor, dual_vertices: torch.Tensor, intersected: torch.Tensor,
+                            grid_size: IntArrayLike) -> Tuple[torch.Tensor, torch.Tensor]:
+    """
+    Pack a conversion's outputs into the .vxz attributes the reference's example
+    writes (examples/mesh2ovox.py:51-54), in one kernel:
+
+        dual_vertices_u8 = uint8(clamp(dual_vertices * grid_size - voxel_indices, 0, 1) * 255)   [N, 3]
+        intersected_u8   = x + 2 y + 4 z of the edge flags                                 [N, 1]
+
+    dual_vertices are the grid-local outputs of mesh_to_flexible_dual_grid over a
+    unit-extent aabb (as in that example); grid_size is an int or three ints.
+    """
+    _require_cuda(voxel_indices, "pack_flexible_dual_grid")
+    if isinstance(grid_size, int):
+        grid_size = [grid_size] * 3
+    res = [float(np.float32(x)) for x in (grid_size.tolist() if isinstance(grid_size, torch.Tensor) else grid_size)]
+    assert len(res) == 3, "grid_size must be an int or 3 values"
+    return _ext().pack_flexible_dual_grid_cuda(voxel_indices, dual_vertices, intersected, res)
