@@ -284,35 +284,42 @@ def run_ours(args, rank, world):
     stages = ctx.stage_times()
     ctx.set_profiling(False)
 
-    # end to end through the public API, host buffers
+    # end to end through the public API, host buffers: every step copies its
+    # inputs in from pinned host memory, converts, and copies all outputs back.
+    # Steps alternate between two streams so that one step's output copy
+    # overlaps the next step's conversion (the library orders the conversions
+    # themselves); the time is the whole run's, start to finish.
     vh = torch.from_numpy(w.vertices).pin_memory()
     fh = torch.from_numpy(w.faces).pin_memory()
-    vox_h = torch.empty((N, 3), dtype=torch.int32).pin_memory()
-    dual_h = torch.empty((N, 3), dtype=torch.float32).pin_memory()
-    flag_h = torch.empty((N, 3), dtype=torch.bool).pin_memory()
+    slots = [tuple(torch.empty((N, 3), dtype=dt).pin_memory() for dt in (torch.int32, torch.float32, torch.bool))
+             for _ in range(2)]
+    streams = [torch.cuda.Stream(dev) for _ in range(2)]
 
-    def e2e_step():
-        vdev = vh.to(dev, non_blocking=True)
-        fdev = fh.to(dev, non_blocking=True)
-        a, b, c = o_voxel.convert.mesh_to_flexible_dual_grid(vdev, fdev, **w.kwargs())
-        vox_h.copy_(a, non_blocking=True)
-        dual_h.copy_(b, non_blocking=True)
-        flag_h.copy_(c, non_blocking=True)
+    def e2e_step(k):
+        with torch.cuda.stream(streams[k % 2]):
+            vdev = vh.to(dev, non_blocking=True)
+            fdev = fh.to(dev, non_blocking=True)
+            outs = o_voxel.convert.mesh_to_flexible_dual_grid(vdev, fdev, **w.kwargs())
+            for h, d in zip(slots[k % 2], outs):
+                h.copy_(d, non_blocking=True)
 
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
-    ems = []
-    for _ in range(args.steps):
-        flush.zero_()
+    def e2e_run(steps):
+        torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        e2e_step()
+        for st_ in streams:
+            st_.wait_event(e0)
+        for k in range(steps):
+            e2e_step(k)
+        for st_ in streams:
+            stream.wait_stream(st_)
         e1.record(stream)
         e1.synchronize()
-        ems.append(e0.elapsed_time(e1))
-    te = torch.tensor([sum(ems)], dtype=torch.float64, device=dev)
+        return e0.elapsed_time(e1)
+
+    e2e_run(2)
+    te = torch.tensor([e2e_run(args.steps)], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
     e2e_ms = float(te.item()) / args.steps
@@ -351,7 +358,8 @@ def run_ours(args, rank, world):
         "meshes_per_s": world / (ms_per_step / 1e3),
         "batched": batched,
         "e2e": {"value": e2e_value, "unit": "Mfaces/s", "ms_per_step": e2e_ms, "h2d_bytes_per_step": 12 * V + 8 * 3 * F,
-                "d2h_bytes_per_step": 27 * N, "api": "o_voxel.convert.mesh_to_flexible_dual_grid"},
+                "d2h_bytes_per_step": 27 * N, "api": "o_voxel.convert.mesh_to_flexible_dual_grid",
+                "pipelining": "two streams; a step's output copy overlaps the next step's conversion; whole-run time"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind,
                      "scope": "whole conversion: compulsory bytes 12V+24F+27N over the conversion time",

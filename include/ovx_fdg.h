@@ -30,7 +30,9 @@
  * provides output buffers with N rows and `finish` enqueues the quadric and
  * solve stages on the stream and returns without synchronising.  A
  * context holds its device workspace and the state between the two calls; it
- * is not safe to use one context from two threads at once.
+ * is not safe to use one context from two threads at once.  Conversions on
+ * one context may use different streams: each begin first waits for the work
+ * the previous conversion queued, so the workspace is never shared while in use.
  */
 #ifndef OVX_FDG_H
 #define OVX_FDG_H

@@ -2214,6 +2214,10 @@ struct ovx_fdg_context
     long long launches = 0; // kernels this library launched (its own, not CUB's)
     bool profiling = false;
     cudaEvent_t ev[kStageEvents] = {};
+    // end of the last conversion's queued work: the next conversion, possibly
+    // on another stream, waits for it before reusing the workspace
+    cudaEvent_t done = nullptr;
+    bool done_valid = false;
 };
 
 namespace
@@ -2236,6 +2240,27 @@ void stage(ovx_fdg_context *c, int i, cudaStream_t st)
 {
     if (c->profiling && c->ev[i])
         cudaEventRecord(c->ev[i], st);
+}
+
+// Orders this call after the context's previous conversion, whatever its stream.
+cudaError_t wait_previous(ovx_fdg_context *c, cudaStream_t st)
+{
+    if (!c->done_valid)
+        return cudaSuccess;
+    return cudaStreamWaitEvent(st, c->done, 0);
+}
+
+cudaError_t mark_done(ovx_fdg_context *c, cudaStream_t st)
+{
+    if (!c->done)
+    {
+        const cudaError_t e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+        if (e != cudaSuccess)
+            return e;
+    }
+    const cudaError_t e = cudaEventRecord(c->done, st);
+    c->done_valid = e == cudaSuccess;
+    return e;
 }
 
 int fail(ovx_fdg_context *c, int status, const char *what)
@@ -2644,13 +2669,15 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(ctx->device);
-    Buf *list[32];
+    Buf *list[48];
     const int n = buffer_list(ctx, list);
     for (int i = 0; i < n; ++i)
         if (list[i]->p)
             cudaFree(list[i]->p);
     if (ctx->host)
         cudaFreeHost(ctx->host);
+    if (ctx->done)
+        cudaEventDestroy(ctx->done);
     for (int i = 0; i < kStageEvents; ++i)
         if (ctx->ev[i])
             cudaEventDestroy(ctx->ev[i]);
@@ -2794,7 +2821,7 @@ int64_t ovx_fdg_workspace_bytes(const ovx_fdg_context *ctx)
 {
     if (!ctx)
         return 0;
-    Buf *list[32];
+    Buf *list[48];
     const int n = buffer_list(const_cast<ovx_fdg_context *>(ctx), list);
     int64_t s = 0;
     for (int i = 0; i < n; ++i)
@@ -2839,6 +2866,7 @@ int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int
     ctx->fw = face_weight;
     ctx->bw = boundary_weight;
     ctx->rw = regularization_weight;
+    OVX_CUDA(wait_previous(ctx, (cudaStream_t)stream));
     rc = occupancy_stage(ctx, (cudaStream_t)stream, true, num_voxels);
     if (rc != OVX_FDG_OK)
         return rc;
@@ -2935,6 +2963,7 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     stage(ctx, EV_CONSTRAINED, st);
     OVX_CUDA(cudaGetLastError());
     OVX_CUDA(cudaMemcpyAsync(&ctx->host[8], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
+    OVX_CUDA(mark_done(ctx, st));
     ctx->finished = 1;
     return OVX_FDG_OK;
 }
@@ -2980,6 +3009,7 @@ int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *tri
     ctx->fw = 0.0f;
     ctx->bw = 0.0f;
     ctx->rw = 0.0f;
+    OVX_CUDA(wait_previous(ctx, (cudaStream_t)stream));
     rc = occupancy_stage(ctx, (cudaStream_t)stream, false, num_voxels);
     if (rc != OVX_FDG_OK)
         return rc;
@@ -3012,6 +3042,7 @@ int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_
                                                           ctx->g, ctx->order == 1, voxel_indices);
     ++ctx->launches;
     OVX_CUDA(cudaGetLastError());
+    OVX_CUDA(mark_done(ctx, st));
     return OVX_FDG_OK;
 }
 

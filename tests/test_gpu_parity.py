@@ -162,3 +162,30 @@ def test_face_record_staging_and_fallback(cuda):
             assert_fdg_equal(tuple(t.cpu().numpy() for t in out), want, f"face_heavy ({step})")
     finally:
         ctx.close()
+
+
+@pytest.mark.gpu
+def test_two_streams_share_the_context(cuda):
+    """Back-to-back conversions on two streams through the shared context: the
+    second waits for the first's queued work, so both stay exact."""
+    import torch
+    import o_voxel
+
+    wa = W.primitives(2, faces_total=60_000)
+    wb = W.ico_cap(3)
+    sa, sb = torch.cuda.Stream(cuda), torch.cuda.Stream(cuda)
+    va, fa = torch.from_numpy(wa.vertices).to(cuda), torch.from_numpy(wa.faces).to(cuda)
+    vb, fb = torch.from_numpy(wb.vertices).to(cuda), torch.from_numpy(wb.faces).to(cuda)
+    torch.cuda.synchronize()
+    outs = []
+    for _ in range(3):
+        with torch.cuda.stream(sa):
+            oa = o_voxel.convert.mesh_to_flexible_dual_grid(va, fa, **wa.kwargs())
+        with torch.cuda.stream(sb):
+            ob = o_voxel.convert.mesh_to_flexible_dual_grid(vb, fb, **wb.kwargs())
+        outs.append((oa, ob))
+    torch.cuda.synchronize()
+    ra, rb = _oracle(wa), _oracle(wb)
+    for oa, ob in outs:
+        assert_fdg_equal(tuple(t.cpu().numpy() for t in oa), ra, "stream a")
+        assert_fdg_equal(tuple(t.cpu().numpy() for t in ob), rb, "stream b")
