@@ -85,7 +85,8 @@ enum
     C_FSTAGED = 5,
     C_LONG = 6,
     C_HUGE = 7,
-    C_WORDS = 8
+    C_ESTAGED = 8,
+    C_WORDS = 12
 };
 enum
 {
@@ -201,6 +202,8 @@ struct GenArgs
     float *btab;                    // FILL of the boundary pass
     uint4 *fstage;                  // COUNT of the face pass: face records {brick, t, code, 0} (NULL: off)
     uint32_t fstage_cap;
+    uint4 *estage;                  // COUNT of the scanline pass: event records {brick, t, code, z} (NULL: off)
+    uint32_t estage_cap;
     uint32_t *counters;
     uint32_t *scan_large;
     uint32_t scan_large_cap;
@@ -260,15 +263,24 @@ __device__ __forceinline__ void put_record(const GenArgs &A, long long b, uint32
     }
 }
 
+// Records of one scanline event kept for staging (one brick each, at most four).
+struct EventStage
+{
+    uint32_t n;
+    uint32_t b[4], code[4];
+    uint32_t zb, t;
+};
+
 // Scanline event sink: (COUNT) sets the occupancy bits of the four voxels
-// around the grid line and counts one record per distinct brick; (FILL)
-// writes those records.
+// around the grid line and counts one record per distinct brick, optionally
+// keeping the records for staging; (FILL) writes those records.
 template <int M>
 struct EventSink
 {
     const GenArgs &A;
     uint32_t t;
     int ax2;
+    EventStage *es = nullptr;
     __device__ __forceinline__ void operator()(int xi, int yi, int zi, float, float, double z) const
     {
         const Grid &g = A.m.g;
@@ -314,7 +326,7 @@ struct EventSink
             if (dup)
                 continue;
             uint32_t code = 0;
-            if (M == FILL)
+            if (M == FILL || es)
             {
                 int o[3];
                 brick_origin(g, b, o);
@@ -326,6 +338,17 @@ struct EventSink
                        ((uint32_t)(zi - o2) << 10);
             }
             put_record<M>(A, b, t, code, zb);
+            if (M == COUNT && es)
+            {
+                es->b[es->n] = (uint32_t)b;
+                es->code[es->n] = code;
+                ++es->n;
+            }
+        }
+        if (M == COUNT && es)
+        {
+            es->zb = zb;
+            es->t = t;
         }
     }
 };
@@ -486,6 +509,8 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
             const int cyi = __shfl_sync(0xffffffffu, yi, rl);
             const int col = __shfl_sync(0xffffffffu, ol, rl);
             const uint32_t ccs = __shfl_sync(0xffffffffu, cstart, rl);
+            EventStage es;
+            es.n = 0;
             if (c < ncol_all)
             {
                 const long long cta = tabase + col;
@@ -496,9 +521,27 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
                 col_event(cr, xi, (cax2 + 1) % 3, cax2, g, z, zi);
                 if (zi >= g.gmin[cax2] && zi < g.gmax[cax2])
                 {
-                    EventSink<M> sink{A, (uint32_t)(cta / 3), cax2};
+                    EventSink<M> sink{A, (uint32_t)(cta / 3), cax2, (M == COUNT && A.estage) ? &es : nullptr};
                     sink(xi, cyi, zi, 0.0f, 0.0f, z);
                 }
+            }
+            if (M == COUNT && A.estage)
+            {
+                // stage this round's records: one reservation for the warp
+                uint32_t tot;
+                const uint32_t off = warp_exclusive_scan(es.n, tot);
+                uint32_t base = 0;
+                if (lane == 0 && tot)
+                    base = atomicAdd(&A.counters[C_ESTAGED], tot);
+                base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if ((uint32_t)k < es.n)
+                    {
+                        const unsigned long long pos = (unsigned long long)base + off + k;
+                        if (pos < A.estage_cap)
+                            A.estage[pos] = make_uint4(es.b[k], es.t, es.code[k], es.zb);
+                    }
             }
         }
     }
@@ -2192,7 +2235,7 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
     Buf vcnt, voff, emax, bkeys, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, longv;
+    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, estage, longv;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     unsigned long long *host = nullptr; // pinned readback words
     std::string err;
@@ -2209,6 +2252,8 @@ struct ovx_fdg_context
     long long n_vox = 0, n_active = 0, n_rec = 0, n_boundary = 0;
     unsigned long long n_fstaged = 0, fstage_want = 0; // face records staged by the count pass (and the most seen)
     bool face_staged = false;                         // all of them fitted: the fill pass need not redo the tests
+    unsigned long long n_estaged = 0, estage_want = 0; // the same for the scanline event records
+    bool event_staged = false;
     int order = 0;                                    // output row order: 0 brick-linear, 1 z-order
     int finished = 0;
     long long launches = 0; // kernels this library launched (its own, not CUB's)
@@ -2228,7 +2273,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
                 &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage, &c->longv,
+                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv,
                 &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
@@ -2446,6 +2491,8 @@ GenArgs make_gen(ovx_fdg_context *ctx)
     A.btab = (float *)ctx->btab.p;
     A.fstage = (uint4 *)ctx->fstage.p;
     A.fstage_cap = cap_u32(ctx->fstage, sizeof(uint4));
+    A.estage = (uint4 *)ctx->estage.p;
+    A.estage_cap = cap_u32(ctx->estage, sizeof(uint4));
     A.counters = (uint32_t *)ctx->counters.p;
     A.scan_large = (uint32_t *)ctx->scan_large.p;
     A.scan_large_cap = cap_u32(ctx->scan_large, 4);
@@ -2459,7 +2506,17 @@ GenArgs make_gen(ovx_fdg_context *ctx)
 template <int M, typename IdxT>
 void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
 {
-    if (ctx->nf > 0)
+    if (M == FILL && ctx->event_staged)
+    {
+        // the count pass staged the records of every pair but the listed large ones
+        if (ctx->n_estaged > 0)
+        {
+            bucket_records<<<blocks_for((long long)ctx->n_estaged, kThreads), kThreads, 0, st>>>(
+                A.estage, (uint32_t)ctx->n_estaged, A.rcnt, A.roff, A.rec, A.counters);
+            ++ctx->launches;
+        }
+    }
+    else if (ctx->nf > 0)
     {
         tri_events<M, IdxT><<<blocks_for(3 * ctx->nf, kEventThreads), kEventThreads, 0, st>>>(A);
         ++ctx->launches;
@@ -2517,6 +2574,13 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(ensure(ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
         OVX_CUDA(ensure(ctx->qtab, (size_t)(nf + 1) * 40));
+    if (full)
+    {
+        // staging room for the event records: the most seen so far, else a guess
+        const unsigned long long guess = std::min(24ull * (unsigned long long)nf, 4ull * (unsigned long long)nf + (16ull << 20));
+        const unsigned long long want = std::max(ctx->estage_want, guess);
+        OVX_CUDA(ensure(ctx->estage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
+    }
     if (full && ctx->fw > 0.0f)
     {
         // staging room for the face records: the most seen so far, else a guess
@@ -2541,7 +2605,11 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     stage(ctx, EV_BEGIN, st);
     GenArgs A = make_gen(ctx);
     if (!full)
+    {
         A.qtab = nullptr;
+        A.estage = nullptr; // occupancy only: no records
+        A.estage_cap = 0;
+    }
     if (ctx->fbytes == 8)
         launch_events<COUNT, long long>(ctx, A, st);
     else
@@ -2620,6 +2688,9 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     ctx->n_active = (long long)ctx->host[1];
     ctx->n_rec = full ? (long long)ctx->host[2] : 0;
     ctx->n_boundary = hc[C_BOUNDARY];
+    ctx->n_estaged = full ? hc[C_ESTAGED] : 0u;
+    ctx->event_staged = full && ctx->n_estaged <= (unsigned long long)cap_u32(ctx->estage, sizeof(uint4));
+    ctx->estage_want = std::max(ctx->estage_want, ctx->n_estaged);
     ctx->n_fstaged = full ? hc[C_FSTAGED] : 0u;
     ctx->face_staged = full && ctx->n_fstaged <= (unsigned long long)cap_u32(ctx->fstage, sizeof(uint4));
     ctx->fstage_want = std::max(ctx->fstage_want, ctx->n_fstaged);
