@@ -2238,6 +2238,7 @@ struct ovx_fdg_context
     Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, estage, longv;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     unsigned long long *host = nullptr; // pinned readback words
+    cudaMemPool_t pool = nullptr;       // workspace pool (keeps its memory until the context is destroyed)
     std::string err;
     // state between begin and finish
     int phase = 0; // 0 idle, 1 after begin (full), 2 after begin (occupancy only)
@@ -2333,7 +2334,11 @@ int cuda_fail(ovx_fdg_context *c, cudaError_t e, const char *where)
             return cuda_fail(ctx, e_, #call);            \
     } while (0)
 
-cudaError_t ensure(Buf &b, size_t bytes)
+// Grows a workspace buffer in stream order from the context's own memory pool:
+// the old block goes back to the pool behind the work queued on `st`, and no
+// call here waits for the device, so contexts converting on other streams
+// (the batched API's workers) are not stalled when one of them grows.
+cudaError_t ensure(cudaStream_t st, ovx_fdg_context *ctx, Buf &b, size_t bytes)
 {
     if (bytes == 0)
         bytes = 16;
@@ -2341,12 +2346,12 @@ cudaError_t ensure(Buf &b, size_t bytes)
         return cudaSuccess;
     if (b.p)
     {
-        cudaFree(b.p);
+        cudaFreeAsync(b.p, st);
         b.p = nullptr;
         b.cap = 0;
     }
     const size_t want = bytes + bytes / 4 + 256;
-    cudaError_t e = cudaMalloc(&b.p, want);
+    cudaError_t e = cudaMallocFromPoolAsync(&b.p, want, ctx->pool, st);
     if (e != cudaSuccess)
     {
         cudaGetLastError();
@@ -2364,7 +2369,7 @@ cudaError_t exclusive_scan(ovx_fdg_context *ctx, const In *in, Out *out, long lo
     cudaError_t e = cub::DeviceScan::ExclusiveScan(nullptr, bytes, in, out, cub::Sum(), Out(0), (int)n, st);
     if (e != cudaSuccess)
         return e;
-    e = ensure(ctx->cub_tmp, bytes);
+    e = ensure(st, ctx, ctx->cub_tmp, bytes);
     if (e != cudaSuccess)
         return e;
     return cub::DeviceScan::ExclusiveScan(ctx->cub_tmp.p, bytes, in, out, cub::Sum(), Out(0), (int)n, st);
@@ -2380,11 +2385,11 @@ inline unsigned blocks_for(long long n, int threads)
 int zorder_row_bases(ovx_fdg_context *ctx, cudaStream_t st)
 {
     const long long na = ctx->n_active, nb = ctx->g.nbricks;
-    OVX_CUDA(ensure(ctx->zkeys, (size_t)(na + 1) * 16));
-    OVX_CUDA(ensure(ctx->zslots, (size_t)(na + 1) * 8));
-    OVX_CUDA(ensure(ctx->zcnt, (size_t)(na + 1) * 4));
-    OVX_CUDA(ensure(ctx->zsbase, (size_t)(na + 1) * 8));
-    OVX_CUDA(ensure(ctx->zbase, (size_t)(nb + 1) * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->zkeys, (size_t)(na + 1) * 16));
+    OVX_CUDA(ensure(st, ctx, ctx->zslots, (size_t)(na + 1) * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->zcnt, (size_t)(na + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->zsbase, (size_t)(na + 1) * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->zbase, (size_t)(nb + 1) * 8));
     if (na == 0)
         return OVX_FDG_OK;
     unsigned long long *kin = (unsigned long long *)ctx->zkeys.p, *kout = kin + (na + 1);
@@ -2402,7 +2407,7 @@ int zorder_row_bases(ovx_fdg_context *ctx, cudaStream_t st)
     const int end_bit = std::min(63, 3 * cb);
     size_t bytes = 0;
     OVX_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, (int)na, 0, end_bit, st));
-    OVX_CUDA(ensure(ctx->cub_tmp, bytes));
+    OVX_CUDA(ensure(st, ctx, ctx->cub_tmp, bytes));
     OVX_CUDA(cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, bytes, kin, kout, vin, vout, (int)na, 0, end_bit, st));
     zorder_counts<<<blocks_for(na + 1, 256), 256, 0, st>>>(vout, na, active, (const uint32_t *)ctx->bcount.p,
                                                           (uint32_t *)ctx->zcnt.p);
@@ -2561,40 +2566,40 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     const Grid &g = ctx->g;
     const long long nf = ctx->nf, nb = g.nbricks;
     const bool boundary = full && ctx->bw > 0.0f;
-    OVX_CUDA(ensure(ctx->bits, (size_t)nb * kWordsPerBrick * 4));
-    OVX_CUDA(ensure(ctx->bcount, (size_t)(nb + 1) * 4));
-    OVX_CUDA(ensure(ctx->bbase, (size_t)(nb + 1) * 8));
-    OVX_CUDA(ensure(ctx->aflag, (size_t)(nb + 1) * 4));
-    OVX_CUDA(ensure(ctx->aslot, (size_t)(nb + 1) * 8));
-    OVX_CUDA(ensure(ctx->active, (size_t)(nb + 1) * 4));
-    OVX_CUDA(ensure(ctx->counters, C_WORDS * 4));
-    OVX_CUDA(ensure(ctx->scan_large, (size_t)(3 * nf + 1) * 4));
-    OVX_CUDA(ensure(ctx->face_large, (size_t)(nf + 1) * 4));
-    OVX_CUDA(ensure(ctx->rcnt, (size_t)(nb + 1) * 4));
-    OVX_CUDA(ensure(ctx->roff, (size_t)(nb + 1) * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->bits, (size_t)nb * kWordsPerBrick * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->bcount, (size_t)(nb + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->bbase, (size_t)(nb + 1) * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->aflag, (size_t)(nb + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->aslot, (size_t)(nb + 1) * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->active, (size_t)(nb + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->counters, C_WORDS * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->scan_large, (size_t)(3 * nf + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->face_large, (size_t)(nf + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->rcnt, (size_t)(nb + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
-        OVX_CUDA(ensure(ctx->qtab, (size_t)(nf + 1) * 40));
+        OVX_CUDA(ensure(st, ctx, ctx->qtab, (size_t)(nf + 1) * 40));
     if (full)
     {
         // staging room for the event records: the most seen so far, else a guess
         const unsigned long long guess = std::min(24ull * (unsigned long long)nf, 4ull * (unsigned long long)nf + (16ull << 20));
         const unsigned long long want = std::max(ctx->estage_want, guess);
-        OVX_CUDA(ensure(ctx->estage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
+        OVX_CUDA(ensure(st, ctx, ctx->estage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
     }
     if (full && ctx->fw > 0.0f)
     {
         // staging room for the face records: the most seen so far, else a guess
         const unsigned long long guess = std::min(24ull * (unsigned long long)nf, 4ull * (unsigned long long)nf + (16ull << 20));
         const unsigned long long want = std::max(ctx->fstage_want, guess);
-        OVX_CUDA(ensure(ctx->fstage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
+        OVX_CUDA(ensure(st, ctx, ctx->fstage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
     }
     if (boundary)
     {
-        OVX_CUDA(ensure(ctx->vcnt, (size_t)(ctx->nv + 1) * 4));
-        OVX_CUDA(ensure(ctx->voff, (size_t)(ctx->nv + 1) * 8));
-        OVX_CUDA(ensure(ctx->emax, (size_t)(3 * nf + 1) * 4));
-        OVX_CUDA(ensure(ctx->bkeys, (size_t)(3 * nf + 1) * 8));
-        OVX_CUDA(ensure(ctx->boff, (size_t)(ctx->nv + 1) * 8));
+        OVX_CUDA(ensure(st, ctx, ctx->vcnt, (size_t)(ctx->nv + 1) * 4));
+        OVX_CUDA(ensure(st, ctx, ctx->voff, (size_t)(ctx->nv + 1) * 8));
+        OVX_CUDA(ensure(st, ctx, ctx->emax, (size_t)(3 * nf + 1) * 4));
+        OVX_CUDA(ensure(st, ctx, ctx->bkeys, (size_t)(3 * nf + 1) * 8));
+        OVX_CUDA(ensure(st, ctx, ctx->boff, (size_t)(ctx->nv + 1) * 8));
     }
     OVX_CUDA(cudaMemsetAsync(ctx->bits.p, 0, (size_t)nb * kWordsPerBrick * 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->counters.p, 0, C_WORDS * 4, st));
@@ -2723,9 +2728,31 @@ int ovx_fdg_context_create(int device, ovx_fdg_context **out)
     cudaSetDevice(device);
     cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
     cudaError_t e = cudaMallocHost((void **)&ctx->host, 32 * sizeof(unsigned long long));
+    if (e == cudaSuccess)
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&ctx->pool, &props);
+        if (e == cudaSuccess)
+        {
+            // freed blocks stay with the pool for the next growth instead of
+            // going back to the driver at every synchronisation
+            unsigned long long keep = ~0ull;
+            e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        else
+            ctx->pool = nullptr;
+    }
     cudaSetDevice(prev);
     if (e != cudaSuccess)
     {
+        cudaGetLastError();
+        if (ctx->pool)
+            cudaMemPoolDestroy(ctx->pool);
+        if (ctx->host)
+            cudaFreeHost(ctx->host);
         delete ctx;
         return OVX_FDG_OUT_OF_MEMORY;
     }
@@ -2744,7 +2771,9 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
     const int n = buffer_list(ctx, list);
     for (int i = 0; i < n; ++i)
         if (list[i]->p)
-            cudaFree(list[i]->p);
+            cudaFree(list[i]->p); // waits for the device, then returns the block to the pool
+    if (ctx->pool)
+        cudaMemPoolDestroy(ctx->pool);
     if (ctx->host)
         cudaFreeHost(ctx->host);
     if (ctx->done)
@@ -2961,12 +2990,12 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     cudaStream_t st = (cudaStream_t)stream;
     OVX_CUDA(cudaSetDevice(ctx->device));
     const long long nb = ctx->g.nbricks;
-    OVX_CUDA(ensure(ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
-    OVX_CUDA(ensure(ctx->btab, (size_t)(ctx->n_boundary + 1) * 40));
-    OVX_CUDA(ensure(ctx->clist, (size_t)(n + 1) * 16 * 4));
-    OVX_CUDA(ensure(ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
-    OVX_CUDA(ensure(ctx->vlist, (size_t)n * 8));
-    OVX_CUDA(ensure(ctx->longv, (size_t)(n + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
+    OVX_CUDA(ensure(st, ctx, ctx->btab, (size_t)(ctx->n_boundary + 1) * 40));
+    OVX_CUDA(ensure(st, ctx, ctx->clist, (size_t)(n + 1) * 16 * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
+    OVX_CUDA(ensure(st, ctx, ctx->vlist, (size_t)n * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->longv, (size_t)(n + 1) * 4));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_LONG, 0, 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONSTRAINED, 0, 4, st));
