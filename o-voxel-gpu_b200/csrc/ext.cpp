@@ -248,17 +248,25 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
                                     f.scalar_type() == torch::kInt64 ? 8 : 4, f.size(0), o, &grid, face_weight,
                                     boundary_weight, regularization_weight, &nv),
                       dc.ctx, "mesh_to_flexible_dual_grid_batch (occupancy)");
-                auto opts = torch::TensorOptions().device(dev);
-                auto vox = torch::empty({nv, 3}, opts.dtype(torch::kInt32));
-                auto dual = torch::empty({nv, 3}, opts.dtype(torch::kFloat32));
-                auto inter = torch::empty({nv, 3}, opts.dtype(torch::kBool));
+                // The outputs belong to the caller's stream, so that the caching
+                // allocator reuses their blocks from one call to the next (the
+                // pool hands out other worker streams each call); the worker
+                // stream that writes them is recorded on them.  Blocks the caller
+                // freed earlier are safe here: this stream waited for the caller.
+                torch::Tensor vox, dual, inter;
+                {
+                    const c10::cuda::CUDAStreamGuard cg(caller);
+                    auto opts = torch::TensorOptions().device(dev);
+                    vox = torch::empty({nv, 3}, opts.dtype(torch::kInt32));
+                    dual = torch::empty({nv, 3}, opts.dtype(torch::kFloat32));
+                    inter = torch::empty({nv, 3}, opts.dtype(torch::kBool));
+                }
                 check(ovx_fdg_finish(dc.ctx, st, nv ? vox.data_ptr<int32_t>() : nullptr, nv ? dual.data_ptr<float>() : nullptr,
                                      nv ? reinterpret_cast<uint8_t *>(inter.data_ptr<bool>()) : nullptr),
                       dc.ctx, "mesh_to_flexible_dual_grid_batch (quadrics)");
-                // the outputs are handed to the caller's stream
-                vox.record_stream(caller);
-                dual.record_stream(caller);
-                inter.record_stream(caller);
+                vox.record_stream(streams[w]);
+                dual.record_stream(streams[w]);
+                inter.record_stream(streams[w]);
                 out[i] = std::make_tuple(vox, dual, inter);
             }
             static const bool sync_check = std::getenv("OVX_FDG_CHECK") != nullptr;

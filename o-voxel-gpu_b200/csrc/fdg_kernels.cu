@@ -26,15 +26,23 @@
 //   btab    line quadric per boundary edge (10 floats)
 //
 // begin (ends with the one host synchronisation of a conversion):
-//   tri_events<COUNT>   one thread per (triangle, axis): scanline events (FP64,
-//                       reference arithmetic) set occupancy bits and count
-//                       event records per brick; the quadric table is written
+//   tri_events<COUNT>   one (triangle, axis) per lane: scanline events (FP64,
+//                       reference arithmetic) set occupancy bits, count event
+//                       records per brick and stage them; the quadric table is
+//                       written; large pairs are listed
+//   large_rows<COUNT>   the listed pairs, cut into units of a few rows
 //   compaction          brick popcounts, scans -> N, active bricks
 //   edges               undirected edges bucketed by smaller vertex; edges
 //                       used once -> boundary list
-//   face_records<COUNT>, boundary_records<COUNT>, scan -> record offsets
+//   face_records<COUNT> one triangle per lane: face tests, records counted and
+//                       staged; triangles over many bricks are listed
+//   large_faces<COUNT>  the listed triangles, 32 bricks per warp
+//   boundary_records<COUNT>, scan -> record offsets
 // finish (no synchronisation):
-//   *_records<FILL>     the same generators write the records
+//   bucket_records      staged event and face records -> brick buckets (when
+//                       a staging buffer overflowed, the generators rerun in
+//                       FILL mode and write the records instead)
+//   boundary_records<FILL>
 //   brick_lists         one CTA per active brick: records -> per-voxel
 //                       contribution lists {key, payload} in global memory
 //                       (a counting sort by voxel; records are taken in bucket
@@ -69,8 +77,8 @@ using namespace ovx;
 namespace
 {
 
-constexpr int kInlineFaceBricks = 64; // face boxes over more bricks go to the CTA-per-triangle path
-constexpr int kChunk = 8;             // columns per tile for large (triangle, axis) pairs
+constexpr int kInlineFaceBricks = 8; // triangles whose face box spans more bricks go to large_faces
+constexpr int kUnitCells = 64;        // cells per unit of work of a large (triangle, axis) pair
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
 
@@ -86,6 +94,9 @@ enum
     C_LONG = 6,
     C_HUGE = 7,
     C_ESTAGED = 8,
+    C_LUNITS = 9,  // units of work of the large (triangle, axis) pairs
+    C_FUNITS = 10, // units of work of the large triangles' face boxes
+    C_BLONG = 11,  // boundary edges walked by a whole warp
     C_WORDS = 12
 };
 enum
@@ -206,11 +217,15 @@ struct GenArgs
     uint32_t estage_cap;
     uint32_t *counters;
     uint32_t *scan_large;
+    uint32_t *scan_units; // per listed pair: its units of work, then (scanned) its first unit
     uint32_t scan_large_cap;
     uint32_t *face_large;
+    uint32_t *face_units; // the same for the listed triangles
     uint32_t face_large_cap;
     const unsigned long long *bkeys;
     uint32_t bkeys_cap;
+    uint32_t *blong; // boundary edges with long walks (their index in bkeys)
+    uint32_t blong_cap;
 };
 
 // Add n to rcnt[b] once per group of lanes of the calling warp that target the
@@ -354,12 +369,14 @@ struct EventSink
 };
 
 constexpr int kEventThreads = 128;   // scanline pass: one (triangle, axis) per lane
-constexpr int kWarpScanWork = 4096;  // (triangle, axis) pairs with more row x column work go to large_events
+constexpr int kWarpScanWork = 256;   // (triangle, axis) pairs with more row x column work go to large_rows
 
 struct EventWarp
 {
     double t[3][3][32]; // sorted vertices (projection coordinates) of each lane's (triangle, axis)
-    int start[32], mid[32];
+    long long ta[32];   // each lane's pair: 3 * triangle + axis
+    int start[32], mid[32]; // first row of the lane's rows, and the row where the second edge pair starts
+    int clo[32], chi[32];   // columns of the lane's rows: [clo, chi)
 };
 
 // Largest lane l with v(l) <= x, for v non-decreasing over the lanes (x >= v(0)).
@@ -392,6 +409,116 @@ __device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t x, uint32_t &to
     return incl - x;
 }
 
+// A large (triangle, axis) pair is cut into units of about kUnitCells cells:
+// blocks of rb rows of narrow pairs, column chunks (nch per row) of wide ones.
+struct LargeSplit
+{
+    int rb, nch;
+};
+
+__device__ __forceinline__ LargeSplit large_split(int cols)
+{
+    if (cols >= kUnitCells)
+        return {1, (cols + kUnitCells - 1) / kUnitCells};
+    return {kUnitCells / cols, 1};
+}
+
+// The rows of the warp's (triangle, axis) pairs (lane l: nrows rows from
+// E.start[l]) spread over the lanes 32 at a time, and the column crossings of
+// those rows again 32 at a time, so the FP64 event arithmetic runs on full
+// warps whatever the pairs' sizes.  COUNT marks the occupancy bits, counts
+// event records per brick and stages them; FILL writes the records.
+template <int M>
+__device__ __forceinline__ void event_rows(const GenArgs &A, EventWarp &E, const int lane, const uint32_t nrows)
+{
+    const Grid &g = A.m.g;
+    uint32_t nrow_all;
+    const uint32_t rstart = warp_exclusive_scan(nrows, nrow_all);
+    __syncwarp();
+    for (uint32_t rb = 0; rb < nrow_all; rb += 32)
+    {
+        // this lane's row: owner pair ol, row yi
+        const uint32_t r = rb + (uint32_t)lane;
+        const int ol = owner_lane(rstart, r);
+        const uint32_t ors = __shfl_sync(0xffffffffu, rstart, ol);
+        const int oax2 = (int)(E.ta[ol] % 3);
+        RowSetup rs;
+        rs.t3x = rs.t3z = rs.t4x = rs.t4z = 0.0;
+        rs.x0 = rs.x1 = 0;
+        int yi = 0;
+        if (r < nrow_all)
+        {
+            AxisScan s;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    s.t[k][c] = E.t[k][c][ol];
+            s.start = E.start[ol];
+            s.mid = E.mid[ol];
+            s.end = 0;
+            s.ax2 = oax2;
+            s.ax0 = (oax2 + 1) % 3;
+            s.ax1 = (oax2 + 2) % 3;
+            yi = s.start + (int)(r - ors);
+            row_setup(s, yi, E.clo[ol], E.chi[ol], g, rs);
+        }
+        const uint32_t ncol = rs.x1 > rs.x0 ? (uint32_t)(rs.x1 - rs.x0) : 0u;
+        uint32_t ncol_all;
+        const uint32_t cstart = warp_exclusive_scan(ncol, ncol_all);
+        for (uint32_t cb = 0; cb < ncol_all; cb += 32)
+        {
+            // this lane's column crossing: owner row lane rl
+            const uint32_t c = cb + (uint32_t)lane;
+            const int rl = owner_lane(cstart, c);
+            RowSetup cr;
+            cr.t3x = __shfl_sync(0xffffffffu, rs.t3x, rl);
+            cr.t3z = __shfl_sync(0xffffffffu, rs.t3z, rl);
+            cr.t4x = __shfl_sync(0xffffffffu, rs.t4x, rl);
+            cr.t4z = __shfl_sync(0xffffffffu, rs.t4z, rl);
+            cr.x0 = __shfl_sync(0xffffffffu, rs.x0, rl);
+            cr.x1 = 0;
+            const int cyi = __shfl_sync(0xffffffffu, yi, rl);
+            const int col = __shfl_sync(0xffffffffu, ol, rl);
+            const uint32_t ccs = __shfl_sync(0xffffffffu, cstart, rl);
+            EventStage es;
+            es.n = 0;
+            if (c < ncol_all)
+            {
+                const long long cta = E.ta[col];
+                const int cax2 = (int)(cta % 3);
+                const int xi = cr.x0 + (int)(c - ccs);
+                double z;
+                int zi;
+                col_event(cr, xi, (cax2 + 1) % 3, cax2, g, z, zi);
+                if (zi >= g.gmin[cax2] && zi < g.gmax[cax2])
+                {
+                    EventSink<M> sink{A, (uint32_t)(cta / 3), cax2, (M == COUNT && A.estage) ? &es : nullptr};
+                    sink(xi, cyi, zi, 0.0f, 0.0f, z);
+                }
+            }
+            if (M == COUNT && A.estage)
+            {
+                // stage this round's records: one reservation for the warp
+                uint32_t tot;
+                const uint32_t off = warp_exclusive_scan(es.n, tot);
+                uint32_t base = 0;
+                if (lane == 0 && tot)
+                    base = atomicAdd(&A.counters[C_ESTAGED], tot);
+                base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if ((uint32_t)k < es.n)
+                    {
+                        const unsigned long long pos = (unsigned long long)base + off + k;
+                        if (pos < A.estage_cap)
+                            A.estage[pos] = make_uint4(es.b[k], es.t, es.code[k], es.zb);
+                    }
+            }
+        }
+    }
+}
+
 // Scanline events (flexible_dual_grid.cpp:195-283), one (triangle, axis) per
 // lane.  The rows of the warp's 32 pairs are spread over the lanes 32 at a
 // time, and the column crossings of those rows again 32 at a time, so the FP64
@@ -405,7 +532,6 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
     const int lane = threadIdx.x & 31;
     EventWarp &E = EW[threadIdx.x >> 5];
     const long long ta = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long tabase = ta - lane;
     const Grid &g = A.m.g;
     uint32_t nrows = 0;
     if (ta < 3 * A.m.nf)
@@ -441,7 +567,11 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
                     {
                         const uint32_t slot = atomicAdd(&A.counters[C_SCAN_LARGE], 1u);
                         if (slot < A.scan_large_cap)
+                        {
+                            const LargeSplit sp = large_split(chi - clo + 1);
                             A.scan_large[slot] = (uint32_t)ta;
+                            A.scan_units[slot] = (uint32_t)((rows + sp.rb - 1) / sp.rb * sp.nch);
+                        }
                         else
                             atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
                     }
@@ -455,227 +585,149 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
                             E.t[k][c][lane] = s.t[k][c];
                     E.start[lane] = s.start;
                     E.mid[lane] = s.mid;
+                    E.clo[lane] = INT_MIN;
+                    E.chi[lane] = INT_MAX;
+                    E.ta[lane] = ta;
                     nrows = (uint32_t)rows;
                 }
             }
         }
     }
-    uint32_t nrow_all;
-    const uint32_t rstart = warp_exclusive_scan(nrows, nrow_all);
     __syncwarp();
-    for (uint32_t rb = 0; rb < nrow_all; rb += 32)
+    event_rows<M>(A, E, lane, nrows);
+}
+
+// In-place exclusive scan of the unit counts of a work list (one CTA): entry i
+// of `units` becomes the first unit of list entry i, entry n the total, which
+// also goes to counters[total_word].  n is read from counters[count_word].
+__global__ void __launch_bounds__(1024) unit_offsets(uint32_t *__restrict__ units, uint32_t cap, uint32_t *__restrict__ counters,
+                                                      int count_word, int total_word)
+{
+    __shared__ unsigned long long wsum[32];
+    const uint32_t n = min(counters[count_word], cap);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = min(n, (uint32_t)tid * per), b1 = min(n, b0 + per);
+    unsigned long long sum = 0;
+    for (uint32_t i = b0; i < b1; ++i)
+        sum += units[i];
+    unsigned long long incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
     {
-        // this lane's row: owner pair ol, row yi
-        const uint32_t r = rb + (uint32_t)lane;
-        const int ol = owner_lane(rstart, r);
-        const uint32_t ors = __shfl_sync(0xffffffffu, rstart, ol);
-        const int oax2 = (int)((tabase + ol) % 3);
-        RowSetup rs;
-        rs.t3x = rs.t3z = rs.t4x = rs.t4z = 0.0;
-        rs.x0 = rs.x1 = 0;
-        int yi = 0;
-        if (r < nrow_all)
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d)
+            incl += y;
+    }
+    if (lane == 31)
+        wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0)
+    {
+        const int nw = blockDim.x >> 5;
+        unsigned long long w = lane < nw ? wsum[lane] : 0ull;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
         {
-            AxisScan s;
-#pragma unroll
-            for (int k = 0; k < 3; ++k)
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    s.t[k][c] = E.t[k][c][ol];
-            s.start = E.start[ol];
-            s.mid = E.mid[ol];
-            s.end = 0;
-            s.ax2 = oax2;
-            s.ax0 = (oax2 + 1) % 3;
-            s.ax1 = (oax2 + 2) % 3;
-            yi = s.start + (int)(r - ors);
-            row_setup(s, yi, INT_MIN, INT_MAX, g, rs);
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, w, d);
+            if (lane >= d)
+                w += y;
         }
-        const uint32_t ncol = rs.x1 > rs.x0 ? (uint32_t)(rs.x1 - rs.x0) : 0u;
-        uint32_t ncol_all;
-        const uint32_t cstart = warp_exclusive_scan(ncol, ncol_all);
-        for (uint32_t cb = 0; cb < ncol_all; cb += 32)
+        if (lane < nw)
+            wsum[lane] = w;
+    }
+    __syncthreads();
+    unsigned long long run = (warp > 0 ? wsum[warp - 1] : 0ull) + incl - sum;
+    for (uint32_t i = b0; i < b1; ++i)
+    {
+        const uint32_t u = units[i];
+        units[i] = (uint32_t)run;
+        run += u;
+    }
+    if (tid == (int)blockDim.x - 1)
+    {
+        if (run >= (1ull << 32))
         {
-            // this lane's column crossing: owner row lane rl
-            const uint32_t c = cb + (uint32_t)lane;
-            const int rl = owner_lane(cstart, c);
-            RowSetup cr;
-            cr.t3x = __shfl_sync(0xffffffffu, rs.t3x, rl);
-            cr.t3z = __shfl_sync(0xffffffffu, rs.t3z, rl);
-            cr.t4x = __shfl_sync(0xffffffffu, rs.t4x, rl);
-            cr.t4z = __shfl_sync(0xffffffffu, rs.t4z, rl);
-            cr.x0 = __shfl_sync(0xffffffffu, rs.x0, rl);
-            cr.x1 = 0;
-            const int cyi = __shfl_sync(0xffffffffu, yi, rl);
-            const int col = __shfl_sync(0xffffffffu, ol, rl);
-            const uint32_t ccs = __shfl_sync(0xffffffffu, cstart, rl);
-            EventStage es;
-            es.n = 0;
-            if (c < ncol_all)
+            atomicOr(&counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+            run = 0;
+        }
+        units[n] = (uint32_t)run;
+        counters[total_word] = (uint32_t)run;
+    }
+}
+
+// Entry i of a scanned unit list with units[i] <= u < units[i + 1] (u below units[n]).
+__device__ __forceinline__ uint32_t unit_owner(const uint32_t *__restrict__ units, uint32_t n, uint32_t u)
+{
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1)
+    {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (units[mid] <= u)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Large (triangle, axis) pairs, cut into units of about kUnitCells cells (a
+// block of rows, or a chunk of one row's columns): one unit per lane, 32 per
+// warp, the rows and column crossings of the warp's units spread over the
+// lanes as for the other pairs.
+template <int M, typename IdxT>
+__global__ void __launch_bounds__(kEventThreads) large_rows(GenArgs A)
+{
+    __shared__ EventWarp EW[kEventThreads / 32];
+    const int lane = threadIdx.x & 31;
+    EventWarp &E = EW[threadIdx.x >> 5];
+    const uint32_t n = min(A.counters[C_SCAN_LARGE], A.scan_large_cap);
+    const uint32_t total = A.counters[C_LUNITS];
+    const int wpb = blockDim.x >> 5;
+    const long long stride = (long long)gridDim.x * wpb * 32;
+    for (long long ub = ((long long)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; ub < (long long)total; ub += stride)
+    {
+        const long long u = ub + lane;
+        uint32_t nrows = 0;
+        if (u < (long long)total)
+        {
+            const uint32_t i = unit_owner(A.scan_units, n, (uint32_t)u);
+            const uint32_t ta = A.scan_large[i];
+            const long long t = ta / 3;
+            const int ax2 = (int)(ta - 3 * t);
+            float v[3][3];
+            if (tri_load<IdxT>(A.m, t, v))
             {
-                const long long cta = tabase + col;
-                const int cax2 = (int)(cta % 3);
-                const int xi = cr.x0 + (int)(c - ccs);
-                double z;
-                int zi;
-                col_event(cr, xi, (cax2 + 1) % 3, cax2, g, z, zi);
-                if (zi >= g.gmin[cax2] && zi < g.gmax[cax2])
+                AxisScan s;
+                axis_setup(v, ax2, A.m.g, s);
+                int clo, chi;
+                axis_col_bounds(s, A.m.g, clo, chi);
+                const LargeSplit sp = large_split(chi - clo + 1);
+                const int j = (int)((uint32_t)u - A.scan_units[i]);
+                const int ch = j % sp.nch;
+                const int r0 = s.start + (j / sp.nch) * sp.rb;
+                const int r1 = min(s.end, r0 + sp.rb);
+                if (r1 > r0)
                 {
-                    EventSink<M> sink{A, (uint32_t)(cta / 3), cax2, (M == COUNT && A.estage) ? &es : nullptr};
-                    sink(xi, cyi, zi, 0.0f, 0.0f, z);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            E.t[k][c][lane] = s.t[k][c];
+                    E.start[lane] = r0;
+                    E.mid[lane] = s.mid;
+                    E.clo[lane] = ch == 0 ? INT_MIN : clo + ch * kUnitCells;
+                    E.chi[lane] = ch == sp.nch - 1 ? INT_MAX : clo + (ch + 1) * kUnitCells;
+                    E.ta[lane] = ta;
+                    nrows = (uint32_t)(r1 - r0);
                 }
             }
-            if (M == COUNT && A.estage)
-            {
-                // stage this round's records: one reservation for the warp
-                uint32_t tot;
-                const uint32_t off = warp_exclusive_scan(es.n, tot);
-                uint32_t base = 0;
-                if (lane == 0 && tot)
-                    base = atomicAdd(&A.counters[C_ESTAGED], tot);
-                base = __shfl_sync(0xffffffffu, base, 0);
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if ((uint32_t)k < es.n)
-                    {
-                        const unsigned long long pos = (unsigned long long)base + off + k;
-                        if (pos < A.estage_cap)
-                            A.estage[pos] = make_uint4(es.b[k], es.t, es.code[k], es.zb);
-                    }
-            }
         }
+        __syncwarp();
+        event_rows<M>(A, E, lane, nrows);
+        __syncwarp();
     }
 }
-
-// One CTA per listed (triangle, axis); threads over (row, column chunk) tiles.
-template <int M, typename IdxT>
-__global__ void __launch_bounds__(128) large_events(GenArgs A)
-{
-    const uint32_t n = min(A.counters[C_SCAN_LARGE], A.scan_large_cap);
-    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
-    {
-        const uint32_t e = A.scan_large[i];
-        const long long t = e / 3;
-        const int ax2 = (int)(e % 3);
-        float v[3][3];
-        if (!tri_load<IdxT>(A.m, t, v))
-            continue;
-        AxisScan s;
-        axis_setup(v, ax2, A.m.g, s);
-        const int rows = s.end - s.start;
-        int clo, chi;
-        axis_col_bounds(s, A.m.g, clo, chi);
-        const int nch = (chi - clo + 1 + kChunk - 1) / kChunk;
-        const long long tiles = (long long)rows * nch;
-        EventSink<M> sink{A, (uint32_t)t, ax2};
-        for (long long k = threadIdx.x; k < tiles; k += blockDim.x)
-        {
-            const int yi = s.start + (int)(k / nch);
-            const int ch = (int)(k % nch);
-            const int lo = ch == 0 ? INT_MIN : clo + ch * kChunk;
-            const int hi = ch == nch - 1 ? INT_MAX : clo + (ch + 1) * kChunk;
-            scan_row(s, yi, lo, hi, A.m.g, sink);
-        }
-    }
-}
-
-// Face tests of the active voxels of one brick inside a triangle's face box,
-// evaluated once into a 512-bit pass mask: COUNT adds the number of passing
-// voxels to the brick's record count, FILL reserves that many slots at once and
-// writes the records.
-template <int M>
-__device__ __forceinline__ void face_brick(const GenArgs &A, const FaceSetup &fs, uint32_t t, int bx, int by, int bz)
-{
-    const Grid &g = A.m.g;
-    const long long b = (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
-    const int o[3] = {g.gmin[0] + bx * kBrick, g.gmin[1] + by * kBrick, g.gmin[2] + bz * kBrick};
-    int lo[3], hi[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-    {
-        lo[a] = (fs.bmin[a] > o[a] ? fs.bmin[a] : o[a]) - o[a];
-        hi[a] = (fs.bmax[a] < o[a] + 8 ? fs.bmax[a] : o[a] + 8) - o[a];
-        if (hi[a] <= lo[a])
-            return;
-    }
-    const uint32_t xmask = ((1u << hi[0]) - 1u) & ~((1u << lo[0]) - 1u);
-    const uint4 *bw4 = reinterpret_cast<const uint4 *>(A.bits + b * kWordsPerBrick);
-    uint32_t pm[kWordsPerBrick];
-    uint32_t count = 0;
-#pragma unroll
-    for (int q4 = 0; q4 < 4; ++q4)
-    {
-        const uint4 wv = bw4[q4];
-        const uint32_t words[4] = {wv.x, wv.y, wv.z, wv.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-        {
-            const int w = q4 * 4 + k;
-            pm[w] = 0u;
-            if ((w >> 1) < lo[2] || (w >> 1) >= hi[2])
-                continue;
-            uint32_t mask = 0;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-            {
-                const int ly = (w & 1) * 4 + q;
-                if (ly >= lo[1] && ly < hi[1])
-                    mask |= xmask << (q * 8);
-            }
-            uint32_t word = words[k] & mask;
-            uint32_t pass = 0u;
-            while (word)
-            {
-                const int bt = __ffs(word) - 1;
-                word &= word - 1u;
-                if (face_test(fs, g, o[0] + (bt & 7), o[1] + (w & 1) * 4 + (bt >> 3), o[2] + (w >> 1)))
-                    pass |= 1u << bt;
-            }
-            pm[w] = pass;
-            count += __popc(pass);
-        }
-    }
-    if (count == 0)
-        return;
-    if (M == COUNT)
-    {
-        agg_add(A.rcnt, b, count);
-        return;
-    }
-    const uint32_t k0 = agg_add(A.rcnt, b, count);
-    if ((unsigned long long)k0 + count > A.roff[b + 1] - A.roff[b])
-    {
-        atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
-        return;
-    }
-    unsigned long long pos = A.roff[b] + k0;
-#pragma unroll
-    for (int w = 0; w < kWordsPerBrick; ++w)
-    {
-        uint32_t pass = pm[w];
-        while (pass)
-        {
-            const int bt = __ffs(pass) - 1;
-            pass &= pass - 1u;
-            Rec r;
-            r.a = t;
-            r.b = kRecFace | (uint32_t)(w * 32 + bt);
-            r.c = 0u;
-            A.rec[pos++] = r;
-        }
-    }
-}
-
-__device__ __forceinline__ void face_bricks(const FaceSetup &fs, const Grid &g, int b0[3], int b1[3])
-{
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-    {
-        b0[a] = (fs.bmin[a] - g.gmin[a]) >> 3;
-        b1[a] = (fs.bmax[a] - 1 - g.gmin[a]) >> 3;
-    }
-}
-
 
 // Face box of a triangle restricted to the brick with origin o, as local
 // [lo, hi) per axis; false if empty.
@@ -712,17 +764,19 @@ __device__ __forceinline__ uint32_t box_word(uint32_t word, int w, const int lo[
 
 constexpr int kFaceThreads = 128; // face pass: one triangle per lane
 constexpr int kFaceWindow = 512; // candidates listed per step of a warp
+static_assert(kFaceWindow >= kBrick * kBrick * kBrick, "a dense item's candidates (up to a whole brick) fit the list");
+static_assert(kFaceWindow >= kWordsPerBrick * 4, "the slot list holds a dense item's words");
 
 struct FaceWarp
 {
     float coef[kFaceCoef][32];         // face-test coefficients of each lane's triangle
     int info[11][32];                  // per lane: first brick (3), bricks along x and y, face box min (3), max (3)
     uint32_t pass[kWordsPerBrick][32]; // face-test hits of each item of the current chunk
-    uint32_t cand[kWordsPerBrick][32]; // candidate words of the chunk's dense items
     int org[3][32];                    // brick origin of each item
     uint8_t own[32];                   // lane whose triangle an item belongs to
+    uint32_t tri[32];                  // triangle of each lane
     uint16_t cl[kFaceWindow];          // candidate list: local voxel index
-    uint8_t cs[kFaceWindow];           // candidate list: item slot
+    alignas(16) uint8_t cs[kFaceWindow]; // candidate list: item slot (a dense item's 16 words while dense items run)
 };
 
 struct FaceCoefArr
@@ -743,6 +797,243 @@ struct FaceCoefSmem
     }
 };
 
+// Records of one (triangle, brick) item whose face-test hits are in column
+// `lane` of pass (hits of them): COUNT adds them to the brick's record count
+// and stages them (one reservation per warp; past the staging capacity they
+// are only counted and the fill pass runs instead), FILL writes them into the
+// brick's bucket.  Called by all lanes of the warp.
+template <int M>
+__device__ __forceinline__ void face_hits(const GenArgs &A, const uint32_t (*pass)[32], const int lane, const uint32_t hits,
+                                          const long long b, const uint32_t tri)
+{
+    if (M == COUNT && A.fstage)
+    {
+        uint32_t incl = hits;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d)
+                incl += y;
+        }
+        uint32_t base = 0;
+        if (lane == 31 && incl)
+            base = atomicAdd(&A.counters[C_FSTAGED], incl);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        unsigned long long pos = (unsigned long long)base + incl - hits;
+        for (int w = 0; w < kWordsPerBrick && hits; ++w)
+        {
+            uint32_t pm = pass[w][lane];
+            while (pm)
+            {
+                const int bt = __ffs(pm) - 1;
+                pm &= pm - 1u;
+                if (pos < A.fstage_cap)
+                    A.fstage[pos] = make_uint4((uint32_t)b, tri, kRecFace | (uint32_t)(w * 32 + bt), 0u);
+                ++pos;
+            }
+        }
+    }
+    if (hits)
+    {
+        const uint32_t k0 = agg_add(A.rcnt, b, hits);
+        if (M == FILL)
+        {
+            if ((unsigned long long)k0 + hits > A.roff[b + 1] - A.roff[b])
+                atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
+            else
+            {
+                unsigned long long pos = A.roff[b] + k0;
+                for (int w = 0; w < kWordsPerBrick; ++w)
+                {
+                    uint32_t pm = pass[w][lane];
+                    while (pm)
+                    {
+                        const int bt = __ffs(pm) - 1;
+                        pm &= pm - 1u;
+                        Rec rr;
+                        rr.a = tri;
+                        rr.b = kRecFace | (uint32_t)(w * 32 + bt);
+                        rr.c = 0u;
+                        A.rec[pos++] = rr;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// A lane's triangle in W: face-test coefficients, first brick and bricks along
+// x and y of its face box, the face box itself, the triangle index.
+__device__ __forceinline__ void face_lane_setup(FaceWarp &W, const int lane, const float v[3][3], const Grid &g, const int bmin[3],
+                                                const int bmax[3], const int b0[3], const int nx, const int ny, const uint32_t t)
+{
+    FaceSetup fs;
+    face_setup(v, g, fs);
+    float c[kFaceCoef];
+    face_coefs(fs, c);
+#pragma unroll
+    for (int i = 0; i < kFaceCoef; ++i)
+        W.coef[i][lane] = c[i];
+    const int inf[11] = {b0[0], b0[1], b0[2], nx, ny, bmin[0], bmin[1], bmin[2], bmax[0], bmax[1], bmax[2]};
+#pragma unroll
+    for (int i = 0; i < 11; ++i)
+        W.info[i][lane] = inf[i];
+    W.tri[lane] = t;
+}
+
+// One round of (triangle, brick) items, one per lane: lane l's item is brick
+// rank r of the face box of lane ol's triangle (coefficients, box and
+// triangle in W at column ol).  The candidates (active voxels of the brick
+// inside the face box) are tested on full warps: items with many of them by
+// the whole warp with the coefficients in registers, the others through a
+// shared list; then the hits become records.  Called by all lanes.
+template <int M>
+__device__ __forceinline__ void face_item(const GenArgs &A, FaceWarp &W, const int lane, const bool valid, const int ol, const int r)
+{
+    const Grid &g = A.m.g;
+    uint32_t cw[kWordsPerBrick];
+    uint32_t cnt = 0;
+    long long b = 0;
+    if (valid)
+    {
+        const int nx = W.info[3][ol], ny = W.info[4][ol];
+        const int bx = W.info[0][ol] + r % nx, by = W.info[1][ol] + (r / nx) % ny, bz = W.info[2][ol] + r / (nx * ny);
+        b = (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
+        const int o[3] = {g.gmin[0] + bx * kBrick, g.gmin[1] + by * kBrick, g.gmin[2] + bz * kBrick};
+        const int bmin[3] = {W.info[5][ol], W.info[6][ol], W.info[7][ol]};
+        const int bmax[3] = {W.info[8][ol], W.info[9][ol], W.info[10][ol]};
+        int lo[3], hi[3];
+        const bool any = brick_box(bmin, bmax, o, lo, hi);
+        const uint4 *bw4 = reinterpret_cast<const uint4 *>(A.bits + b * kWordsPerBrick);
+#pragma unroll
+        for (int q4 = 0; q4 < 4; ++q4)
+        {
+            const uint4 wv = any ? bw4[q4] : make_uint4(0u, 0u, 0u, 0u);
+            const uint32_t words[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+            {
+                cw[q4 * 4 + k] = any ? box_word(words[k], q4 * 4 + k, lo, hi) : 0u;
+                cnt += __popc(cw[q4 * 4 + k]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            W.org[a][lane] = o[a];
+        W.own[lane] = (uint8_t)ol;
+    }
+    else
+    {
+#pragma unroll
+        for (int w = 0; w < kWordsPerBrick; ++w)
+            cw[w] = 0u;
+    }
+#pragma unroll
+    for (int w = 0; w < kWordsPerBrick; ++w)
+        W.pass[w][lane] = 0u;
+    // items with many candidates are tested by the whole warp with the
+    // triangle's coefficients in registers; the others go through the list
+    const bool dense = cnt > 32u;
+    const uint32_t dmask = __ballot_sync(0xffffffffu, dense);
+    __syncwarp();
+    for (uint32_t dm = dmask; dm; dm &= dm - 1u)
+    {
+        // one dense item: its candidates are compacted into the shared list,
+        // then tested by all lanes with the triangle's coefficients in registers
+        const int sd = __ffs(dm) - 1;
+        const int so = W.own[sd];
+        float c[kFaceCoef];
+#pragma unroll
+        for (int i = 0; i < kFaceCoef; ++i)
+            c[i] = W.coef[i][so];
+        // this lane's half word of the item's candidates, passed on by the
+        // item's lane through the slot list (unused while dense items run)
+        uint32_t *dwords = reinterpret_cast<uint32_t *>(W.cs);
+        if (lane == sd)
+        {
+#pragma unroll
+            for (int ww = 0; ww < kWordsPerBrick; ++ww)
+                dwords[ww] = cw[ww];
+        }
+        __syncwarp();
+        const int w = lane >> 1;
+        const uint32_t word = dwords[w];
+        uint32_t bits = (lane & 1) ? (word & 0xffff0000u) : (word & 0x0000ffffu);
+        uint32_t ntot;
+        uint32_t pos = warp_exclusive_scan((uint32_t)__popc(bits), ntot);
+        while (bits)
+        {
+            const int bt = __ffs(bits) - 1;
+            bits &= bits - 1u;
+            W.cl[pos++] = (uint16_t)(w * 32 + bt);
+        }
+        __syncwarp();
+        const int ox = W.org[0][sd], oy = W.org[1][sd], oz = W.org[2][sd];
+        for (uint32_t k = lane; k < ntot; k += 32)
+        {
+            const int lv = W.cl[k];
+            if (face_test_c(FaceCoefArr{c}, g, ox + (lv & 7), oy + ((lv >> 3) & 7), oz + (lv >> 6)))
+                atomicOr(&W.pass[lv >> 5][sd], 1u << (lv & 31));
+        }
+        __syncwarp();
+    }
+    const uint32_t lcnt = dense ? 0u : cnt;
+    uint32_t off = lcnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1)
+    {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, off, d);
+        if (lane >= d)
+            off += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
+    off -= lcnt;
+    for (uint32_t wbeg = 0; wbeg < total; wbeg += kFaceWindow)
+    {
+        // list the candidates that fall in [wbeg, wbeg + kFaceWindow)
+        const uint32_t wend = wbeg + kFaceWindow;
+        if (cnt && !dense && off < wend && off + cnt > wbeg)
+        {
+            uint32_t idx = off;
+#pragma unroll 1
+            for (int w = 0; w < kWordsPerBrick && idx < wend; ++w)
+            {
+                uint32_t word = cw[w];
+                while (word && idx < wend)
+                {
+                    const int bt = __ffs(word) - 1;
+                    word &= word - 1u;
+                    if (idx >= wbeg)
+                    {
+                        W.cl[idx - wbeg] = (uint16_t)(w * 32 + bt);
+                        W.cs[idx - wbeg] = (uint8_t)lane;
+                    }
+                    ++idx;
+                }
+            }
+        }
+        __syncwarp();
+        const uint32_t n = total - wbeg < (uint32_t)kFaceWindow ? total - wbeg : (uint32_t)kFaceWindow;
+        for (uint32_t k = lane; k < n; k += 32)
+        {
+            const int lv = W.cl[k], sl = W.cs[k];
+            const int x = W.org[0][sl] + (lv & 7), y = W.org[1][sl] + ((lv >> 3) & 7), z = W.org[2][sl] + (lv >> 6);
+            if (face_test_c(FaceCoefSmem{&W.coef[0][W.own[sl]]}, g, x, y, z))
+                atomicOr(&W.pass[lv >> 5][sl], 1u << (lv & 31));
+        }
+        __syncwarp();
+    }
+    uint32_t hits = 0;
+    if (cnt)
+    {
+#pragma unroll
+        for (int w = 0; w < kWordsPerBrick; ++w)
+            hits += __popc(W.pass[w][lane]);
+    }
+    face_hits<M>(A, W.pass, lane, hits, b, W.tri[ol]);
+}
+
 // Face stage (flexible_dual_grid.cpp:298-414), one triangle per lane.  The
 // warp's (triangle, brick) items are taken 32 at a time; the candidates of
 // those items (active voxels of the brick inside the triangle's face box) are
@@ -756,7 +1047,6 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
     const int lane = threadIdx.x & 31;
     FaceWarp &W = FW[threadIdx.x >> 5];
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long tbase = t - lane;
     const Grid &g = A.m.g;
     int nbk = 0;
     if (t < A.m.nf)
@@ -783,24 +1073,17 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
                     {
                         const uint32_t slot = atomicAdd(&A.counters[C_FACE_LARGE], 1u);
                         if (slot < A.face_large_cap)
+                        {
                             A.face_large[slot] = (uint32_t)t;
+                            A.face_units[slot] = (uint32_t)n;
+                        }
                         else
                             atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
                     }
                 }
                 else
                 {
-                    FaceSetup fs;
-                    face_setup(v, g, fs);
-                    float c[kFaceCoef];
-                    face_coefs(fs, c);
-#pragma unroll
-                    for (int i = 0; i < kFaceCoef; ++i)
-                        W.coef[i][lane] = c[i];
-                    const int inf[11] = {b0[0], b0[1], b0[2], nx, ny, bmin[0], bmin[1], bmin[2], bmax[0], bmax[1], bmax[2]};
-#pragma unroll
-                    for (int i = 0; i < 11; ++i)
-                        W.info[i][lane] = inf[i];
+                    face_lane_setup(W, lane, v, g, bmin, bmax, b0, nx, ny, (uint32_t)t);
                     nbk = (int)n;
                 }
             }
@@ -834,201 +1117,7 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
         }
         const int ol = lo_l;
         const int r = it - __shfl_sync(0xffffffffu, istart, ol);
-        uint32_t cw[kWordsPerBrick];
-        uint32_t cnt = 0;
-        long long b = 0;
-        if (it < nitems)
-        {
-            const int nx = W.info[3][ol], ny = W.info[4][ol];
-            const int bx = W.info[0][ol] + r % nx, by = W.info[1][ol] + (r / nx) % ny, bz = W.info[2][ol] + r / (nx * ny);
-            b = (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
-            const int o[3] = {g.gmin[0] + bx * kBrick, g.gmin[1] + by * kBrick, g.gmin[2] + bz * kBrick};
-            const int bmin[3] = {W.info[5][ol], W.info[6][ol], W.info[7][ol]};
-            const int bmax[3] = {W.info[8][ol], W.info[9][ol], W.info[10][ol]};
-            int lo[3], hi[3];
-            const bool any = brick_box(bmin, bmax, o, lo, hi);
-            const uint4 *bw4 = reinterpret_cast<const uint4 *>(A.bits + b * kWordsPerBrick);
-#pragma unroll
-            for (int q4 = 0; q4 < 4; ++q4)
-            {
-                const uint4 wv = any ? bw4[q4] : make_uint4(0u, 0u, 0u, 0u);
-                const uint32_t words[4] = {wv.x, wv.y, wv.z, wv.w};
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                {
-                    cw[q4 * 4 + k] = any ? box_word(words[k], q4 * 4 + k, lo, hi) : 0u;
-                    cnt += __popc(cw[q4 * 4 + k]);
-                }
-            }
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-                W.org[a][lane] = o[a];
-            W.own[lane] = (uint8_t)ol;
-        }
-        else
-        {
-#pragma unroll
-            for (int w = 0; w < kWordsPerBrick; ++w)
-                cw[w] = 0u;
-        }
-#pragma unroll
-        for (int w = 0; w < kWordsPerBrick; ++w)
-            W.pass[w][lane] = 0u;
-        // items with many candidates are tested by the whole warp with the
-        // triangle's coefficients in registers; the others go through the list
-        const bool dense = cnt > 32u;
-        const uint32_t dmask = __ballot_sync(0xffffffffu, dense);
-        if (dense)
-        {
-#pragma unroll
-            for (int w = 0; w < kWordsPerBrick; ++w)
-                W.cand[w][lane] = cw[w];
-        }
-        __syncwarp();
-        for (uint32_t dm = dmask; dm; dm &= dm - 1u)
-        {
-            // one dense item: its candidates are compacted into the shared list,
-            // then tested by all lanes with the triangle's coefficients in registers
-            const int sd = __ffs(dm) - 1;
-            const int so = W.own[sd];
-            float c[kFaceCoef];
-#pragma unroll
-            for (int i = 0; i < kFaceCoef; ++i)
-                c[i] = W.coef[i][so];
-            const int w = lane >> 1;
-            const uint32_t word = W.cand[w][sd];
-            uint32_t bits = (lane & 1) ? (word & 0xffff0000u) : (word & 0x0000ffffu);
-            uint32_t ntot;
-            uint32_t pos = warp_exclusive_scan((uint32_t)__popc(bits), ntot);
-            while (bits)
-            {
-                const int bt = __ffs(bits) - 1;
-                bits &= bits - 1u;
-                W.cl[pos++] = (uint16_t)(w * 32 + bt);
-            }
-            __syncwarp();
-            const int ox = W.org[0][sd], oy = W.org[1][sd], oz = W.org[2][sd];
-            for (uint32_t k = lane; k < ntot; k += 32)
-            {
-                const int lv = W.cl[k];
-                if (face_test_c(FaceCoefArr{c}, g, ox + (lv & 7), oy + ((lv >> 3) & 7), oz + (lv >> 6)))
-                    atomicOr(&W.pass[lv >> 5][sd], 1u << (lv & 31));
-            }
-            __syncwarp();
-        }
-        const uint32_t lcnt = dense ? 0u : cnt;
-        uint32_t off = lcnt;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1)
-        {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, off, d);
-            if (lane >= d)
-                off += y;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
-        off -= lcnt;
-        for (uint32_t wbeg = 0; wbeg < total; wbeg += kFaceWindow)
-        {
-            // list the candidates that fall in [wbeg, wbeg + kFaceWindow)
-            const uint32_t wend = wbeg + kFaceWindow;
-            if (cnt && !dense && off < wend && off + cnt > wbeg)
-            {
-                uint32_t idx = off;
-#pragma unroll 1
-                for (int w = 0; w < kWordsPerBrick && idx < wend; ++w)
-                {
-                    uint32_t word = cw[w];
-                    while (word && idx < wend)
-                    {
-                        const int bt = __ffs(word) - 1;
-                        word &= word - 1u;
-                        if (idx >= wbeg)
-                        {
-                            W.cl[idx - wbeg] = (uint16_t)(w * 32 + bt);
-                            W.cs[idx - wbeg] = (uint8_t)lane;
-                        }
-                        ++idx;
-                    }
-                }
-            }
-            __syncwarp();
-            const uint32_t n = total - wbeg < (uint32_t)kFaceWindow ? total - wbeg : (uint32_t)kFaceWindow;
-            for (uint32_t k = lane; k < n; k += 32)
-            {
-                const int lv = W.cl[k], sl = W.cs[k];
-                const int x = W.org[0][sl] + (lv & 7), y = W.org[1][sl] + ((lv >> 3) & 7), z = W.org[2][sl] + (lv >> 6);
-                if (face_test_c(FaceCoefSmem{&W.coef[0][W.own[sl]]}, g, x, y, z))
-                    atomicOr(&W.pass[lv >> 5][sl], 1u << (lv & 31));
-            }
-            __syncwarp();
-        }
-        uint32_t hits = 0;
-        if (cnt)
-        {
-#pragma unroll
-            for (int w = 0; w < kWordsPerBrick; ++w)
-                hits += __popc(W.pass[w][lane]);
-        }
-        if (M == COUNT && A.fstage)
-        {
-            // stage the records now (one reservation per warp) so that the
-            // fill pass need not repeat the tests; past the capacity they are
-            // only counted and the fill pass runs instead
-            uint32_t incl = hits;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1)
-            {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= d)
-                    incl += y;
-            }
-            uint32_t base = 0;
-            if (lane == 31 && incl)
-                base = atomicAdd(&A.counters[C_FSTAGED], incl);
-            base = __shfl_sync(0xffffffffu, base, 31);
-            unsigned long long pos = (unsigned long long)base + incl - hits;
-            const uint32_t tri = (uint32_t)(tbase + ol);
-            for (int w = 0; w < kWordsPerBrick && hits; ++w)
-            {
-                uint32_t pm = W.pass[w][lane];
-                while (pm)
-                {
-                    const int bt = __ffs(pm) - 1;
-                    pm &= pm - 1u;
-                    if (pos < A.fstage_cap)
-                        A.fstage[pos] = make_uint4((uint32_t)b, tri, kRecFace | (uint32_t)(w * 32 + bt), 0u);
-                    ++pos;
-                }
-            }
-        }
-        if (hits)
-        {
-            const uint32_t k0 = agg_add(A.rcnt, b, hits);
-            if (M == FILL)
-            {
-                if ((unsigned long long)k0 + hits > A.roff[b + 1] - A.roff[b])
-                    atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
-                else
-                {
-                    unsigned long long pos = A.roff[b] + k0;
-                    const uint32_t tri = (uint32_t)(tbase + ol);
-                    for (int w = 0; w < kWordsPerBrick; ++w)
-                    {
-                        uint32_t pm = W.pass[w][lane];
-                        while (pm)
-                        {
-                            const int bt = __ffs(pm) - 1;
-                            pm &= pm - 1u;
-                            Rec rr;
-                            rr.a = tri;
-                            rr.b = kRecFace | (uint32_t)(w * 32 + bt);
-                            rr.c = 0u;
-                            A.rec[pos++] = rr;
-                        }
-                    }
-                }
-            }
-        }
+        face_item<M>(A, W, lane, it < nitems, ol, r);
         __syncwarp();
     }
 }
@@ -1057,28 +1146,59 @@ __global__ void __launch_bounds__(kThreads) bucket_records(const uint4 *__restri
     rec[base + k] = o;
 }
 
-// One CTA per listed triangle; threads over the bricks of its face box.
+// Triangles whose face box spans more than kInlineFaceBricks bricks: their
+// (triangle, brick) items, all listed triangles' items one after another, 32
+// per warp and round, one per lane; each lane sets up its own item's triangle
+// and the round runs as in face_records.
 template <int M, typename IdxT>
-__global__ void __launch_bounds__(128) large_face_records(GenArgs A)
+__global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
 {
+    __shared__ FaceWarp FW[kFaceThreads / 32];
+    const int lane = threadIdx.x & 31;
+    FaceWarp &W = FW[threadIdx.x >> 5];
+    const Grid &g = A.m.g;
     const uint32_t n = min(A.counters[C_FACE_LARGE], A.face_large_cap);
-    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
+    const uint32_t total = A.counters[C_FUNITS];
+    const int wpb = blockDim.x >> 5;
+    const long long stride = (long long)gridDim.x * wpb * 32;
+    for (long long ub = ((long long)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; ub < (long long)total; ub += stride)
     {
-        const long long t = A.face_large[i];
-        float v[3][3];
-        if (!tri_load<IdxT>(A.m, t, v))
-            continue;
-        FaceSetup fs;
-        face_setup(v, A.m.g, fs);
-        int b0[3], b1[3];
-        face_bricks(fs, A.m.g, b0, b1);
-        const long long nx = b1[0] - b0[0] + 1, ny = b1[1] - b0[1] + 1, nz = b1[2] - b0[2] + 1;
-        for (long long k = threadIdx.x; k < nx * ny * nz; k += blockDim.x)
-            face_brick<M>(A, fs, (uint32_t)t, b0[0] + (int)(k % nx), b0[1] + (int)((k / nx) % ny), b0[2] + (int)(k / (nx * ny)));
+        const long long u = ub + lane;
+        bool valid = false;
+        int r = 0;
+        if (u < (long long)total)
+        {
+            const uint32_t i = unit_owner(A.face_units, n, (uint32_t)u);
+            const uint32_t t = A.face_large[i];
+            r = (int)((uint32_t)u - A.face_units[i]);
+            float v[3][3];
+            if (tri_load<IdxT>(A.m, t, v))
+            {
+                int bmin[3], bmax[3];
+                face_box(v, g, bmin, bmax);
+                int b0[3], b1[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                {
+                    b0[a] = (bmin[a] - g.gmin[a]) >> 3;
+                    b1[a] = (bmax[a] - 1 - g.gmin[a]) >> 3;
+                }
+                face_lane_setup(W, lane, v, g, bmin, bmax, b0, b1[0] - b0[0] + 1, b1[1] - b0[1] + 1, t);
+                valid = true;
+            }
+        }
+        __syncwarp();
+        face_item<M>(A, W, lane, valid, lane, r);
+        __syncwarp();
     }
 }
 
-// One thread per boundary edge: the reference DDA walk; one record per active voxel visited.
+constexpr int kLongWalk = 64; // boundary edges with a longer step bound are walked by a whole warp
+
+// One thread per boundary edge: the reference DDA walk; one record per active
+// voxel visited.  Edges whose walk may take more than kLongWalk steps are
+// listed (COUNT) and left to boundary_long; FILL writes every edge's line
+// quadric here.
 template <int M>
 __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
 {
@@ -1094,6 +1214,18 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
         Dda d;
         if (!boundary_setup(v0, v1, g, d, M == FILL ? A.btab + (size_t)i * 10 : nullptr))
             continue;
+        if (d.guard > kLongWalk)
+        {
+            if (M == COUNT)
+            {
+                const uint32_t slot = atomicAdd(&A.counters[C_BLONG], 1u);
+                if (slot < A.blong_cap)
+                    A.blong[slot] = i;
+                else
+                    atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+            }
+            continue;
+        }
         for (;;)
         {
             if (in_grid(g, d.cur[0], d.cur[1], d.cur[2]))
@@ -1107,6 +1239,56 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
                 break;
         }
         if (d.guard < 0)
+            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_WALK_GUARD);
+    }
+}
+
+// The listed long boundary edges, one warp each.  Every lane runs the same
+// DDA walk (the steps are cheap arithmetic); lane k visits steps k, k + 32,
+// ..., so the occupancy lookups and records of 32 steps go out together.
+template <int M>
+__global__ void __launch_bounds__(kThreads) boundary_long(GenArgs A)
+{
+    const uint32_t n = min(A.counters[C_BLONG], A.blong_cap);
+    const Grid &g = A.m.g;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < n; j += gridDim.x * wpb)
+    {
+        const uint32_t i = A.blong[j];
+        const unsigned long long e = A.bkeys[i];
+        const uint32_t ia = (uint32_t)(e >> 32), ib = (uint32_t)(e & 0xffffffffull);
+        float v0[3], v1[3];
+        vertex_load(A.m, ia, v0);
+        vertex_load(A.m, ib, v1);
+        Dda d;
+        if (!boundary_setup(v0, v1, g, d, nullptr))
+            continue; // the same edge for the whole warp
+        bool alive = true;
+        while (alive)
+        {
+            int c[3] = {0, 0, 0};
+            bool mine = false;
+            for (int k = 0; k < 32 && alive; ++k)
+            {
+                if (k == lane)
+                {
+                    c[0] = d.cur[0];
+                    c[1] = d.cur[1];
+                    c[2] = d.cur[2];
+                    mine = true;
+                }
+                alive = dda_step(d);
+            }
+            if (mine && in_grid(g, c[0], c[1], c[2]))
+            {
+                uint32_t bit;
+                const long long w = voxel_word(g, c[0], c[1], c[2], bit);
+                if (A.bits[w] & (1u << bit))
+                    put_record<M>(A, w >> 4, i, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), 0u);
+            }
+        }
+        if (M == COUNT && lane == 0 && d.guard < 0)
             atomicOr(&A.counters[C_STATUS], (uint32_t)ST_WALK_GUARD);
     }
 }
@@ -1715,7 +1897,9 @@ constexpr int kWarpSortMax = 32 * kWarpSortPer;      // longer lists go to voxel
 constexpr int kLongMidMax = 1024;                    // ... one CTA of 128 threads, shared-memory sort
 constexpr int kLongHugeMax = 8192;                   // ... one CTA of 256 threads; longer: in-place insertion sort
 
-__global__ void __launch_bounds__(128) voxel_accumulate(SolveArgs A, long long nrows)
+// 12 resident CTAs per SM (at most 40 registers): the sums wait on gathers,
+// and the extra warps hide more of that than the few spills cost
+__global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long long nrows)
 {
     const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -2233,8 +2417,8 @@ struct ovx_fdg_context
 {
     int device = 0;
     int sms = 148;
-    Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, face_large, qtab;
-    Buf vcnt, voff, emax, bkeys, boff, btab;
+    Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, scan_units, face_large, face_units, qtab;
+    Buf vcnt, voff, emax, bkeys, blong, boff, btab;
     Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, estage, longv;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     unsigned long long *host = nullptr; // pinned readback words
@@ -2272,8 +2456,8 @@ namespace
 template <typename Ctx>
 int buffer_list(Ctx *c, Buf **out)
 {
-    Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large,
-                &c->face_large, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
+    Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large, &c->scan_units,
+                &c->face_large, &c->face_units, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->blong, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
                 &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv,
                 &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
@@ -2500,11 +2684,16 @@ GenArgs make_gen(ovx_fdg_context *ctx)
     A.estage_cap = cap_u32(ctx->estage, sizeof(uint4));
     A.counters = (uint32_t *)ctx->counters.p;
     A.scan_large = (uint32_t *)ctx->scan_large.p;
-    A.scan_large_cap = cap_u32(ctx->scan_large, 4);
+    A.scan_units = (uint32_t *)ctx->scan_units.p;
+    // a list holds as many entries as its unit list holds beyond the total
+    A.scan_large_cap = std::min(cap_u32(ctx->scan_large, 4), cap_u32(ctx->scan_units, 4) - 1u);
     A.face_large = (uint32_t *)ctx->face_large.p;
-    A.face_large_cap = cap_u32(ctx->face_large, 4);
+    A.face_units = (uint32_t *)ctx->face_units.p;
+    A.face_large_cap = std::min(cap_u32(ctx->face_large, 4), cap_u32(ctx->face_units, 4) - 1u);
     A.bkeys = (const unsigned long long *)ctx->bkeys.p;
     A.bkeys_cap = cap_u32(ctx->bkeys, 8);
+    A.blong = (uint32_t *)ctx->blong.p;
+    A.blong_cap = cap_u32(ctx->blong, 4);
     return A;
 }
 
@@ -2513,7 +2702,7 @@ void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
 {
     if (M == FILL && ctx->event_staged)
     {
-        // the count pass staged the records of every pair but the listed large ones
+        // the count pass staged the records of every pair
         if (ctx->n_estaged > 0)
         {
             bucket_records<<<blocks_for((long long)ctx->n_estaged, kThreads), kThreads, 0, st>>>(
@@ -2525,9 +2714,14 @@ void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
     {
         tri_events<M, IdxT><<<blocks_for(3 * ctx->nf, kEventThreads), kEventThreads, 0, st>>>(A);
         ++ctx->launches;
+        if (M == COUNT)
+        {
+            unit_offsets<<<1, 1024, 0, st>>>(A.scan_units, A.scan_large_cap, A.counters, C_SCAN_LARGE, C_LUNITS);
+            ++ctx->launches;
+        }
+        large_rows<M, IdxT><<<ctx->sms * 8, kEventThreads, 0, st>>>(A);
+        ++ctx->launches;
     }
-    large_events<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
-    ++ctx->launches;
 }
 
 template <int M, typename IdxT>
@@ -2549,13 +2743,22 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
             face_records<M, IdxT><<<blocks_for(ctx->nf, kFaceThreads), kFaceThreads, 0, st>>>(A);
             ++ctx->launches;
         }
-        large_face_records<M, IdxT><<<ctx->sms * 4, 128, 0, st>>>(A);
-        ++ctx->launches;
+        if (!(M == FILL && ctx->face_staged))
+        {
+            if (M == COUNT)
+            {
+                unit_offsets<<<1, 1024, 0, st>>>(A.face_units, A.face_large_cap, A.counters, C_FACE_LARGE, C_FUNITS);
+                ++ctx->launches;
+            }
+            large_faces<M, IdxT><<<ctx->sms * 7, kFaceThreads, 0, st>>>(A);
+            ++ctx->launches;
+        }
     }
     if (ctx->bw > 0.0f && ctx->nf > 0)
     {
         boundary_records<M><<<ctx->sms * 8, kThreads, 0, st>>>(A);
-        ++ctx->launches;
+        boundary_long<M><<<ctx->sms * 4, kThreads, 0, st>>>(A);
+        ctx->launches += 2;
     }
 }
 
@@ -2574,7 +2777,9 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(ensure(st, ctx, ctx->active, (size_t)(nb + 1) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->counters, C_WORDS * 4));
     OVX_CUDA(ensure(st, ctx, ctx->scan_large, (size_t)(3 * nf + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->scan_units, (size_t)(3 * nf + 2) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->face_large, (size_t)(nf + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->face_units, (size_t)(nf + 2) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->rcnt, (size_t)(nb + 1) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
@@ -2599,6 +2804,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         OVX_CUDA(ensure(st, ctx, ctx->voff, (size_t)(ctx->nv + 1) * 8));
         OVX_CUDA(ensure(st, ctx, ctx->emax, (size_t)(3 * nf + 1) * 4));
         OVX_CUDA(ensure(st, ctx, ctx->bkeys, (size_t)(3 * nf + 1) * 8));
+        OVX_CUDA(ensure(st, ctx, ctx->blong, (size_t)(3 * nf + 1) * 4));
         OVX_CUDA(ensure(st, ctx, ctx->boff, (size_t)(ctx->nv + 1) * 8));
     }
     OVX_CUDA(cudaMemsetAsync(ctx->bits.p, 0, (size_t)nb * kWordsPerBrick * 4, st));

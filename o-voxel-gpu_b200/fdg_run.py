@@ -4,7 +4,8 @@
     python o-voxel-gpu_b200/fdg_run.py --workload subdivided --grid 1024 --stages
 
 Workloads: ico_cap (5120 faces, grid 64), primitives (282k faces, grid 512),
-subdivided (10.3M faces, grid 512 or 1024), sheets (precision stress, grid 1024).
+subdivided (10.3M faces, grid 512 or 1024), sheets (precision stress, grid 1024),
+lowpoly (about 1200 large faces, grid 512 or 1024).
 Every conversion goes through ovx_fdg_begin/ovx_fdg_finish on the current
 stream; with --stages the last conversion is repeated with the library's stage
 timers on.  Prints one JSON line.  This is the command the kernel launch lists
@@ -31,6 +32,8 @@ def make_workload(name: str, grid: int = 0):
         return W.subdivided(1, grid_size=grid or 512)
     if name == "sheets":
         return W.sheets(3)
+    if name == "lowpoly":
+        return W.lowpoly(5, grid_size=grid or 512)
     raise SystemExit(f"unknown workload {name}")
 
 

@@ -314,6 +314,20 @@ def sheets(seed: int = 3, n_sheets: int = 2000, n_creases: int = 1000, grid_size
                     meta={"config": f"{n_sheets} near-coplanar sheets (0.3 voxel spacing), {n_creases} creases, 20% slivers, grid {grid_size}"})
 
 
+def lowpoly(seed: int = 5, faces_total: int = 1_200, grid_size: int = 512) -> Workload:
+    """A low-poly soup of primitives on a fine grid: about a thousand triangles,
+    most spanning thousands of cells per projection and hundreds of bricks,
+    so the large-triangle paths do nearly all the work."""
+    rng = np.random.default_rng(seed)
+    v, f = _primitive_soup(rng, 16, faces_total)
+    v, f = add_slivers(rng, v, f, 0.01)
+    lo, hi = v.min(0), v.max(0)
+    pad = (hi - lo) / (grid_size - 1) * 0.5
+    aabb = [list(map(float, lo - pad)), list(map(float, hi + pad))]
+    return Workload("lowpoly", v.astype(np.float32), f.astype(np.int64), grid_size, aabb,
+                    meta={"config": f"16 primitives, {f.shape[0]} faces, grid {grid_size}, per-mesh aabb"})
+
+
 def batch(seed: int = 4, n_meshes: int = 256, f_lo: int = 1_000, f_hi: int = 500_000,
           grids=(64, 128, 256, 512)) -> List[Workload]:
     rng = np.random.default_rng(seed)

@@ -1,5 +1,6 @@
-"""GPU parity at full size: the 10.3M-face subdivided mesh at grid 512 and 1024
-and the grid-1024 precision-stress sheets, bit for bit against the CPU oracle.
+"""GPU parity at full size: the 10.3M-face subdivided mesh at grid 512 and 1024,
+a low-poly mesh of large triangles at grid 512 and 1024, and the grid-1024
+precision-stress sheets, bit for bit against the CPU oracle.
 
 The sheets case also states the dual-vertex error of the FP32 path (GPU and
 CPU alike) against the FP64 restatement of the same algorithm, in voxel edges.
@@ -43,6 +44,15 @@ def test_subdivided_10m_faces(cuda, grid):
     w = W.subdivided(1, grid_size=grid)
     assert w.num_faces == 10_299_999
     assert_fdg_equal(_gpu_abi(w, cuda), _oracle(w), f"subdivided grid {grid}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("grid", [512, 1024])
+def test_lowpoly_large_triangles(cuda, grid):
+    """About 1200 triangles on a fine grid: nearly every (triangle, axis) pair
+    and face box goes through the large-triangle paths, cut into units."""
+    w = W.lowpoly(5, grid_size=grid)
+    assert_fdg_equal(_gpu_abi(w, cuda), _oracle(w), f"lowpoly grid {grid}")
 
 
 @pytest.mark.gpu
