@@ -22,7 +22,7 @@
 //   qtab    plane quadric per triangle (10 floats)
 //   contrib per-voxel contribution lists, 16 B entries; brick b owns entries
 //           [4*roff[b], 4*roff[b+1]) (a record yields at most 4 contributions)
-//   vlist   per output row: first entry (40 bits) | entry count << 40
+//   vlist   per output row: first entry (40 bits) | entry count << 40 | sorted << 63
 //   btab    line quadric per boundary edge (10 floats)
 //
 // begin (ends with the one host synchronisation of a conversion):
@@ -81,6 +81,14 @@ constexpr int kInlineFaceBricks = 8; // triangles whose face box spans more bric
 constexpr int kUnitCells = 64;        // cells per unit of work of a large (triangle, axis) pair
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
+constexpr int kListStage = 512; // contributions of a brick that brick_lists stages (and sorts) in shared memory
+// vlist word: first entry (bits 0-39) | count (bits 40-62) | sorted flag (bit 63)
+constexpr uint32_t kListCountMax = (1u << 23) - 1u;
+constexpr unsigned long long kListSorted = 1ull << 63;
+#ifndef OVX_FDG_WARP_SORT_MIN
+#define OVX_FDG_WARP_SORT_MIN 16
+#endif
+constexpr int kWarpSortMin = OVX_FDG_WARP_SORT_MIN; // lists this long or longer are ordered by the whole warp
 
 // device counter words
 enum
@@ -1496,7 +1504,7 @@ struct SolveArgs
     uint32_t *longv;            // rows whose lists are too long for voxel_accumulate: up to kLongMidMax
                                 // entries from the front (counter C_LONG), longer ones from the back (C_HUGE)
     uint32_t longv_cap;
-    unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40
+    unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40 | sorted << 63
     float *clist; // deferred constrained searches, 16 words each
     uint32_t clist_cap;
 };
@@ -1701,6 +1709,12 @@ __device__ __forceinline__ void contrib_apply(const Contrib &c, Acc &a)
 // contributions); then one thread per voxel orders its list by key, sums it in
 // that order (the reference CPU order) and solves.
 // ---------------------------------------------------------------------------
+// Order key of a contribution list entry {key lo, key hi, payload, 0}.
+__device__ __forceinline__ unsigned long long entry_key(const uint4 &e)
+{
+    return (unsigned long long)e.x | ((unsigned long long)e.y << 32);
+}
+
 struct ListShared
 {
     uint32_t obits[kWordsPerBrick]; // occupancy words (bit = local index)
@@ -1709,9 +1723,10 @@ struct ListShared
     int zorder;
     uint32_t cnt[512];
     uint32_t off[512];
-    uint32_t scan_tmp[kConsumeThreads / 32 + 1];
+    uint32_t scan_tmp[kConsumeThreads / 32 + 1]; // per-warp offsets, then the brick's total
     int nvox;
     uint32_t status;
+    uint4 ent[kListStage]; // the brick's lists, when they fit: filled, short lists sorted, copied out
 };
 
 struct ListCount
@@ -1810,8 +1825,10 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
                 S.scan_tmp[k] = r;
                 r += x;
             }
+            S.scan_tmp[kConsumeThreads / 32] = r;
         }
         __syncthreads();
+        const bool staged = S.scan_tmp[kConsumeThreads / 32] <= (uint32_t)kListStage;
         uint32_t run = S.scan_tmp[warp] + incl - sum;
         const unsigned long long first = 4ull * A.roff[b];
 #pragma unroll
@@ -1820,17 +1837,54 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
             const int j = tid * per + k;
             if (j < nvox)
             {
-                if (v[k] == 0u || v[k] >= (1u << 24))
+                if (v[k] == 0u || v[k] > kListCountMax)
                     atomicOr(&S.status, (uint32_t)ST_REPLAY); // every active voxel has a scanline contribution
-                A.vlist[vbase + j] = (first + run) | ((unsigned long long)v[k] << 40);
+                const bool sorted = staged && v[k] < (uint32_t)kWarpSortMin;
+                A.vlist[vbase + j] = (first + run) | ((unsigned long long)v[k] << 40) | (sorted ? kListSorted : 0ull);
             }
             S.off[j] = run;
             run += v[k];
         }
     }
     __syncthreads();
+    const uint32_t total = S.scan_tmp[kConsumeThreads / 32];
+    uint4 *out = A.contrib + 4ull * A.roff[b];
+    if (total <= (uint32_t)kListStage)
     {
-        ListFill fs{S, A.contrib + 4ull * A.roff[b], 4ull * nrec};
+        // the lists fit in shared memory: fill them there, sort the short ones
+        // (one thread per voxel), copy the brick's lists out in one sweep
+        {
+            ListFill fs{S, S.ent, (unsigned long long)kListStage};
+            for (unsigned long long r = tid; r < nrec; r += blockDim.x)
+                expand(S, rec[r], fs);
+        }
+        __syncthreads();
+        for (int j = tid; j < nvox; j += blockDim.x)
+        {
+            const uint32_t c = S.cnt[j];
+            if (c < 2u || c >= (uint32_t)kWarpSortMin)
+                continue;
+            uint4 *L = S.ent + (S.off[j] - c);
+            for (uint32_t x = 1; x < c; ++x)
+            {
+                const uint4 e = L[x];
+                const unsigned long long k = entry_key(e);
+                uint32_t y = x;
+                while (y > 0 && entry_key(L[y - 1]) > k)
+                {
+                    L[y] = L[y - 1];
+                    --y;
+                }
+                L[y] = e;
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < total; i += blockDim.x)
+            out[i] = S.ent[i];
+    }
+    else
+    {
+        ListFill fs{S, out, 4ull * nrec};
         for (unsigned long long r = tid; r < nrec; r += blockDim.x)
             expand(S, rec[r], fs);
     }
@@ -1842,10 +1896,6 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
 // One thread per voxel row: order the voxel's contributions by key, sum them in
 // that order, regularise and solve (flexible_dual_grid.cpp:763-797); voxels
 // whose unconstrained solution leaves the box go to the constrained-search list.
-__device__ __forceinline__ unsigned long long entry_key(const uint4 &e)
-{
-    return (unsigned long long)e.x | ((unsigned long long)e.y << 32);
-}
 
 __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src)
 {
@@ -1888,10 +1938,6 @@ __device__ __forceinline__ void voxel_finish(const SolveArgs &A, long long row, 
         c[4 + i] = q[i];
 }
 
-#ifndef OVX_FDG_WARP_SORT_MIN
-#define OVX_FDG_WARP_SORT_MIN 16
-#endif
-constexpr int kWarpSortMin = OVX_FDG_WARP_SORT_MIN; // lists this long or longer are ordered by the whole warp
 constexpr int kWarpSortPer = 2;                      // ... up to 2 entries per lane
 constexpr int kWarpSortMax = 32 * kWarpSortPer;      // longer lists go to voxel_accumulate_long
 constexpr int kLongMidMax = 1024;                    // ... one CTA of 128 threads, shared-memory sort
@@ -1906,7 +1952,8 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
     const bool valid = row < nrows;
     const unsigned long long d = valid ? A.vlist[row] : 0ull;
     const unsigned long long first = d & ((1ull << 40) - 1ull);
-    const uint32_t n = (uint32_t)(d >> 40);
+    const uint32_t n = (uint32_t)(d >> 40) & kListCountMax;
+    const bool sorted = (d & kListSorted) != 0ull;
     // The warp orders the longer lists of its 32 voxels one after another: each
     // lane holds up to kWarpSortPer entries of the list and finds their ranks
     // among the list's (unique) keys, then stores the entries at those ranks.
@@ -1970,10 +2017,10 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
     }
     const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
     uint4 *lst = A.contrib + first;
-    if (n < (uint32_t)kWarpSortMin)
+    if (n < (uint32_t)kWarpSortMin && !sorted)
     {
-        // short lists (nearly sorted already: brick_lists fills them in bucket
-        // order): insertion sort in place
+        // short lists that brick_lists could not sort in shared memory:
+        // insertion sort in place
         for (uint32_t x = 1; x < n; ++x)
         {
             const uint4 e = lst[x];
@@ -2030,7 +2077,7 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
         const long long row = A.longv[kHuge ? A.longv_cap - 1u - li : li];
         const unsigned long long d = A.vlist[row];
         const unsigned long long first = d & ((1ull << 40) - 1ull);
-        const uint32_t n = (uint32_t)(d >> 40);
+        const uint32_t n = (uint32_t)(d >> 40) & kListCountMax;
         const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
         uint4 *lst = A.contrib + first;
         Acc a;
