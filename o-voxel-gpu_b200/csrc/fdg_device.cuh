@@ -415,28 +415,27 @@ __device__ __forceinline__ void face_coefs(const FaceSetup &fs, float c[kFaceCoe
 }
 
 // Box-triangle test at the voxel's min corner (flexible_dual_grid.cpp:324-409):
-// plane slab, then the 9 projected edge half-planes.  `C(i)` returns face-test
-// coefficient i (see kFaceCoef), so registers and shared memory share one code path.
+// plane slab and the 9 projected edge half-planes.  All ten are evaluated and
+// combined (the reference stops at the first failing one; the result is the
+// same), so the lanes of a warp do not diverge on where they stop.  `C(i)`
+// returns face-test coefficient i (see kFaceCoef), so registers and shared
+// memory share one code path.
 template <typename Coef>
 __device__ __forceinline__ bool face_test_c(const Coef &C, const Grid &g, int x, int y, int z)
 {
     const float p0 = g.vs[0] * (float)x, p1 = g.vs[1] * (float)y, p2 = g.vs[2] * (float)z;
     const float nd = dot3f(C(0), C(1), C(2), p0, p1, p2);
-    if ((nd + C(3)) * (nd + C(4)) > 0.0f)
-        return false;
+    bool ok = !((nd + C(3)) * (nd + C(4)) > 0.0f);
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-        if (dot2f(C(5 + 2 * k), C(6 + 2 * k), p0, p1) + C(11 + k) < 0.0f)
-            return false;
+        ok &= !(dot2f(C(5 + 2 * k), C(6 + 2 * k), p0, p1) + C(11 + k) < 0.0f);
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-        if (dot2f(C(14 + 2 * k), C(15 + 2 * k), p1, p2) + C(20 + k) < 0.0f)
-            return false;
+        ok &= !(dot2f(C(14 + 2 * k), C(15 + 2 * k), p1, p2) + C(20 + k) < 0.0f);
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-        if (dot2f(C(23 + 2 * k), C(24 + 2 * k), p2, p0) + C(29 + k) < 0.0f)
-            return false;
-    return true;
+        ok &= !(dot2f(C(23 + 2 * k), C(24 + 2 * k), p2, p0) + C(29 + k) < 0.0f);
+    return ok;
 }
 
 struct FaceCoefRegs
