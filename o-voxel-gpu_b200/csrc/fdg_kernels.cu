@@ -2468,7 +2468,8 @@ struct ovx_fdg_context
     Buf vcnt, voff, emax, bkeys, blong, boff, btab;
     Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, estage, longv;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
-    unsigned long long *host = nullptr; // pinned readback words
+    unsigned long long *host = nullptr;     // readback words: pinned, mapped host memory
+    unsigned long long *host_dev = nullptr; // the same words as the device addresses them
     cudaMemPool_t pool = nullptr;       // workspace pool (keeps its memory until the context is destroyed)
     std::string err;
     // state between begin and finish
@@ -2696,6 +2697,51 @@ Mesh make_mesh(const ovx_fdg_context *c)
     return m;
 }
 
+// Host readback words of a context: [0] rows, [1] active bricks, [2] records,
+// [kHostCounters..] the counters after begin, [kHostFinish..] after finish.
+constexpr int kHostCounters = 4;
+constexpr int kHostFinish = 16;
+constexpr int kHostWords = 32;
+static_assert(kHostCounters * 8 + C_WORDS * 4 <= kHostFinish * 8 && kHostFinish * 8 + C_WORDS * 4 <= kHostWords * 8,
+              "readback regions overlap");
+
+__global__ void copy_word(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst)
+{
+    *dst = *src;
+}
+
+// Up to four device words/blocks to copy into the mapped readback words.
+struct Readback
+{
+    const void *src[4];
+    int bytes[4]; // multiples of 4
+    int dst[4];   // index of the first 8-byte host word
+    int n;
+    void add(const void *p, int nbytes, int word)
+    {
+        src[n] = p;
+        bytes[n] = nbytes;
+        dst[n] = word;
+        ++n;
+    }
+};
+
+// Writes the readback words into mapped host memory from a kernel: a
+// cudaMemcpyAsync would queue on a copy engine, where it waits behind any
+// large copy another stream has queued (such as the previous conversion's
+// outputs going to the host), and the host would wait with it.
+__global__ void readback(Readback r, unsigned long long *host)
+{
+    const int i = threadIdx.x;
+    if (i >= r.n)
+        return;
+    const uint32_t *s = (const uint32_t *)r.src[i];
+    volatile uint32_t *d = (volatile uint32_t *)(host + r.dst[i]);
+    for (int k = 0; k < r.bytes[i] / 4; ++k)
+        d[k] = s[k];
+    __threadfence_system();
+}
+
 uint32_t cap_u32(const Buf &b, size_t elem)
 {
     const size_t n = b.cap / elem;
@@ -2911,9 +2957,10 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, boff, ctx->nv + 1, st));
         edge_emit<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (const uint32_t *)ctx->emax.p, ctx->nv, boff,
                                                                      (unsigned long long *)ctx->bkeys.p);
-        // boundary edge count -> counters[C_BOUNDARY] (low word of the u64 total; at most 3F < 2^32)
-        OVX_CUDA(cudaMemcpyAsync((uint32_t *)ctx->counters.p + C_BOUNDARY, boff + ctx->nv, 4, cudaMemcpyDeviceToDevice, st));
-        ctx->launches += 4;
+        // boundary edge count -> counters[C_BOUNDARY] (low word of the u64 total; at most 3F < 2^32), by a
+        // kernel rather than a copy, which could queue behind another stream's large copy
+        copy_word<<<1, 1, 0, st>>>((const uint32_t *)(boff + ctx->nv), (uint32_t *)ctx->counters.p + C_BOUNDARY);
+        ctx->launches += 5;
         OVX_CUDA(cudaGetLastError());
     }
     stage(ctx, EV_EDGES, st);
@@ -2927,15 +2974,22 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
             launch_faces_boundary<COUNT, int>(ctx, A, st);
         OVX_CUDA(cudaGetLastError());
         OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->rcnt.p, (unsigned long long *)ctx->roff.p, nb + 1, st));
-        OVX_CUDA(cudaMemcpyAsync(&ctx->host[2], (unsigned long long *)ctx->roff.p + nb, 8, cudaMemcpyDeviceToHost, st));
     }
     stage(ctx, EV_RECORD_COUNT, st);
 
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[0], (unsigned long long *)ctx->bbase.p + nb, 8, cudaMemcpyDeviceToHost, st));
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[1], (unsigned long long *)ctx->aslot.p + nb, 8, cudaMemcpyDeviceToHost, st));
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[4], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
+    {
+        Readback r{};
+        r.add((unsigned long long *)ctx->bbase.p + nb, 8, 0);
+        r.add((unsigned long long *)ctx->aslot.p + nb, 8, 1);
+        if (full)
+            r.add((unsigned long long *)ctx->roff.p + nb, 8, 2);
+        r.add(ctx->counters.p, C_WORDS * 4, kHostCounters);
+        readback<<<1, 32, 0, st>>>(r, ctx->host_dev);
+        ++ctx->launches;
+    }
+    OVX_CUDA(cudaGetLastError());
     OVX_CUDA(cudaStreamSynchronize(st));
-    const uint32_t *hc = (const uint32_t *)&ctx->host[4];
+    const uint32_t *hc = (const uint32_t *)&ctx->host[kHostCounters];
     const int rc = status_to_error(ctx, hc[C_STATUS]);
     if (rc != OVX_FDG_OK)
         return rc;
@@ -2980,7 +3034,9 @@ int ovx_fdg_context_create(int device, ovx_fdg_context **out)
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
-    cudaError_t e = cudaMallocHost((void **)&ctx->host, 32 * sizeof(unsigned long long));
+    cudaError_t e = cudaHostAlloc((void **)&ctx->host, kHostWords * sizeof(unsigned long long), cudaHostAllocMapped);
+    if (e == cudaSuccess)
+        e = cudaHostGetDevicePointer((void **)&ctx->host_dev, ctx->host, 0);
     if (e == cudaSuccess)
     {
         cudaMemPoolProps props = {};
@@ -3315,7 +3371,13 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     ++ctx->launches;
     stage(ctx, EV_CONSTRAINED, st);
     OVX_CUDA(cudaGetLastError());
-    OVX_CUDA(cudaMemcpyAsync(&ctx->host[8], ctx->counters.p, C_WORDS * 4, cudaMemcpyDeviceToHost, st));
+    {
+        Readback r{};
+        r.add(ctx->counters.p, C_WORDS * 4, kHostFinish);
+        readback<<<1, 32, 0, st>>>(r, ctx->host_dev);
+        ++ctx->launches;
+    }
+    OVX_CUDA(cudaGetLastError());
     OVX_CUDA(mark_done(ctx, st));
     ctx->finished = 1;
     return OVX_FDG_OK;
@@ -3330,7 +3392,7 @@ int ovx_fdg_sync_status(ovx_fdg_context *ctx, void *stream)
     if (!ctx->finished)
         return OVX_FDG_OK;
     ctx->finished = 0;
-    return status_to_error(ctx, ((const uint32_t *)&ctx->host[8])[C_STATUS]);
+    return status_to_error(ctx, ((const uint32_t *)&ctx->host[kHostFinish])[C_STATUS]);
 }
 
 int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *triangles, int64_t num_triangles,
