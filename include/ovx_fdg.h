@@ -115,6 +115,17 @@ int ovx_z_order_encode(void *stream, const int32_t *x, const int32_t *y, const i
 int ovx_z_order_decode(void *stream, const int32_t *codes, int64_t n, int32_t *x, int32_t *y, int32_t *z);
 
 /*
+ * Hilbert codes, o_voxel.serialize.encode_seq / decode_seq with mode='hilbert'
+ * (serialize.py:7-66, src/serialize/hilbert.cu:33-130 (CPU) and :132-240
+ * (CUDA), src/ext.cpp:30-31): J. Skilling's transposed Hilbert index of the
+ * low 10 bits of x, y, z, its three words interleaved like the z-order code;
+ * device int32 arrays of length n, enqueued on `stream`.  Coordinates must lie
+ * in [0, 1024).
+ */
+int ovx_hilbert_encode(void *stream, const int32_t *x, const int32_t *y, const int32_t *z, int64_t n, int32_t *codes);
+int ovx_hilbert_decode(void *stream, const int32_t *codes, int64_t n, int32_t *x, int32_t *y, int32_t *z);
+
+/*
  * .vxz attribute packing of a conversion's outputs, as the reference's example
  * does before writing (examples/mesh2ovox.py:51-54): dual_u8[i][a] =
  * uint8(clamp(dual[i][a] * resolution[a] - voxel[i][a], 0, 1) * 255) (float32,

@@ -383,30 +383,53 @@ std::tuple<torch::Tensor, torch::Tensor> pack_flexible_dual_grid_cuda(const torc
     return std::make_tuple(du, fu);
 }
 
-// o_voxel.serialize z-order codes (reference: src/ext.cpp:28-29, src/serialize/api.cu)
-torch::Tensor z_order_encode_cuda(const torch::Tensor &x, const torch::Tensor &y, const torch::Tensor &z)
+// o_voxel.serialize codes (reference: src/ext.cpp:28-31, src/serialize/api.cu): z-order and Hilbert
+using EncodeFn = int (*)(void *, const int32_t *, const int32_t *, const int32_t *, int64_t, int32_t *);
+using DecodeFn = int (*)(void *, const int32_t *, int64_t, int32_t *, int32_t *, int32_t *);
+
+torch::Tensor encode_codes(EncodeFn fn, const char *name, const torch::Tensor &x, const torch::Tensor &y, const torch::Tensor &z)
 {
-    TORCH_CHECK(x.is_cuda() && y.is_cuda() && z.is_cuda(), "z_order_encode_cuda: CUDA tensors expected");
-    TORCH_CHECK(x.numel() == y.numel() && x.numel() == z.numel(), "z_order_encode_cuda: x, y, z differ in length");
+    TORCH_CHECK(x.is_cuda() && y.is_cuda() && z.is_cuda(), name, ": CUDA tensors expected");
+    TORCH_CHECK(x.numel() == y.numel() && x.numel() == z.numel(), name, ": x, y, z differ in length");
     const c10::cuda::CUDAGuard guard(x.device());
     auto xi = x.to(torch::kInt32).contiguous(), yi = y.to(torch::kInt32).contiguous(), zi = z.to(torch::kInt32).contiguous();
     auto codes = torch::empty_like(xi);
-    const int rc = ovx_z_order_encode(at::cuda::getCurrentCUDAStream(x.get_device()).stream(), xi.data_ptr<int32_t>(),
-                                      yi.data_ptr<int32_t>(), zi.data_ptr<int32_t>(), xi.numel(), codes.data_ptr<int32_t>());
-    TORCH_CHECK(rc == OVX_FDG_OK, "z_order_encode_cuda failed: ", ovx_fdg_status_string(rc));
+    const int rc = fn(at::cuda::getCurrentCUDAStream(x.get_device()).stream(), xi.data_ptr<int32_t>(), yi.data_ptr<int32_t>(),
+                      zi.data_ptr<int32_t>(), xi.numel(), codes.data_ptr<int32_t>());
+    TORCH_CHECK(rc == OVX_FDG_OK, name, " failed: ", ovx_fdg_status_string(rc));
     return codes;
+}
+
+std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> decode_codes(DecodeFn fn, const char *name, const torch::Tensor &codes)
+{
+    TORCH_CHECK(codes.is_cuda(), name, ": CUDA tensor expected");
+    const c10::cuda::CUDAGuard guard(codes.device());
+    auto c = codes.to(torch::kInt32).contiguous();
+    auto x = torch::empty_like(c), y = torch::empty_like(c), z = torch::empty_like(c);
+    const int rc = fn(at::cuda::getCurrentCUDAStream(codes.get_device()).stream(), c.data_ptr<int32_t>(), c.numel(),
+                      x.data_ptr<int32_t>(), y.data_ptr<int32_t>(), z.data_ptr<int32_t>());
+    TORCH_CHECK(rc == OVX_FDG_OK, name, " failed: ", ovx_fdg_status_string(rc));
+    return std::make_tuple(x, y, z);
+}
+
+torch::Tensor z_order_encode_cuda(const torch::Tensor &x, const torch::Tensor &y, const torch::Tensor &z)
+{
+    return encode_codes(ovx_z_order_encode, "z_order_encode_cuda", x, y, z);
 }
 
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> z_order_decode_cuda(const torch::Tensor &codes)
 {
-    TORCH_CHECK(codes.is_cuda(), "z_order_decode_cuda: CUDA tensor expected");
-    const c10::cuda::CUDAGuard guard(codes.device());
-    auto c = codes.to(torch::kInt32).contiguous();
-    auto x = torch::empty_like(c), y = torch::empty_like(c), z = torch::empty_like(c);
-    const int rc = ovx_z_order_decode(at::cuda::getCurrentCUDAStream(codes.get_device()).stream(), c.data_ptr<int32_t>(),
-                                      c.numel(), x.data_ptr<int32_t>(), y.data_ptr<int32_t>(), z.data_ptr<int32_t>());
-    TORCH_CHECK(rc == OVX_FDG_OK, "z_order_decode_cuda failed: ", ovx_fdg_status_string(rc));
-    return std::make_tuple(x, y, z);
+    return decode_codes(ovx_z_order_decode, "z_order_decode_cuda", codes);
+}
+
+torch::Tensor hilbert_encode_cuda(const torch::Tensor &x, const torch::Tensor &y, const torch::Tensor &z)
+{
+    return encode_codes(ovx_hilbert_encode, "hilbert_encode_cuda", x, y, z);
+}
+
+std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> hilbert_decode_cuda(const torch::Tensor &codes)
+{
+    return decode_codes(ovx_hilbert_decode, "hilbert_decode_cuda", codes);
 }
 
 PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
@@ -430,4 +453,6 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
     m.def("flexible_dual_grid_to_mesh_cuda", &flexible_dual_grid_to_mesh_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("pack_flexible_dual_grid_cuda", &pack_flexible_dual_grid_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("z_order_decode_cuda", &z_order_decode_cuda, py::call_guard<py::gil_scoped_release>());
+    m.def("hilbert_encode_cuda", &hilbert_encode_cuda, py::call_guard<py::gil_scoped_release>());
+    m.def("hilbert_decode_cuda", &hilbert_decode_cuda, py::call_guard<py::gil_scoped_release>());
 }

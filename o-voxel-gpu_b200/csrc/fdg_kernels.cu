@@ -2301,6 +2301,79 @@ __global__ void z_order_decode_kernel(const int32_t *__restrict__ codes, long lo
     z[i] = (int32_t)compact3_10(c);
 }
 
+// Hilbert codes (o_voxel.serialize mode 'hilbert', src/serialize/hilbert.cu:33-130):
+// J. Skilling's transposed Hilbert index ("Programming the Hilbert curve",
+// AIP Conf. Proc. 707, 2004) for 3 axes of 10 bits, its three transposed words
+// interleaved like the z-order code.  One thread per code; the bit planes are
+// walked with the axes in registers.
+__device__ __forceinline__ void hilbert_exchange(uint32_t &a0, uint32_t &ai, uint32_t q)
+{
+    const uint32_t low = q - 1u;
+    if (ai & q)
+        a0 ^= low;
+    else
+    {
+        const uint32_t swap = (a0 ^ ai) & low;
+        a0 ^= swap;
+        ai ^= swap;
+    }
+}
+
+__global__ void hilbert_encode_kernel(const int32_t *__restrict__ x, const int32_t *__restrict__ y, const int32_t *__restrict__ z,
+                                      long long n, int32_t *__restrict__ codes)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    uint32_t a0 = (uint32_t)x[i] & 1023u, a1 = (uint32_t)y[i] & 1023u, a2 = (uint32_t)z[i] & 1023u;
+    // undo the excess work, top bit plane first
+#pragma unroll
+    for (uint32_t q = 1u << 9; q > 1u; q >>= 1)
+    {
+        hilbert_exchange(a0, a0, q);
+        hilbert_exchange(a0, a1, q);
+        hilbert_exchange(a0, a2, q);
+    }
+    // Gray encode
+    a1 ^= a0;
+    a2 ^= a1;
+    uint32_t flip = 0;
+#pragma unroll
+    for (uint32_t q = 1u << 9; q > 1u; q >>= 1)
+        if (a2 & q)
+            flip ^= q - 1u;
+    a0 ^= flip;
+    a1 ^= flip;
+    a2 ^= flip;
+    codes[i] = (int32_t)((spread3_10(a0) << 2) | (spread3_10(a1) << 1) | spread3_10(a2));
+}
+
+__global__ void hilbert_decode_kernel(const int32_t *__restrict__ codes, long long n, int32_t *__restrict__ x,
+                                      int32_t *__restrict__ y, int32_t *__restrict__ z)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t c = (uint32_t)codes[i];
+    uint32_t a0 = compact3_10(c >> 2), a1 = compact3_10(c >> 1), a2 = compact3_10(c);
+    // Gray decode
+    const uint32_t half = a2 >> 1;
+    a2 ^= a1;
+    a1 ^= a0;
+    a0 ^= half;
+    // redo the excess work, bottom bit plane first
+#pragma unroll
+    for (uint32_t q = 2u; q != (1u << 10); q <<= 1)
+    {
+        hilbert_exchange(a0, a2, q);
+        hilbert_exchange(a0, a1, q);
+        hilbert_exchange(a0, a0, q);
+    }
+    x[i] = (int32_t)a0;
+    y[i] = (int32_t)a1;
+    z[i] = (int32_t)a2;
+}
+
 // ===========================================================================
 // allocation-free occupancy (ovx_fdg_occupancy_noalloc)
 // ===========================================================================
@@ -3133,6 +3206,26 @@ int ovx_z_order_decode(void *stream, const int32_t *codes, int64_t n, int32_t *x
     if (n == 0)
         return OVX_FDG_OK;
     z_order_decode_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(codes, n, x, y, z);
+    return cudaGetLastError() == cudaSuccess ? OVX_FDG_OK : OVX_FDG_CUDA_ERROR;
+}
+
+int ovx_hilbert_encode(void *stream, const int32_t *x, const int32_t *y, const int32_t *z, int64_t n, int32_t *codes)
+{
+    if (n < 0 || (n > 0 && (!x || !y || !z || !codes)))
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (n == 0)
+        return OVX_FDG_OK;
+    hilbert_encode_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(x, y, z, n, codes);
+    return cudaGetLastError() == cudaSuccess ? OVX_FDG_OK : OVX_FDG_CUDA_ERROR;
+}
+
+int ovx_hilbert_decode(void *stream, const int32_t *codes, int64_t n, int32_t *x, int32_t *y, int32_t *z)
+{
+    if (n < 0 || (n > 0 && (!x || !y || !z || !codes)))
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (n == 0)
+        return OVX_FDG_OK;
+    hilbert_decode_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(codes, n, x, y, z);
     return cudaGetLastError() == cudaSuccess ? OVX_FDG_OK : OVX_FDG_CUDA_ERROR;
 }
 

@@ -35,6 +35,8 @@ PROTOTYPES = [
     ("ovx_fdg_set_output_order", ctypes.c_int, [_P, ctypes.c_int]),
     ("ovx_z_order_encode", ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
     ("ovx_z_order_decode", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
+    ("ovx_hilbert_encode", ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
+    ("ovx_hilbert_decode", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
     ("ovx_fdg_pack", ctypes.c_int, [_P, _P, _P, _P, _I64, _P, _P, _P]),
     ("ovx_fdg_mesh_context_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
     ("ovx_fdg_mesh_context_destroy", None, [_P]),

@@ -89,7 +89,29 @@ def build_ref_zorder(force=False):
     return REF_ZORDER_SO
 
 
+REF_HILBERT_SO = os.path.join(REF_DIR, "hilbert_ref.so")
+
+
+def build_ref_hilbert(force=False):
+    """Compile the reference's Hilbert source (src/serialize/hilbert.cu; its CPU
+    functions are what the binding calls) into oracle/_ref; returns the .so path
+    or None if the source is absent."""
+    src = os.path.join(REFERENCE_ROOT, "src", "serialize", "hilbert.cu")
+    if not os.path.exists(src):
+        return REF_HILBERT_SO if os.path.exists(REF_HILBERT_SO) else None
+    binding = os.path.join(HERE, "ref_hilbert_binding.cu")
+    if not (force or _newer(REF_HILBERT_SO, [src, binding])):
+        return REF_HILBERT_SO
+    os.makedirs(REF_DIR, exist_ok=True)
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    cmd = [nvcc, "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC", "-shared",
+           "-I", os.path.dirname(src), src, binding, "-o", REF_HILBERT_SO]
+    subprocess.check_call(cmd)
+    return REF_HILBERT_SO
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
     print(build_ref_zorder(force="--force" in sys.argv))
+    print(build_ref_hilbert(force="--force" in sys.argv))

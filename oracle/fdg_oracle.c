@@ -689,3 +689,100 @@ void fdg_oracle_z_order_decode(int64_t n, const int32_t *codes, int32_t *x, int3
         z[k] = (int32_t)d;
     }
 }
+
+/*
+ * Hilbert codes of o_voxel.serialize.encode_seq / decode_seq, mode 'hilbert'
+ * (serialize/hilbert.cu:33-130 and serialize.py:7-66).  The reference uses
+ * J. Skilling's transposed-index form of the Hilbert curve ("Programming the
+ * Hilbert curve", AIP Conf. Proc. 707, 2004) for 3 axes of 10 bits: the axes
+ * are turned into the transposed index (undo the excess work bit plane by bit
+ * plane from the top, then Gray-encode), and the three transposed words are
+ * interleaved like the z-order code (word 0 the most significant of each
+ * triple).  Decoding runs the inverse steps.  Coordinates in [0, 1024).
+ */
+static void skilling_axes_to_transpose(uint32_t a[3])
+{
+    for (uint32_t q = 1u << 9; q > 1u; q >>= 1)
+    {
+        const uint32_t low = q - 1u;
+        for (int i = 0; i < 3; ++i)
+        {
+            if (a[i] & q)
+                a[0] ^= low;
+            else
+            {
+                const uint32_t swap = (a[0] ^ a[i]) & low;
+                a[0] ^= swap;
+                a[i] ^= swap;
+            }
+        }
+    }
+    a[1] ^= a[0];
+    a[2] ^= a[1];
+    uint32_t flip = 0;
+    for (uint32_t q = 1u << 9; q > 1u; q >>= 1)
+        if (a[2] & q)
+            flip ^= q - 1u;
+    a[0] ^= flip;
+    a[1] ^= flip;
+    a[2] ^= flip;
+}
+
+static void skilling_transpose_to_axes(uint32_t a[3])
+{
+    const uint32_t half = a[2] >> 1;
+    a[2] ^= a[1];
+    a[1] ^= a[0];
+    a[0] ^= half;
+    for (uint32_t q = 2u; q != (1u << 10); q <<= 1)
+    {
+        const uint32_t low = q - 1u;
+        for (int i = 2; i >= 0; --i)
+        {
+            if (a[i] & q)
+                a[0] ^= low;
+            else
+            {
+                const uint32_t swap = (a[0] ^ a[i]) & low;
+                a[0] ^= swap;
+                a[i] ^= swap;
+            }
+        }
+    }
+}
+
+void fdg_oracle_hilbert_encode(int64_t n, const int32_t *x, const int32_t *y, const int32_t *z, int32_t *codes)
+{
+    for (int64_t k = 0; k < n; ++k)
+    {
+        uint32_t a[3] = {(uint32_t)x[k] & 1023u, (uint32_t)y[k] & 1023u, (uint32_t)z[k] & 1023u};
+        skilling_axes_to_transpose(a);
+        uint32_t c = 0;
+        for (int i = 0; i < 10; ++i)
+        {
+            c |= ((a[0] >> i) & 1u) << (3 * i + 2);
+            c |= ((a[1] >> i) & 1u) << (3 * i + 1);
+            c |= ((a[2] >> i) & 1u) << (3 * i);
+        }
+        codes[k] = (int32_t)c;
+    }
+}
+
+void fdg_oracle_hilbert_decode(int64_t n, const int32_t *codes, int32_t *x, int32_t *y, int32_t *z)
+{
+    for (int64_t k = 0; k < n; ++k)
+    {
+        const uint32_t c = (uint32_t)codes[k];
+        uint32_t a[3] = {0, 0, 0};
+        for (int i = 0; i < 10; ++i)
+        {
+            a[0] |= ((c >> (3 * i + 2)) & 1u) << i;
+            a[1] |= ((c >> (3 * i + 1)) & 1u) << i;
+            a[2] |= ((c >> (3 * i)) & 1u) << i;
+        }
+        skilling_transpose_to_axes(a);
+        x[k] = (int32_t)a[0];
+        y[k] = (int32_t)a[1];
+        z[k] = (int32_t)a[2];
+    }
+}

@@ -65,6 +65,8 @@ def lib():
         _LIB.fdg_oracle_free_ptr.argtypes = [ctypes.c_void_p]
         _LIB.fdg_oracle_z_order_encode.argtypes = [ctypes.c_int64] + [ctypes.c_void_p] * 4
         _LIB.fdg_oracle_z_order_decode.argtypes = [ctypes.c_int64] + [ctypes.c_void_p] * 4
+        _LIB.fdg_oracle_hilbert_encode.argtypes = [ctypes.c_int64] + [ctypes.c_void_p] * 4
+        _LIB.fdg_oracle_hilbert_decode.argtypes = [ctypes.c_int64] + [ctypes.c_void_p] * 4
     return _LIB
 
 
@@ -81,6 +83,32 @@ def z_order_decode(codes):
     x, y, z = (np.empty(codes.shape[0], dtype=np.int32) for _ in range(3))
     lib().fdg_oracle_z_order_decode(codes.shape[0], codes.ctypes.data, x.ctypes.data, y.ctypes.data, z.ctypes.data)
     return x, y, z
+
+
+def hilbert_encode(x, y, z) -> np.ndarray:
+    """Oracle Hilbert codes (int32) of int coordinates in [0, 1024)."""
+    x, y, z = (np.ascontiguousarray(a, dtype=np.int32) for a in (x, y, z))
+    out = np.empty(x.shape[0], dtype=np.int32)
+    lib().fdg_oracle_hilbert_encode(x.shape[0], x.ctypes.data, y.ctypes.data, z.ctypes.data, out.ctypes.data)
+    return out
+
+
+def hilbert_decode(codes):
+    codes = np.ascontiguousarray(codes, dtype=np.int32)
+    x, y, z = (np.empty(codes.shape[0], dtype=np.int32) for _ in range(3))
+    lib().fdg_oracle_hilbert_decode(codes.shape[0], codes.ctypes.data, x.ctypes.data, y.ctypes.data, z.ctypes.data)
+    return x, y, z
+
+
+def ref_hilbert_lib():
+    """The reference's own CPU Hilbert functions (oracle/_ref/hilbert_ref.so), or None if not built."""
+    so = os.path.join(HERE, "_ref", "hilbert_ref.so")
+    if not os.path.exists(so):
+        return None
+    L = ctypes.CDLL(so)
+    L.ref_hilbert_encode.argtypes = [ctypes.c_size_t] + [ctypes.c_void_p] * 4
+    L.ref_hilbert_decode.argtypes = [ctypes.c_size_t] + [ctypes.c_void_p] * 4
+    return L
 
 
 def ref_z_order_lib():

@@ -8,12 +8,14 @@ grid range, weights) and the reference outputs in the reference's own row
 order (first-touch insertion order): voxel coordinates, dual vertices and
 intersected flags, plus the occupancy-only result of intersect_occ_cpu.
 
-Also z_order.npz: z-order codes from the reference's own CPU implementation
-(src/serialize/z_order.cu, built into oracle/_ref).
+Also z_order.npz and hilbert.npz: serialisation codes from the reference's
+own CPU implementations (src/serialize/z_order.cu and hilbert.cu, built into
+oracle/_ref).
 
 Run from the repository root where the reference source tree is available:
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py z_order    # only the z-order fixture
+    python tests/golden/make_golden.py hilbert    # only the Hilbert fixture
 """
 import os
 import sys
@@ -54,11 +56,36 @@ def make_z_order():
     print(f"z_order: {n} coordinates")
 
 
+def make_hilbert():
+    """hilbert.npz: the same kind of coordinates, the reference's CPU Hilbert
+    codes of them (src/serialize/hilbert.cu, built into oracle/_ref/hilbert_ref.so),
+    and the reference's decode of those codes."""
+    B.build_ref_hilbert()
+    L = O.ref_hilbert_lib()
+    if L is None:
+        raise SystemExit("reference Hilbert source not built (needs the reference source tree)")
+    rng = np.random.default_rng(4321)
+    xyz = rng.integers(0, 1024, size=(4096, 3), dtype=np.uint32)
+    edge = np.array([[0, 0, 0], [1023, 1023, 1023], [1023, 0, 0], [0, 1023, 0], [0, 0, 1023], [512, 256, 128],
+                     [1, 2, 4], [7, 7, 7], [8, 8, 8], [511, 512, 513], [1, 0, 0], [0, 1, 0], [0, 0, 1]], dtype=np.uint32)
+    xyz = np.ascontiguousarray(np.concatenate([edge, xyz]))
+    x, y, z = (np.ascontiguousarray(xyz[:, k]) for k in range(3))
+    n = xyz.shape[0]
+    codes = np.empty(n, dtype=np.uint32)
+    L.ref_hilbert_encode(n, x.ctypes.data, y.ctypes.data, z.ctypes.data, codes.ctypes.data)
+    dx, dy, dz = (np.empty(n, dtype=np.uint32) for _ in range(3))
+    L.ref_hilbert_decode(n, codes.ctypes.data, dx.ctypes.data, dy.ctypes.data, dz.ctypes.data)
+    np.savez_compressed(os.path.join(HERE, "hilbert.npz"), xyz=xyz.astype(np.int32), codes=codes.astype(np.int32),
+                        decoded=np.stack([dx, dy, dz], 1).astype(np.int32))
+    print(f"hilbert: {n} coordinates")
+
+
 def main():
-    if len(sys.argv) > 1 and sys.argv[1] == "z_order":
-        make_z_order()
+    if len(sys.argv) > 1 and sys.argv[1] in ("z_order", "hilbert"):
+        (make_z_order if sys.argv[1] == "z_order" else make_hilbert)()
         return
     make_z_order()
+    make_hilbert()
     B.build_ref()
     mod = O.ref_module()
     if mod is None:

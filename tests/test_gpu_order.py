@@ -1,6 +1,7 @@
 """Output row order: order='z_order' gives the native rows sorted by their
 o_voxel.serialize.encode_seq code, identically; encode_seq / decode_seq on
-the GPU against the golden codes of the reference implementation."""
+the GPU, in both modes (z_order, hilbert), against the golden codes of the
+reference implementation."""
 import os
 
 import numpy as np
@@ -11,6 +12,7 @@ from fdg_check import assert_fdg_equal
 from oracle import oracle as O
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "z_order.npz")
+GOLDEN_HILBERT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "hilbert.npz")
 
 
 @pytest.mark.gpu
@@ -30,6 +32,32 @@ def test_encode_decode_seq_golden(cuda):
     x = d["xyz"]
     assert np.array_equal(codes_p, O.z_order_encode(x[:, 2], x[:, 0], x[:, 1]))
     assert np.array_equal(o_voxel.serialize.decode_seq(torch.from_numpy(codes_p).to(cuda), permute=perm).cpu().numpy(), x)
+
+
+@pytest.mark.gpu
+def test_encode_decode_seq_hilbert_golden(cuda):
+    import torch
+    import o_voxel
+
+    d = np.load(GOLDEN_HILBERT)
+    xyz = torch.from_numpy(d["xyz"]).to(cuda)
+    codes = o_voxel.serialize.encode_seq(xyz, mode="hilbert")
+    assert np.array_equal(codes.cpu().numpy(), d["codes"])
+    back = o_voxel.serialize.decode_seq(codes, mode="hilbert")
+    assert np.array_equal(back.cpu().numpy(), d["decoded"])
+    perm = [1, 2, 0]
+    codes_p = o_voxel.serialize.encode_seq(xyz, permute=perm, mode="hilbert").cpu().numpy()
+    x = d["xyz"]
+    assert np.array_equal(codes_p, O.hilbert_encode(x[:, 1], x[:, 2], x[:, 0]))
+    back_p = o_voxel.serialize.decode_seq(torch.from_numpy(codes_p).to(cuda), permute=perm, mode="hilbert")
+    assert np.array_equal(back_p.cpu().numpy(), x)
+    # every code of a 64^3 block of the curve, through the C ABI, against the oracle
+    all_codes = torch.arange(1 << 18, dtype=torch.int32, device=cuda)
+    dec = o_voxel.serialize.decode_seq(all_codes, mode="hilbert").cpu().numpy()
+    ox, oy, oz = O.hilbert_decode(np.arange(1 << 18, dtype=np.int32))
+    assert np.array_equal(dec, np.stack([ox, oy, oz], 1))
+    assert np.array_equal(o_voxel.serialize.encode_seq(torch.from_numpy(dec).to(cuda), mode="hilbert").cpu().numpy(),
+                          np.arange(1 << 18, dtype=np.int32))
 
 
 def _by_code(vox, *cols):

@@ -10,9 +10,9 @@ import pytest
 import fdg_workloads as W
 from oracle import oracle as O
 
-# conversion fixtures (z_order.npz holds serialisation codes; test_serialize_cpu.py covers it)
+# conversion fixtures (z_order.npz and hilbert.npz hold serialisation codes; test_serialize_cpu.py covers them)
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if os.path.basename(p) != "z_order.npz")
+                if os.path.basename(p) not in ("z_order.npz", "hilbert.npz"))
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])

@@ -72,7 +72,7 @@ def test_order_and_serialize_argument_checks():
         o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=8, aabb=[[0, 0, 0], [1, 1, 1]], order="hilbert")
     with pytest.raises(RuntimeError, match="CUDA tensors only"):
         o_voxel.serialize.encode_seq(torch.zeros(4, 3, dtype=torch.int32))
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(RuntimeError, match="CUDA tensors only"):
         o_voxel.serialize.encode_seq(torch.zeros(4, 3, dtype=torch.int32), mode="hilbert")
     with pytest.raises(ValueError):
         o_voxel.serialize.decode_seq(torch.zeros(4, dtype=torch.int32), mode="peano")
