@@ -2539,7 +2539,7 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, scan_units, face_large, face_units, qtab;
     Buf vcnt, voff, emax, bkeys, blong, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, contrib, vlist, fstage, estage, longv;
+    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, fstage, estage, longv;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     unsigned long long *host = nullptr;     // readback words: pinned, mapped host memory
     unsigned long long *host_dev = nullptr; // the same words as the device addresses them
@@ -2568,6 +2568,9 @@ struct ovx_fdg_context
     // end of the last conversion's queued work: the next conversion, possibly
     // on another stream, waits for it before reusing the workspace
     cudaEvent_t done = nullptr;
+    // second stream of begin: the boundary-edge pipeline runs on it beside the scanline pass
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool done_valid = false;
 };
 
@@ -2579,7 +2582,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large, &c->scan_units,
                 &c->face_large, &c->face_units, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->blong, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv,
+                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv,
                 &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
@@ -2667,17 +2670,32 @@ cudaError_t ensure(cudaStream_t st, ovx_fdg_context *ctx, Buf &b, size_t bytes)
     return cudaSuccess;
 }
 
+// Exclusive scan with CUB; `tmp` is the scratch of the stream it runs on.
 template <typename In, typename Out>
-cudaError_t exclusive_scan(ovx_fdg_context *ctx, const In *in, Out *out, long long n, cudaStream_t st)
+cudaError_t exclusive_scan(ovx_fdg_context *ctx, const In *in, Out *out, long long n, cudaStream_t st, Buf *tmp = nullptr)
 {
+    Buf &t = tmp ? *tmp : ctx->cub_tmp;
     size_t bytes = 0;
     cudaError_t e = cub::DeviceScan::ExclusiveScan(nullptr, bytes, in, out, cub::Sum(), Out(0), (int)n, st);
     if (e != cudaSuccess)
         return e;
-    e = ensure(st, ctx, ctx->cub_tmp, bytes);
+    e = ensure(st, ctx, t, bytes);
     if (e != cudaSuccess)
         return e;
-    return cub::DeviceScan::ExclusiveScan(ctx->cub_tmp.p, bytes, in, out, cub::Sum(), Out(0), (int)n, st);
+    return cub::DeviceScan::ExclusiveScan(t.p, bytes, in, out, cub::Sum(), Out(0), (int)n, st);
+}
+
+// The context's second stream and its fork/join events, created on first use.
+cudaError_t side_stream(ovx_fdg_context *ctx)
+{
+    cudaError_t e = cudaSuccess;
+    if (!ctx->side)
+        e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !ctx->fork_ev)
+        e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess && !ctx->join_ev)
+        e = cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming);
+    return e;
 }
 
 inline unsigned blocks_for(long long n, int threads)
@@ -2979,6 +2997,44 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->bcount.p + nb, 0, 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->aflag.p + nb, 0, 4, st));
 
+    if (boundary && nf > 0)
+    {
+        // undirected edges and the boundary list (edges used once), on the side
+        // stream: they need only the mesh, so they run beside the scanline pass
+        OVX_CUDA(side_stream(ctx));
+        cudaStream_t es = ctx->side;
+        OVX_CUDA(cudaEventRecord(ctx->fork_ev, st));
+        OVX_CUDA(cudaStreamWaitEvent(es, ctx->fork_ev, 0));
+        OVX_CUDA(cudaMemsetAsync(ctx->vcnt.p, 0, (size_t)(ctx->nv + 1) * 4, es));
+        uint32_t *vcnt = (uint32_t *)ctx->vcnt.p;
+        unsigned long long *voff = (unsigned long long *)ctx->voff.p;
+        if (ctx->fbytes == 8)
+            edge_count<long long><<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const long long *)ctx->faces, nf, ctx->nv, vcnt);
+        else
+            edge_count<int><<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const int *)ctx->faces, nf, ctx->nv, vcnt);
+        OVX_CUDA(cudaGetLastError());
+        OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, voff, ctx->nv + 1, es, &ctx->cub_tmp_side));
+        if (ctx->fbytes == 8)
+            edge_fill<long long><<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const long long *)ctx->faces, nf, ctx->nv, voff, vcnt,
+                                                                               (uint32_t *)ctx->emax.p);
+        else
+            edge_fill<int><<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const int *)ctx->faces, nf, ctx->nv, voff, vcnt,
+                                                                         (uint32_t *)ctx->emax.p);
+        OVX_CUDA(cudaGetLastError());
+        // edge_fill left vcnt all zero: reuse it for the per-vertex boundary counts
+        edge_sort_count<<<blocks_for(ctx->nv, kThreads), kThreads, 0, es>>>(voff, (uint32_t *)ctx->emax.p, ctx->nv, vcnt);
+        OVX_CUDA(cudaGetLastError());
+        unsigned long long *boff = (unsigned long long *)ctx->boff.p;
+        OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, boff, ctx->nv + 1, es, &ctx->cub_tmp_side));
+        edge_emit<<<blocks_for(ctx->nv, kThreads), kThreads, 0, es>>>(voff, (const uint32_t *)ctx->emax.p, ctx->nv, boff,
+                                                                     (unsigned long long *)ctx->bkeys.p);
+        // boundary edge count -> counters[C_BOUNDARY] (low word of the u64 total; at most 3F < 2^32), by a
+        // kernel rather than a copy, which could queue behind another stream's large copy
+        copy_word<<<1, 1, 0, es>>>((const uint32_t *)(boff + ctx->nv), (uint32_t *)ctx->counters.p + C_BOUNDARY);
+        ctx->launches += 5;
+        OVX_CUDA(cudaGetLastError());
+        OVX_CUDA(cudaEventRecord(ctx->join_ev, es));
+    }
     stage(ctx, EV_BEGIN, st);
     GenArgs A = make_gen(ctx);
     if (!full)
@@ -3006,36 +3062,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     stage(ctx, EV_COMPACT, st);
 
     if (boundary && nf > 0)
-    {
-        OVX_CUDA(cudaMemsetAsync(ctx->vcnt.p, 0, (size_t)(ctx->nv + 1) * 4, st));
-        uint32_t *vcnt = (uint32_t *)ctx->vcnt.p;
-        unsigned long long *voff = (unsigned long long *)ctx->voff.p;
-        if (ctx->fbytes == 8)
-            edge_count<long long><<<blocks_for(nf, kThreads), kThreads, 0, st>>>((const long long *)ctx->faces, nf, ctx->nv, vcnt);
-        else
-            edge_count<int><<<blocks_for(nf, kThreads), kThreads, 0, st>>>((const int *)ctx->faces, nf, ctx->nv, vcnt);
-        OVX_CUDA(cudaGetLastError());
-        OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, voff, ctx->nv + 1, st));
-        if (ctx->fbytes == 8)
-            edge_fill<long long><<<blocks_for(nf, kThreads), kThreads, 0, st>>>((const long long *)ctx->faces, nf, ctx->nv, voff, vcnt,
-                                                                               (uint32_t *)ctx->emax.p);
-        else
-            edge_fill<int><<<blocks_for(nf, kThreads), kThreads, 0, st>>>((const int *)ctx->faces, nf, ctx->nv, voff, vcnt,
-                                                                         (uint32_t *)ctx->emax.p);
-        OVX_CUDA(cudaGetLastError());
-        // edge_fill left vcnt all zero: reuse it for the per-vertex boundary counts
-        edge_sort_count<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (uint32_t *)ctx->emax.p, ctx->nv, vcnt);
-        OVX_CUDA(cudaGetLastError());
-        unsigned long long *boff = (unsigned long long *)ctx->boff.p;
-        OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, boff, ctx->nv + 1, st));
-        edge_emit<<<blocks_for(ctx->nv, kThreads), kThreads, 0, st>>>(voff, (const uint32_t *)ctx->emax.p, ctx->nv, boff,
-                                                                     (unsigned long long *)ctx->bkeys.p);
-        // boundary edge count -> counters[C_BOUNDARY] (low word of the u64 total; at most 3F < 2^32), by a
-        // kernel rather than a copy, which could queue behind another stream's large copy
-        copy_word<<<1, 1, 0, st>>>((const uint32_t *)(boff + ctx->nv), (uint32_t *)ctx->counters.p + C_BOUNDARY);
-        ctx->launches += 5;
-        OVX_CUDA(cudaGetLastError());
-    }
+        OVX_CUDA(cudaStreamWaitEvent(st, ctx->join_ev, 0)); // the boundary edges, from the side stream
     stage(ctx, EV_EDGES, st);
 
     if (full)
@@ -3160,6 +3187,12 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
         cudaFreeHost(ctx->host);
     if (ctx->done)
         cudaEventDestroy(ctx->done);
+    if (ctx->side)
+        cudaStreamDestroy(ctx->side);
+    if (ctx->fork_ev)
+        cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev)
+        cudaEventDestroy(ctx->join_ev);
     for (int i = 0; i < kStageEvents; ++i)
         if (ctx->ev[i])
             cudaEventDestroy(ctx->ev[i]);
