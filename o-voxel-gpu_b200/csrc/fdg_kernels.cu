@@ -81,7 +81,7 @@ constexpr int kInlineFaceBricks = 8; // triangles whose face box spans more bric
 constexpr int kUnitCells = 64;        // cells per unit of work of a large (triangle, axis) pair
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
-constexpr int kListStage = 512; // contributions of a brick that brick_lists stages (and sorts) in shared memory
+constexpr int kListStage = 768; // contributions of a brick that brick_lists stages (and sorts) in shared memory
 // vlist word: first entry (bits 0-39) | count (bits 40-62) | sorted flag (bit 63)
 constexpr uint32_t kListCountMax = (1u << 23) - 1u;
 constexpr unsigned long long kListSorted = 1ull << 63;
@@ -1726,7 +1726,10 @@ struct ListShared
     uint32_t scan_tmp[kConsumeThreads / 32 + 1]; // per-warp offsets, then the brick's total
     int nvox;
     uint32_t status;
-    uint4 ent[kListStage]; // the brick's lists, when they fit: filled, short lists sorted, copied out
+    // the brick's lists, when they fit (keys and payloads apart: 12 bytes an
+    // entry): filled, short lists sorted, copied out
+    unsigned long long skey[kListStage];
+    uint32_t spay[kListStage];
 };
 
 struct ListCount
@@ -1754,6 +1757,23 @@ struct ListFill
             return;
         }
         out[k] = make_uint4((uint32_t)key, (uint32_t)(key >> 32), pay, 0u);
+    }
+};
+
+// The same into the brick's shared staging arrays.
+struct ListStageFill
+{
+    ListShared &S;
+    __device__ __forceinline__ void operator()(int i, unsigned long long key, uint32_t pay) const
+    {
+        const uint32_t k = atomicAdd(&S.off[i], 1u);
+        if (k >= (uint32_t)kListStage)
+        {
+            atomicOr(&S.status, (uint32_t)ST_REPLAY);
+            return;
+        }
+        S.skey[k] = key;
+        S.spay[k] = pay;
     }
 };
 
@@ -1854,7 +1874,7 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
         // the lists fit in shared memory: fill them there, sort the short ones
         // (one thread per voxel), copy the brick's lists out in one sweep
         {
-            ListFill fs{S, S.ent, (unsigned long long)kListStage};
+            ListStageFill fs{S};
             for (unsigned long long r = tid; r < nrec; r += blockDim.x)
                 expand(S, rec[r], fs);
         }
@@ -1864,23 +1884,29 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
             const uint32_t c = S.cnt[j];
             if (c < 2u || c >= (uint32_t)kWarpSortMin)
                 continue;
-            uint4 *L = S.ent + (S.off[j] - c);
+            unsigned long long *K = S.skey + (S.off[j] - c);
+            uint32_t *P = S.spay + (S.off[j] - c);
             for (uint32_t x = 1; x < c; ++x)
             {
-                const uint4 e = L[x];
-                const unsigned long long k = entry_key(e);
+                const unsigned long long k = K[x];
+                const uint32_t pv = P[x];
                 uint32_t y = x;
-                while (y > 0 && entry_key(L[y - 1]) > k)
+                while (y > 0 && K[y - 1] > k)
                 {
-                    L[y] = L[y - 1];
+                    K[y] = K[y - 1];
+                    P[y] = P[y - 1];
                     --y;
                 }
-                L[y] = e;
+                K[y] = k;
+                P[y] = pv;
             }
         }
         __syncthreads();
         for (uint32_t i = tid; i < total; i += blockDim.x)
-            out[i] = S.ent[i];
+        {
+            const unsigned long long k = S.skey[i];
+            out[i] = make_uint4((uint32_t)k, (uint32_t)(k >> 32), S.spay[i], 0u);
+        }
     }
     else
     {
