@@ -9,8 +9,11 @@ vertices shifted by ``aabb[0]`` in float32 before the conversion (fused into the
 kernels here when ``aabb[0]`` is known on the host).
 
 Differences, all deliberate:
-  * CUDA tensors only.  There is no CPU path in this product; CPU inputs raise
-    ``RuntimeError`` (the reference would run its single-threaded CPU code).
+  * Host (CPU) inputs are converted on the current CUDA device: they go up
+    through pinned memory and the results come back as CPU tensors (the
+    reference would run its single-threaded CPU code).  There is no CPU
+    implementation in this product: without a CUDA device, CPU inputs raise
+    ``RuntimeError``.
   * int64 faces are consumed directly instead of being cast to int32; indices
     outside ``[0, V)`` raise ``RuntimeError`` (the reference reads out of bounds).
   * Output rows are in a deterministic brick order (8x8x8 bricks, x fastest),
@@ -159,6 +162,28 @@ def _require_cuda(t: torch.Tensor, name: str):
         raise RuntimeError(f"{name}: this implementation runs on CUDA tensors only (got a {t.device} tensor)")
 
 
+def _host_device(t: torch.Tensor, name: str) -> torch.device:
+    """The CUDA device that converts host (CPU) inputs: the current one."""
+    if not torch.cuda.is_available():
+        raise RuntimeError(f"{name}: this implementation runs on CUDA tensors only (got a {t.device} tensor "
+                           "and no CUDA device is available)")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _upload(t: torch.Tensor, dev: torch.device) -> torch.Tensor:
+    return t.contiguous().pin_memory().to(dev, non_blocking=True)
+
+
+def _download(ts):
+    """Device results -> CPU tensors (pinned), after the copies have landed."""
+    hs = tuple(torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in ts)
+    for h, t in zip(hs, ts):
+        h.copy_(t, non_blocking=True)
+    if ts:
+        torch.cuda.current_stream(ts[0].device).synchronize()
+    return hs
+
+
 @torch.no_grad()
 def mesh_to_flexible_dual_grid(
     vertices: torch.Tensor,
@@ -176,8 +201,9 @@ def mesh_to_flexible_dual_grid(
     Convert a triangle mesh into a sparse flexible dual grid.
 
     Args:
-        vertices (torch.Tensor): [V, 3] mesh vertices (CUDA).
-        faces (torch.Tensor): [F, 3] triangle vertex indices (CUDA, int32 or int64).
+        vertices (torch.Tensor): [V, 3] mesh vertices (CUDA; CPU tensors are converted on the
+            current CUDA device and give CPU results).
+        faces (torch.Tensor): [F, 3] triangle vertex indices (int32 or int64, on the vertices' device).
         voxel_size: size of each voxel (float or 3 values); one of voxel_size/grid_size is required.
         grid_size: voxels per axis (int or 3 values).
         aabb: [[x0, y0, z0], [x1, y1, z1]] bounding box; computed from the vertices if omitted.
@@ -199,16 +225,23 @@ def mesh_to_flexible_dual_grid(
     """
     oc = _order_code(order)
     vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg = _grid_setup(vertices, faces, voxel_size, grid_size, aabb)
-    _require_cuda(vertices, "mesh_to_flexible_dual_grid")
+    host = not vertices.is_cuda
+    if host:
+        dev = _host_device(vertices, "mesh_to_flexible_dual_grid")
+        if aabb_cpu is None:
+            aabb_cpu = aabb.detach()
+        vertices, faces = _upload(vertices, dev), _upload(faces, dev)
     if aabb_cpu is not None:
         origin = [float(x) for x in aabb_cpu[0].tolist()]
-        return _ext().mesh_to_flexible_dual_grid_cuda_ex(vertices, faces, origin, voxel_size_arg, grid_range_arg,
-                                                         float(face_weight), float(boundary_weight),
-                                                         float(regularization_weight), oc)
-    # aabb derived on the device: shift with torch, exactly like the reference wrapper
-    vertices = vertices - aabb[0].reshape(1, 3)
-    return _ext().mesh_to_flexible_dual_grid_cuda(vertices, faces, voxel_size_arg, grid_range_arg, float(face_weight),
-                                                  float(boundary_weight), float(regularization_weight), oc)
+        out = _ext().mesh_to_flexible_dual_grid_cuda_ex(vertices, faces, origin, voxel_size_arg, grid_range_arg,
+                                                        float(face_weight), float(boundary_weight),
+                                                        float(regularization_weight), oc)
+    else:
+        # aabb derived on the device: shift with torch, exactly like the reference wrapper
+        vertices = vertices - aabb[0].reshape(1, 3)
+        out = _ext().mesh_to_flexible_dual_grid_cuda(vertices, faces, voxel_size_arg, grid_range_arg, float(face_weight),
+                                                     float(boundary_weight), float(regularization_weight), oc)
+    return _download(out) if host else out
 
 
 @torch.no_grad()
@@ -227,10 +260,14 @@ def intersect_occ(
     mesh_to_flexible_dual_grid, without quadrics or dual vertices.
     """
     vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg = _grid_setup(vertices, faces, voxel_size, grid_size, aabb)
-    _require_cuda(vertices, "intersect_occ")
+    host = not vertices.is_cuda
+    if host:
+        dev = _host_device(vertices, "intersect_occ")
+        vertices, faces, aabb = _upload(vertices, dev), _upload(faces, dev), aabb.to(dev)
     vertices = vertices - aabb[0].reshape(1, 3)
     triangles = vertices[faces.to(dtype=torch.long)].contiguous()
-    return _ext().intersect_occ_cuda(triangles, voxel_size_arg, grid_range_arg, _order_code(order))
+    out = _ext().intersect_occ_cuda(triangles, voxel_size_arg, grid_range_arg, _order_code(order))
+    return _download((out,))[0] if host else out
 
 
 @torch.no_grad()
@@ -251,7 +288,8 @@ def mesh_to_flexible_dual_grid_batch(
     returns for that mesh.
 
     Args:
-        meshes: sequence of (vertices [V,3], faces [F,3]) CUDA tensors, all on one device.
+        meshes: sequence of (vertices [V,3], faces [F,3]) CUDA tensors, all on one device
+            (CPU meshes are uploaded to the current CUDA device and give CPU results).
         voxel_size, grid_size, aabb: as in mesh_to_flexible_dual_grid, either one value
             for every mesh or a list with one value per mesh (with exactly three
             meshes a list of three numbers is one per-axis value: give per-mesh
@@ -280,11 +318,14 @@ def mesh_to_flexible_dual_grid_batch(
     vs_list = per_mesh_list(voxel_size, (3,)) if not isinstance(voxel_size, float) else False
     gs_list = per_mesh_list(grid_size, (3,)) if not isinstance(grid_size, int) else False
     ab_list = per_mesh_list(aabb, (2, 3))
-    verts, fcs, origins, vsizes, granges = [], [], [], [], []
+    verts, fcs, origins, vsizes, granges, host = [], [], [], [], [], []
     for i, (v, f) in enumerate(meshes):
         v, f, ab, ab_cpu, vs_arg, gr_arg = _grid_setup(v, f, per_mesh(voxel_size, i, vs_list),
                                                       per_mesh(grid_size, i, gs_list), per_mesh(aabb, i, ab_list))
-        _require_cuda(v, "mesh_to_flexible_dual_grid_batch")
+        host.append(not v.is_cuda)
+        if host[-1]:
+            dev = _host_device(v, "mesh_to_flexible_dual_grid_batch")
+            v, f = _upload(v, dev), _upload(f, dev)
         if ab_cpu is None:
             ab_cpu = ab.detach().cpu()
         verts.append(v)
@@ -292,9 +333,10 @@ def mesh_to_flexible_dual_grid_batch(
         origins.append([float(x) for x in ab_cpu[0].tolist()])
         vsizes.append(vs_arg)
         granges.append(gr_arg)
-    return _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
-                                                        float(boundary_weight), float(regularization_weight),
-                                                        int(workers), _order_code(order))
+    out = _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
+                                                       float(boundary_weight), float(regularization_weight),
+                                                       int(workers), _order_code(order))
+    return [_download(o) if h else o for o, h in zip(out, host)]
 
 
 @torch.no_grad()

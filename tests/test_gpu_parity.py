@@ -189,3 +189,41 @@ def test_two_streams_share_the_context(cuda):
     for oa, ob in outs:
         assert_fdg_equal(tuple(t.cpu().numpy() for t in oa), ra, "stream a")
         assert_fdg_equal(tuple(t.cpu().numpy() for t in ob), rb, "stream b")
+
+
+@pytest.mark.gpu
+def test_host_tensors(cuda):
+    """CPU inputs (the reference's CPU call) convert on the GPU and come back as
+    CPU tensors equal to the device results and to the oracle."""
+    import torch
+    import o_voxel
+
+    w = W.ico_cap(0)
+    v, f = torch.from_numpy(w.vertices), torch.from_numpy(w.faces)
+    host = o_voxel.convert.mesh_to_flexible_dual_grid(v, f, **w.kwargs())
+    assert all(t.device.type == "cpu" for t in host)
+    dev = o_voxel.convert.mesh_to_flexible_dual_grid(v.to(cuda), f.to(cuda), **w.kwargs())
+    for h, d in zip(host, dev):
+        assert torch.equal(h, d.cpu())
+    r = O.run_workload(w, "f32")
+    assert_fdg_equal(tuple(t.numpy() for t in host), (r.voxels, r.dual, r.intersected), "host tensors")
+    # aabb derived from the CPU vertices, as the reference CPU path does
+    kw = dict(w.kwargs())
+    kw.pop("aabb")
+    host2 = o_voxel.convert.mesh_to_flexible_dual_grid(v, f, **kw)
+    lo, hi = v.min(0).values, v.max(0).values
+    pad = (hi - lo) / (kw["grid_size"] - 1)
+    box = torch.stack([lo - pad * 0.5, hi + pad * 0.5]).tolist()
+    dev2 = o_voxel.convert.mesh_to_flexible_dual_grid(v.to(cuda), f.to(cuda), aabb=box, **kw)
+    for h, d in zip(host2, dev2):
+        assert torch.equal(h, d.cpu())
+    occ = o_voxel.convert.intersect_occ(v, f, grid_size=w.grid_size, aabb=w.aabb)
+    assert occ.device.type == "cpu"
+    assert torch.equal(occ, o_voxel.convert.intersect_occ(v.to(cuda), f.to(cuda), grid_size=w.grid_size, aabb=w.aabb).cpu())
+    batch = o_voxel.convert.mesh_to_flexible_dual_grid_batch([(v, f), (v.to(cuda), f.to(cuda))], grid_size=w.grid_size,
+                                                            aabb=w.aabb, face_weight=w.face_weight,
+                                                            boundary_weight=w.boundary_weight,
+                                                            regularization_weight=w.regularization_weight, workers=2)
+    assert batch[0][0].device.type == "cpu" and batch[1][0].is_cuda
+    for a, b, c in zip(batch[0], batch[1], host):
+        assert torch.equal(a, b.cpu()) and torch.equal(a, c)
