@@ -169,7 +169,7 @@ def run_reference(args, rank):
 BATCH_WORKERS = 8
 
 
-def run_batched(dev, steps=2):
+def run_batched(dev, steps=3, warmup=2):
     """256 seeded meshes built like the 282k-face one, face counts log-uniform in
     [1k, 500k] (about 21M faces in all), grid 64/128/256/512 per mesh, per-mesh
     aabb: the batched API against the same meshes converted one call at a time."""
@@ -193,7 +193,9 @@ def run_batched(dev, steps=2):
         o_voxel.convert.mesh_to_flexible_dual_grid_batch(meshes, grid_size=grids, aabb=aabbs, workers=BATCH_WORKERS, **kw)
 
     def timed(fn):
-        fn()
+        # the workers' contexts reach their largest workspaces during the warm-up
+        for _ in range(warmup):
+            fn()
         torch.cuda.synchronize()
         ms = []
         for _ in range(steps):
@@ -203,12 +205,13 @@ def run_batched(dev, steps=2):
             e1.record()
             torch.cuda.synchronize()
             ms.append(e0.elapsed_time(e1))
-        return sum(ms) / len(ms)
+        return statistics.median(ms), ms
 
-    t_plain = timed(plain)
-    t_batch = timed(batched)
+    t_plain, plain_ms = timed(plain)
+    t_batch, batch_ms = timed(batched)
     return {"workload": "256 meshes, faces log-uniform 1k-500k, grids 64-512, per-mesh aabb",
-            "meshes": len(ws), "faces": int(F), "workers": BATCH_WORKERS, "steps": steps,
+            "meshes": len(ws), "faces": int(F), "workers": BATCH_WORKERS, "steps": steps, "warmup": warmup,
+            "timing": "median of the steps", "plain_step_ms": plain_ms, "batched_step_ms": batch_ms,
             "plain_ms": t_plain, "plain_meshes_per_s": len(ws) / (t_plain / 1e3),
             "batched_ms": t_batch, "batched_meshes_per_s": len(ws) / (t_batch / 1e3),
             "batched_mfaces_per_s": F / (t_batch / 1e3) / 1e6, "speedup": t_plain / t_batch,
