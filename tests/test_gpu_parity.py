@@ -124,8 +124,9 @@ def test_bad_face_index_raises(cuda):
 
 def _face_heavy_workload():
     """Eight medium, slightly tilted triangles at grid 128: each hits hundreds of
-    voxels in the face stage, far more than the library's first guess of face
-    records per triangle, while each face box spans at most 64 bricks."""
+    voxels in the face and scanline stages, far more than the library's first
+    guess of records per triangle, and spans about 16 bricks (the large-triangle
+    units of large_rows and large_faces)."""
     rng = np.random.default_rng(11)
     verts, faces = [], []
     for k in range(8):
@@ -142,9 +143,9 @@ def _face_heavy_workload():
 
 @pytest.mark.gpu
 def test_face_record_staging_and_fallback(cuda):
-    """The first conversion on a fresh context overflows the staging array for
-    face records and re-runs the face tests in the fill pass; the second one
-    fits and buckets the staged records.  Both are bit-exact."""
+    """The first conversion on a fresh context overflows the staging arrays for
+    face and scanline records and re-runs those stages in the fill pass; the
+    second one fits and buckets the staged records.  Both are bit-exact."""
     import torch
     import ovx_fdg_abi as abi
 
