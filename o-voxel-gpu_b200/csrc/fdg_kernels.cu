@@ -1983,12 +1983,12 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
     // The warp orders the longer lists of its 32 voxels one after another: each
     // lane holds up to kWarpSortPer entries of the list and finds their ranks
     // among the list's (unique) keys, then stores the entries at those ranks.
-    for (int v = 0; v < 32; ++v)
+    const uint32_t need = __ballot_sync(0xffffffffu, n >= (uint32_t)kWarpSortMin && n <= (uint32_t)kWarpSortMax);
+    for (uint32_t m = need; m; m &= m - 1u)
     {
+        const int v = __ffs(m) - 1;
         const uint32_t nv = __shfl_sync(0xffffffffu, n, v);
         const unsigned long long fv = __shfl_sync(0xffffffffu, first, v);
-        if (nv < (uint32_t)kWarpSortMin || nv > (uint32_t)kWarpSortMax)
-            continue;
         uint4 *L = A.contrib + fv;
         const uint4 pad = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
         uint4 e[kWarpSortPer];
