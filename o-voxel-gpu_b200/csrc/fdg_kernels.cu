@@ -1794,13 +1794,11 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     load_brick_ranks(S, A.bits, b, A.zorder);
     const int nvox = S.nvox;
     const unsigned long long vbase = A.bbase[b];
-    // voxel coordinates of the brick's rows
-    for (int w = 0; w < kWordsPerBrick; ++w)
+    // voxel coordinates of the brick's rows (every thread a quarter of the brick)
+    for (int lv = tid; lv < 512; lv += blockDim.x)
     {
-        const uint32_t word = S.obits[w];
-        if (tid < 32 && ((word >> tid) & 1u))
+        if ((S.obits[lv >> 5] >> (lv & 31)) & 1u)
         {
-            const int lv = w * 32 + tid;
             const long long row = (long long)(vbase + dense_index(S, lv));
             A.vox[row * 3 + 0] = o[0] + (lv & 7);
             A.vox[row * 3 + 1] = o[1] + ((lv >> 3) & 7);
