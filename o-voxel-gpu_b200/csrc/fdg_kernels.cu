@@ -814,6 +814,11 @@ template <int M>
 __device__ __forceinline__ void face_hits(const GenArgs &A, const uint32_t (*pass)[32], const int lane, const uint32_t hits,
                                           const long long b, const uint32_t tri)
 {
+    // COUNT: k0 is this item's first rank among brick b's records -- the scanline
+    // records were all counted before, so it is the item's place in the bucket
+    uint32_t k0 = 0;
+    if (hits)
+        k0 = agg_add(A.rcnt, b, hits);
     if (M == COUNT && A.fstage)
     {
         uint32_t incl = hits;
@@ -829,6 +834,7 @@ __device__ __forceinline__ void face_hits(const GenArgs &A, const uint32_t (*pas
             base = atomicAdd(&A.counters[C_FSTAGED], incl);
         base = __shfl_sync(0xffffffffu, base, 31);
         unsigned long long pos = (unsigned long long)base + incl - hits;
+        uint32_t rank = k0;
         for (int w = 0; w < kWordsPerBrick && hits; ++w)
         {
             uint32_t pm = pass[w][lane];
@@ -837,34 +843,31 @@ __device__ __forceinline__ void face_hits(const GenArgs &A, const uint32_t (*pas
                 const int bt = __ffs(pm) - 1;
                 pm &= pm - 1u;
                 if (pos < A.fstage_cap)
-                    A.fstage[pos] = make_uint4((uint32_t)b, tri, kRecFace | (uint32_t)(w * 32 + bt), 0u);
+                    A.fstage[pos] = make_uint4((uint32_t)b, tri, kRecFace | (uint32_t)(w * 32 + bt), rank);
                 ++pos;
+                ++rank;
             }
         }
     }
-    if (hits)
+    if (M == FILL && hits)
     {
-        const uint32_t k0 = agg_add(A.rcnt, b, hits);
-        if (M == FILL)
+        if ((unsigned long long)k0 + hits > A.roff[b + 1] - A.roff[b])
+            atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
+        else
         {
-            if ((unsigned long long)k0 + hits > A.roff[b + 1] - A.roff[b])
-                atomicOr(&A.counters[C_STATUS], (uint32_t)ST_REPLAY);
-            else
+            unsigned long long pos = A.roff[b] + k0;
+            for (int w = 0; w < kWordsPerBrick; ++w)
             {
-                unsigned long long pos = A.roff[b] + k0;
-                for (int w = 0; w < kWordsPerBrick; ++w)
+                uint32_t pm = pass[w][lane];
+                while (pm)
                 {
-                    uint32_t pm = pass[w][lane];
-                    while (pm)
-                    {
-                        const int bt = __ffs(pm) - 1;
-                        pm &= pm - 1u;
-                        Rec rr;
-                        rr.a = tri;
-                        rr.b = kRecFace | (uint32_t)(w * 32 + bt);
-                        rr.c = 0u;
-                        A.rec[pos++] = rr;
-                    }
+                    const int bt = __ffs(pm) - 1;
+                    pm &= pm - 1u;
+                    Rec rr;
+                    rr.a = tri;
+                    rr.b = kRecFace | (uint32_t)(w * 32 + bt);
+                    rr.c = 0u;
+                    A.rec[pos++] = rr;
                 }
             }
         }
@@ -1130,7 +1133,7 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
     }
 }
 
-// Staged face records -> their bricks' buckets (after the scanline records).
+// Staged scanline records -> their bricks' buckets, through a cursor per brick.
 __global__ void __launch_bounds__(kThreads) bucket_records(const uint4 *__restrict__ stage, uint32_t n, uint32_t *__restrict__ cursor,
                                                            const unsigned long long *__restrict__ roff, Rec *__restrict__ rec,
                                                            uint32_t *__restrict__ counters)
@@ -1199,6 +1202,37 @@ __global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
         face_item<M>(A, W, lane, valid, lane, r);
         __syncwarp();
     }
+}
+
+// Staged face records -> their places in the bricks' buckets: the count pass
+// staged each with its rank in the brick, so no cursor is needed.
+__global__ void __launch_bounds__(kThreads) place_records(const uint4 *__restrict__ stage, uint32_t n,
+                                                          const unsigned long long *__restrict__ roff, Rec *__restrict__ rec,
+                                                          uint32_t *__restrict__ counters)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint4 r = stage[i];
+    const long long b = (long long)r.x;
+    const unsigned long long base = roff[b];
+    if ((unsigned long long)r.w >= roff[b + 1] - base)
+    {
+        atomicOr(&counters[C_STATUS], (uint32_t)ST_REPLAY);
+        return;
+    }
+    Rec o;
+    o.a = r.y;
+    o.b = r.z;
+    o.c = 0u;
+    rec[base + r.w] = o;
+}
+
+__global__ void copy_words(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = src[i];
 }
 
 constexpr int kLongWalk = 64; // boundary edges with a longer step bound are walked by a whole warp
@@ -2563,7 +2597,7 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, scan_units, face_large, face_units, qtab;
     Buf vcnt, voff, emax, bkeys, blong, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, fstage, estage, longv;
+    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, fstage, estage, longv, face_end;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     unsigned long long *host = nullptr;     // readback words: pinned, mapped host memory
     unsigned long long *host_dev = nullptr; // the same words as the device addresses them
@@ -2606,7 +2640,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large, &c->scan_units,
                 &c->face_large, &c->face_units, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->blong, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv,
+                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv, &c->face_end,
                 &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
@@ -2941,10 +2975,15 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
         {
             if (ctx->n_fstaged > 0)
             {
-                bucket_records<<<blocks_for((long long)ctx->n_fstaged, kThreads), kThreads, 0, st>>>(
-                    A.fstage, (uint32_t)ctx->n_fstaged, A.rcnt, A.roff, A.rec, A.counters);
+                place_records<<<blocks_for((long long)ctx->n_fstaged, kThreads), kThreads, 0, st>>>(
+                    A.fstage, (uint32_t)ctx->n_fstaged, A.roff, A.rec, A.counters);
                 ++ctx->launches;
             }
+            // the boundary records follow the face records: the bucket cursors
+            // as the count pass left them after the faces
+            copy_words<<<blocks_for(ctx->g.nbricks + 1, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->face_end.p, A.rcnt,
+                                                                                    ctx->g.nbricks + 1);
+            ++ctx->launches;
         }
         else
         {
@@ -2959,6 +2998,13 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
                 ++ctx->launches;
             }
             large_faces<M, IdxT><<<ctx->sms * 7, kFaceThreads, 0, st>>>(A);
+            ++ctx->launches;
+        }
+        if (M == COUNT && A.fstage)
+        {
+            // record counts after the scanline and face records, for the fill pass
+            copy_words<<<blocks_for(ctx->g.nbricks + 1, kThreads), kThreads, 0, st>>>(A.rcnt, (uint32_t *)ctx->face_end.p,
+                                                                                    ctx->g.nbricks + 1);
             ++ctx->launches;
         }
     }
@@ -3005,6 +3051,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         const unsigned long long guess = std::min(24ull * (unsigned long long)nf, 4ull * (unsigned long long)nf + (16ull << 20));
         const unsigned long long want = std::max(ctx->fstage_want, guess);
         OVX_CUDA(ensure(st, ctx, ctx->fstage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
+        OVX_CUDA(ensure(st, ctx, ctx->face_end, (size_t)(nb + 1) * 4));
     }
     if (boundary)
     {
