@@ -23,6 +23,8 @@
 //   contrib per-voxel contribution lists, 16 B entries; brick b owns entries
 //           [4*roff[b], 4*roff[b+1]) (a record yields at most 4 contributions)
 //   vlist   per output row: first entry (40 bits) | entry count << 40 | sorted << 63
+//   estage, fstage  event and face records staged by the count pass (16 B,
+//           {brick, t, code, z} and {brick, t, code, rank in the brick})
 //   btab    line quadric per boundary edge (10 floats)
 //
 // begin (ends with the one host synchronisation of a conversion):
@@ -36,20 +38,23 @@
 //                       used once -> boundary list
 //   face_records<COUNT> one triangle per lane: face tests, records counted and
 //                       staged; triangles over many bricks are listed
-//   large_faces<COUNT>  the listed triangles, 32 bricks per warp
+//   large_faces<COUNT>  the listed triangles' (triangle, brick) items, one per lane
 //   boundary_records<COUNT>, scan -> record offsets
+//   (the edges run on a second stream beside the scanline pass)
 // finish (no synchronisation):
-//   bucket_records      staged event and face records -> brick buckets (when
-//                       a staging buffer overflowed, the generators rerun in
-//                       FILL mode and write the records instead)
+//   bucket_records      staged event records -> brick buckets, a cursor per brick
+//   place_records       staged face records -> their ranks in the buckets
+//                       (when a staging buffer overflowed, the generators rerun
+//                       in FILL mode and write the records instead)
 //   boundary_records<FILL>
 //   brick_lists         one CTA per active brick: records -> per-voxel
-//                       contribution lists {key, payload} in global memory
-//                       (a counting sort by voxel; records are taken in bucket
-//                       order, close to key order, so lists come out nearly sorted)
-//   voxel_accumulate    one thread per voxel: insertion-sorts its list by key,
-//                       sums it sequentially in FP32 in that order (bit-identical
-//                       to the reference CPU sums), regularises, CPQR-solves
+//                       contribution lists {key, payload} (a counting sort by
+//                       voxel), staged and the short ones sorted in shared
+//                       memory when the brick's lists fit there
+//   voxel_accumulate    one thread per voxel: sorts its list by key unless it is
+//                       marked sorted, sums it sequentially in FP32 in that order
+//                       (bit-identical to the reference CPU sums), regularises,
+//                       CPQR-solves
 //   constrained_solve   box-constrained search for the few voxels whose
 //                       unconstrained solution leaves the voxel
 //
