@@ -218,6 +218,24 @@ def run_batched(dev, steps=3, warmup=2):
             "api": "o_voxel.convert.mesh_to_flexible_dual_grid_batch vs one mesh_to_flexible_dual_grid call per mesh"}
 
 
+# ----------------------------------------------------------------------------- ranks
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The largest of the ranks' times (every rank calls this, in the same
+    order); the tensor lives on `device` (CUDA under NCCL, CPU under gloo)."""
+    import torch
+
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(faces: int, world: int, ms_per_step: float) -> float:
+    """Whole-job Mfaces/s of `world` replicas, each converting `faces` faces per
+    step, timed by the slowest rank."""
+    return world * faces / (ms_per_step / 1e3) / 1e6
+
+
 # ----------------------------------------------------------------------------- our arm
 def run_ours(args, rank, world):
     import numpy as np
@@ -276,14 +294,11 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     launches = ctx.kernel_launches() - launches0
     clk = clocks.stop()
-    t_local = sum(ms)
-    t = torch.tensor([t_local], dtype=torch.float64, device=dev)
+    t_total = max_over_ranks(sum(ms), world, dev)
     if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
-    t_total = float(t.item())
     ms_per_step = t_total / args.steps
-    value = world * F / (ms_per_step / 1e3) / 1e6
+    value = replica_value(F, world, ms_per_step)
     if ctx.handle:
         ctx._check(abi.lib().ovx_fdg_sync_status(ctx.handle, abi.ctypes.c_void_p(stream.cuda_stream)), "status")
 
@@ -329,11 +344,8 @@ def run_ours(args, rank, world):
         return e0.elapsed_time(e1)
 
     e2e_run(2)
-    te = torch.tensor([e2e_run(args.steps)], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_ms = float(te.item()) / args.steps
-    e2e_value = world * F / (e2e_ms / 1e3) / 1e6
+    e2e_ms = max_over_ranks(e2e_run(args.steps), world, dev) / args.steps
+    e2e_value = replica_value(F, world, e2e_ms)
 
     if rank != 0:
         ctx.close()
