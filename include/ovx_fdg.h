@@ -2,7 +2,9 @@
  * ovx_fdg.h -- C ABI of the B200 mesh -> flexible dual grid library
  * (libovx_fdg.so).  Plain pointers and sizes; device pointers are CUDA device
  * memory on the context's device; `stream` is a cudaStream_t passed as void*
- * (NULL = legacy default stream).
+ * (NULL = legacy default stream).  Calls that take a context make its device
+ * current while they run and give the calling thread its previous current
+ * device back on return.
  *
  * The entry points replace the reference's CUDA operator for this path:
  *

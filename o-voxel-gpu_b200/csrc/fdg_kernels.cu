@@ -2687,6 +2687,25 @@ int fail(ovx_fdg_context *c, int status, const char *what)
     return status;
 }
 
+// Makes `device` current for the scope of a C ABI call and gives the calling
+// thread its previous device back on return.
+struct DeviceScope
+{
+    int prev = -1;
+    int dev;
+    cudaError_t status;
+    explicit DeviceScope(int device) : dev(device)
+    {
+        cudaGetDevice(&prev);
+        status = prev == device ? cudaSuccess : cudaSetDevice(device);
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0 && prev != dev)
+            cudaSetDevice(prev);
+    }
+};
+
 int cuda_fail(ovx_fdg_context *c, cudaError_t e, const char *where)
 {
     if (c)
@@ -3342,7 +3361,8 @@ int ovx_fdg_set_profiling(ovx_fdg_context *ctx, int enable)
 {
     if (!ctx)
         return OVX_FDG_INVALID_ARGUMENT;
-    OVX_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    OVX_CUDA(scope.status);
     if (enable)
         for (int i = 0; i < kStageEvents; ++i)
             if (!ctx->ev[i])
@@ -3465,7 +3485,8 @@ int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int
     int rc = check_grid(ctx, grid, g);
     if (rc != OVX_FDG_OK)
         return rc;
-    OVX_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    OVX_CUDA(scope.status);
     ctx->g = g;
     ctx->verts = vertices;
     ctx->nv = num_vertices;
@@ -3499,7 +3520,8 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     if (!voxel_indices || !dual_vertices || !intersected)
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "NULL output buffer");
     cudaStream_t st = (cudaStream_t)stream;
-    OVX_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    OVX_CUDA(scope.status);
     const long long nb = ctx->g.nbricks;
     OVX_CUDA(ensure(st, ctx, ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
     OVX_CUDA(ensure(st, ctx, ctx->btab, (size_t)(ctx->n_boundary + 1) * 40));
@@ -3589,7 +3611,8 @@ int ovx_fdg_sync_status(ovx_fdg_context *ctx, void *stream)
 {
     if (!ctx)
         return OVX_FDG_INVALID_ARGUMENT;
-    OVX_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    OVX_CUDA(scope.status);
     OVX_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     if (!ctx->finished)
         return OVX_FDG_OK;
@@ -3615,7 +3638,8 @@ int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *tri
     int rc = check_grid(ctx, grid, g);
     if (rc != OVX_FDG_OK)
         return rc;
-    OVX_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    OVX_CUDA(scope.status);
     ctx->g = g;
     ctx->verts = triangles;
     ctx->nv = num_triangles * 3;
@@ -3646,7 +3670,8 @@ int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_
     if (!voxel_indices)
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "NULL output buffer");
     cudaStream_t st = (cudaStream_t)stream;
-    OVX_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    OVX_CUDA(scope.status);
     const unsigned long long *base = (const unsigned long long *)ctx->bbase.p;
     if (ctx->order == 1)
     {

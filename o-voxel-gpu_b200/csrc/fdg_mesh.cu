@@ -247,6 +247,25 @@ __global__ void mesh_triangles(const uint4 *__restrict__ cand, const uint32_t *_
         t[k] = (int32_t)(order[k] == 4 ? mid : q[order[k]]);
 }
 
+// Makes `device` current for the scope of a C ABI call and gives the calling
+// thread its previous device back on return.
+struct DeviceScope
+{
+    int prev = -1;
+    int dev;
+    cudaError_t status;
+    explicit DeviceScope(int device) : dev(device)
+    {
+        cudaGetDevice(&prev);
+        status = prev == device ? cudaSuccess : cudaSetDevice(device);
+    }
+    ~DeviceScope()
+    {
+        if (prev >= 0 && prev != dev)
+            cudaSetDevice(prev);
+    }
+};
+
 struct Buf
 {
     void *p = nullptr;
@@ -342,7 +361,7 @@ void ovx_fdg_mesh_context_destroy(ovx_fdg_mesh_context *ctx)
 {
     if (!ctx)
         return;
-    cudaSetDevice(ctx->device);
+    const DeviceScope scope(ctx->device);
     for (Buf *b : {&ctx->keys, &ctx->vals, &ctx->cand, &ctx->valid, &ctx->qoff, &ctx->cub_tmp})
         if (b->p)
             cudaFree(b->p);
@@ -387,7 +406,8 @@ int ovx_fdg_to_mesh_begin(ovx_fdg_mesh_context *ctx, void *stream, const int32_t
     *num_vertices = 0;
     *num_triangles = 0;
     cudaStream_t st = (cudaStream_t)stream;
-    MESH_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    MESH_CUDA(scope.status);
     const long long n = num_voxels, ne = 3 * n;
     unsigned long long cap = 2;
     while (cap < 2ull * (unsigned long long)(n > 0 ? n : 1))
@@ -443,7 +463,8 @@ int ovx_fdg_to_mesh_finish(ovx_fdg_mesh_context *ctx, void *stream, float *verti
     if (!vertices || (L > 0 && !triangles))
         return mfail(ctx, OVX_FDG_INVALID_ARGUMENT, "NULL output buffer");
     cudaStream_t st = (cudaStream_t)stream;
-    MESH_CUDA(cudaSetDevice(ctx->device));
+    const DeviceScope scope(ctx->device);
+    MESH_CUDA(scope.status);
     mesh_vertices<<<blocks_for(3 * n, kThreads), kThreads, 0, st>>>(ctx->coords, ctx->dual, n, ctx->g, vertices);
     if (L > 0)
         mesh_triangles<<<blocks_for(ne, kThreads), kThreads, 0, st>>>((const uint4 *)ctx->cand.p, (const uint32_t *)ctx->valid.p,
