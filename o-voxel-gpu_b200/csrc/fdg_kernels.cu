@@ -2619,6 +2619,7 @@ struct ovx_fdg_context
     float origin[3] = {0, 0, 0};
     float fw = 0, bw = 0, rw = 0;
     long long n_vox = 0, n_active = 0, n_rec = 0, n_boundary = 0;
+    unsigned long long n_lunits = 0, n_funits = 0, n_blong = 0; // large-pair and large-face units, long boundary edges
     unsigned long long n_fstaged = 0, fstage_want = 0; // face records staged by the count pass (and the most seen)
     bool face_staged = false;                         // all of them fitted: the fill pass need not redo the tests
     unsigned long long n_estaged = 0, estage_want = 0; // the same for the scanline event records
@@ -2985,8 +2986,14 @@ void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
             unit_offsets<<<1, 1024, 0, st>>>(A.scan_units, A.scan_large_cap, A.counters, C_SCAN_LARGE, C_LUNITS);
             ++ctx->launches;
         }
-        large_rows<M, IdxT><<<ctx->sms * 8, kEventThreads, 0, st>>>(A);
-        ++ctx->launches;
+        // the fill pass knows the units (32 a warp); the count pass does not yet
+        const long long rows_grid = M == FILL ? std::min<long long>(ctx->sms * 8, blocks_for((long long)ctx->n_lunits, kEventThreads))
+                                              : ctx->sms * 8;
+        if (rows_grid > 0)
+        {
+            large_rows<M, IdxT><<<(unsigned)rows_grid, kEventThreads, 0, st>>>(A);
+            ++ctx->launches;
+        }
     }
 }
 
@@ -3021,8 +3028,13 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
                 unit_offsets<<<1, 1024, 0, st>>>(A.face_units, A.face_large_cap, A.counters, C_FACE_LARGE, C_FUNITS);
                 ++ctx->launches;
             }
-            large_faces<M, IdxT><<<ctx->sms * 7, kFaceThreads, 0, st>>>(A);
-            ++ctx->launches;
+            const long long faces_grid =
+                M == FILL ? std::min<long long>(ctx->sms * 7, blocks_for((long long)ctx->n_funits, kFaceThreads)) : ctx->sms * 7;
+            if (faces_grid > 0)
+            {
+                large_faces<M, IdxT><<<(unsigned)faces_grid, kFaceThreads, 0, st>>>(A);
+                ++ctx->launches;
+            }
         }
         if (M == COUNT && A.fstage)
         {
@@ -3034,9 +3046,21 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
     }
     if (ctx->bw > 0.0f && ctx->nf > 0)
     {
-        boundary_records<M><<<ctx->sms * 8, kThreads, 0, st>>>(A);
-        boundary_long<M><<<ctx->sms * 4, kThreads, 0, st>>>(A);
-        ctx->launches += 2;
+        // at most 3F boundary edges; the fill pass knows the counts
+        const long long nb_edges = M == FILL ? ctx->n_boundary : 3 * ctx->nf;
+        const long long rec_grid = std::min<long long>(ctx->sms * 8, blocks_for(nb_edges, kThreads));
+        if (rec_grid > 0)
+        {
+            boundary_records<M><<<(unsigned)rec_grid, kThreads, 0, st>>>(A);
+            ++ctx->launches;
+        }
+        const long long nb_long = M == FILL ? (long long)ctx->n_blong : 3 * ctx->nf;
+        const long long long_grid = std::min<long long>(ctx->sms * 4, blocks_for(nb_long, kThreads / 32));
+        if (long_grid > 0)
+        {
+            boundary_long<M><<<(unsigned)long_grid, kThreads, 0, st>>>(A);
+            ++ctx->launches;
+        }
     }
 }
 
@@ -3195,6 +3219,9 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     ctx->n_active = (long long)ctx->host[1];
     ctx->n_rec = full ? (long long)ctx->host[2] : 0;
     ctx->n_boundary = hc[C_BOUNDARY];
+    ctx->n_lunits = hc[C_LUNITS];
+    ctx->n_funits = hc[C_FUNITS];
+    ctx->n_blong = hc[C_BLONG];
     ctx->n_estaged = full ? hc[C_ESTAGED] : 0u;
     ctx->event_staged = full && ctx->n_estaged <= (unsigned long long)cap_u32(ctx->estage, sizeof(uint4));
     ctx->estage_want = std::max(ctx->estage_want, ctx->n_estaged);
@@ -3584,13 +3611,14 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     }
     stage(ctx, EV_CONSUME, st);
     voxel_accumulate<<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
-    voxel_accumulate_long<kLongMidMax, 128, false><<<ctx->sms * 8, 128, long_smem<kLongMidMax>(), st>>>(SA);
+    // one CTA per long list, at most one per row
+    voxel_accumulate_long<kLongMidMax, 128, false><<<(unsigned)std::min<long long>(ctx->sms * 8, n), 128, long_smem<kLongMidMax>(), st>>>(SA);
     OVX_CUDA(cudaFuncSetAttribute(voxel_accumulate_long<kLongHugeMax, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)long_smem<kLongHugeMax>()));
-    voxel_accumulate_long<kLongHugeMax, 256, true><<<ctx->sms * 2, 256, long_smem<kLongHugeMax>(), st>>>(SA);
+    voxel_accumulate_long<kLongHugeMax, 256, true><<<(unsigned)std::min<long long>(ctx->sms * 2, n), 256, long_smem<kLongHugeMax>(), st>>>(SA);
     ctx->launches += 3;
     stage(ctx, EV_SOLVE, st);
-    constrained_solve<<<ctx->sms * 8, 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
+    constrained_solve<<<(unsigned)std::min<long long>(ctx->sms * 8, blocks_for(n, 128)), 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
                                                     ctx->g, dual_vertices);
     ++ctx->launches;
     stage(ctx, EV_CONSTRAINED, st);
