@@ -2893,6 +2893,8 @@ struct Readback
     int n;
     void add(const void *p, int nbytes, int word)
     {
+        if (n >= 4)
+            return; // the callers add at most four
         src[n] = p;
         bytes[n] = nbytes;
         dst[n] = word;
