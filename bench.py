@@ -1,7 +1,7 @@
 """Benchmark: mesh -> flexible dual grid on B200.
 
 One step = one full conversion (occupancy, quadrics, solve) of the seeded
-280k-face / grid-512 primitives mesh (the reference's headline single-mesh
+282k-face / grid-512 primitives mesh (the reference's headline single-mesh
 case; its asset is not distributed, so a synthetic stand-in with the same
 size is used).  Prints one JSON line on rank 0.
 
@@ -11,11 +11,23 @@ size is used).  Prints one JSON line on rank 0.
              with pinned host inputs: H2D copy, conversion, D2H of all outputs
   roofline   compulsory bytes of a conversion (12V + 8*3F + 27N) over the
              conversion time against the measured HBM copy bandwidth
-  cpu_baseline  the reference's CPU implementation on the host cores
+  workloads  the 10.3M-face subdivided mesh at grid 512, timed the same way,
+             with its own roofline and memory
+  reference_gpu  the reference's own CUDA implementation of the path (built
+             from its sources into baseline/_ref by baseline/build_ref_gpu.py),
+             timed on the same GPU, same inputs, same method, on both meshes
+  cpu_baseline  the reference's CPU implementation on the host cores: every
+             core converts the full 282k-face mesh once
   batched    256 mixed meshes (grids 64-512): the batched API against one
              call per mesh, meshes/s of each (single GPU only)
 
---impl reference times the reference CPU implementation alone.
+--impl reference times the reference CPU implementation alone, on the same
+mesh: one step = every host core converts the full mesh once.
+
+--workload NAME [--grid G] [--stages] runs one synthetic workload a few times
+through the C ABI and prints its own JSON line (per-workload timings; the
+command the ncu captures under profiles/ name).
+
 Multi-GPU: replicas only (each rank converts its own copy; no collective).
 """
 import argparse
@@ -33,14 +45,33 @@ sys.path.insert(0, os.path.join(REPO, "o-voxel-gpu_b200"))
 sys.path.insert(0, REPO)
 
 METRIC = "Mfaces/s & meshes/s mesh→FDG @grid512, batched vs plain GPU, exact occ"
-PUBLISHED_MFACES = 10.3  # reference CUDA path, RTX 4090, 280k faces, grid 512 (derived in BASELINE.md)
-CPU_SAMPLE_FACES = 48_000
+# reference CUDA path as published: 280k faces at grid 512 in 27.1 ms on an RTX 4090 (README.md:39)
+PUBLISHED_MFACES = 10.3
+HEADLINE = "primitives-282k-faces-grid512"
+LARGE = "subdivided-10.3M-faces-grid512"
+CPU_BUDGET_S = 150.0  # timed CPU reference steps stop once this much time has gone
 
 
-def load_workload():
+def load_workload(name=HEADLINE):
     import fdg_workloads as W
 
-    return W.primitives(1)
+    if name == HEADLINE:
+        return W.primitives(1)
+    if name == LARGE:
+        return W.subdivided(1, grid_size=512)
+    raise ValueError(name)
+
+
+def grid_args(w):
+    """The reference wrapper's derivation for the grid_size + aabb form
+    (o_voxel/convert/flexible_dual_grid.py:161-178): float32 voxel size
+    (aabb1 - aabb0) / grid, grid_range [0, 0, 0, g...], origin aabb0."""
+    import numpy as np
+
+    ab = np.asarray(w.aabb, dtype=np.float32).reshape(2, 3)
+    g = np.broadcast_to(np.asarray(w.grid_size, dtype=np.int32), (3,))
+    vs = ((ab[1] - ab[0]) / g.astype(np.float32)).astype(np.float32)
+    return ab[0], vs, [0, 0, 0, int(g[0]), int(g[1]), int(g[2])]
 
 
 def peaks():
@@ -52,9 +83,15 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def algorithmic_bytes(V, F, N, face_bytes=8):
+    """Compulsory I/O of one conversion: vertices in, faces in, voxels, dual
+    vertices and flags out (12V + 3F x face index bytes + 27N)."""
+    return 12 * V + face_bytes * 3 * F + 27 * N
+
+
 # ----------------------------------------------------------------------------- CPU baseline
 def _ref_worker(args):
-    """Runs in a spawned process: one conversion of the sample by the reference CPU code."""
+    """Runs in a spawned process: one conversion of the mesh by the reference CPU code."""
     kind, v, f, vs, gr, fw, bw, rw = args
     sys.path.insert(0, REPO)
     from oracle import oracle as O
@@ -68,33 +105,41 @@ def _ref_worker(args):
 
 
 class CpuBaseline:
-    """The reference CPU implementation on all host cores: one conversion of a
-    bounded face sample per core per step (the reference CPU path is single-threaded)."""
+    """The reference CPU implementation on all host cores.  The reference CPU
+    path is single-threaded (flexible_dual_grid.cpp:660-992), so a step runs
+    one full conversion of the mesh on every core at once: the step's wall
+    time gives the throughput of the whole host, each process's own time the
+    latency of one conversion."""
 
-    def __init__(self, w, sample_faces=CPU_SAMPLE_FACES, cores=None):
+    def __init__(self, w, cores=None):
         from oracle import oracle as O
 
         self.kind = "reference" if O.ref_module() is not None else "port"
         v, f, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
-        self.faces = min(sample_faces, f.shape[0])
+        self.faces = int(f.shape[0])
         self.cores = cores or os.cpu_count() or 1
-        self.job = (self.kind, v, f[: self.faces], vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+        self.job = (self.kind, v, f, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
         self.pool = mp.get_context("spawn").Pool(self.cores)
-        self.pool.map(_ref_worker, [self.job] * self.cores)  # warm the workers
+        self.latencies = []
 
     def step(self):
         t0 = time.perf_counter()
-        self.pool.map(_ref_worker, [self.job] * self.cores)
-        return time.perf_counter() - t0
+        lat = self.pool.map(_ref_worker, [self.job] * self.cores)
+        wall = time.perf_counter() - t0
+        self.latencies.extend(lat)
+        return wall
 
     def close(self):
         self.pool.close()
         self.pool.join()
 
     def describe(self, value):
+        src = ("reference src/convert/flexible_dual_grid.cpp built against the Eigen-API shim" if self.kind == "reference"
+               else "C restatement of it")
         return {"value": value, "unit": "Mfaces/s", "cores": self.cores, "kind": self.kind,
-                "sample": f"first {self.faces} faces of the 282k-face grid-512 mesh, one conversion per core per step "
-                          f"({'reference src/convert/flexible_dual_grid.cpp built against the Eigen-API shim' if self.kind == 'reference' else 'C restatement of it'})"}
+                "latency_ms": 1e3 * statistics.median(self.latencies) if self.latencies else None,
+                "latency_note": "one single-threaded conversion of the full mesh, median over the processes of the timed steps",
+                "sample": f"the full {self.faces}-face grid-512 mesh, one conversion per core per step, {self.cores} cores ({src})"}
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -146,20 +191,32 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- reference arm
 def run_reference(args, rank):
+    """The reference CPU implementation alone, on the headline mesh.  A step
+    converts the full mesh once on every host core; the first step warms the
+    processes.  A CPU step takes tens of seconds, so the timed steps stop after
+    CPU_BUDGET_S (at least two), and the line reports the steps that ran."""
     if rank != 0:
         return
     w = load_workload()
     cb = CpuBaseline(w)
-    for _ in range(args.warmup):
+    warm = min(args.warmup, 1)
+    for _ in range(warm):
         cb.step()
-    times = [cb.step() for _ in range(args.steps)]
+    cb.latencies.clear()
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < args.steps and (len(times) < 2 or time.perf_counter() - t_start < CPU_BUDGET_S):
+        times.append(cb.step())
     cb.close()
     t = sum(times) / len(times)
     value = cb.cores * cb.faces / t / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mfaces/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64,f32", "data": "synthetic (seeded primitives mesh)",
-            "config": {"workload": "primitives-282k-faces-grid512", "grid": 512, "faces": int(w.num_faces)},
+            "steps": len(times), "warmup": warm, "steps_requested": args.steps, "warmup_requested": args.warmup,
+            "steps_note": f"a step converts the full mesh on every core ({t:.1f} s); timed steps stop after {CPU_BUDGET_S:.0f} s "
+                          f"(at least two) and one warm-up step is run, so that the run ends within minutes",
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64,f32",
+            "data": "synthetic: seeded 48-primitive mesh (no dataset on the box)",
+            "config": {"workload": HEADLINE, "faces": int(w.num_faces), "vertices": int(w.vertices.shape[0]), "grid": 512},
             "cpu_baseline": cb.describe(value),
             "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -169,7 +226,7 @@ def run_reference(args, rank):
 BATCH_WORKERS = 8
 
 
-def run_batched(dev, steps=3, warmup=2):
+def run_batched(dev, steps=10, warmup=2):
     """256 seeded meshes built like the 282k-face one, face counts log-uniform in
     [1k, 500k] (about 21M faces in all), grid 64/128/256/512 per mesh, per-mesh
     aabb: the batched API against the same meshes converted one call at a time."""
@@ -193,7 +250,7 @@ def run_batched(dev, steps=3, warmup=2):
         o_voxel.convert.mesh_to_flexible_dual_grid_batch(meshes, grid_size=grids, aabb=aabbs, workers=BATCH_WORKERS, **kw)
 
     def timed(fn):
-        # the workers' contexts reach their largest workspaces during the warm-up
+        # the contexts reach their largest workspaces during the warm-up
         for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
@@ -211,9 +268,12 @@ def run_batched(dev, steps=3, warmup=2):
     t_batch, batch_ms = timed(batched)
     return {"workload": "256 meshes, faces log-uniform 1k-500k, grids 64-512, per-mesh aabb",
             "meshes": len(ws), "faces": int(F), "workers": BATCH_WORKERS, "steps": steps, "warmup": warmup,
-            "timing": "median of the steps", "plain_step_ms": plain_ms, "batched_step_ms": batch_ms,
-            "plain_ms": t_plain, "plain_meshes_per_s": len(ws) / (t_plain / 1e3),
-            "batched_ms": t_batch, "batched_meshes_per_s": len(ws) / (t_batch / 1e3),
+            "timing": "median of the steps (CUDA events on the caller's stream, host included)",
+            "plain_step_ms": plain_ms, "batched_step_ms": batch_ms,
+            "plain_ms": t_plain, "plain_spread_ms": [min(plain_ms), max(plain_ms)],
+            "plain_meshes_per_s": len(ws) / (t_plain / 1e3),
+            "batched_ms": t_batch, "batched_spread_ms": [min(batch_ms), max(batch_ms)],
+            "batched_meshes_per_s": len(ws) / (t_batch / 1e3),
             "batched_mfaces_per_s": F / (t_batch / 1e3) / 1e6, "speedup": t_plain / t_batch,
             "api": "o_voxel.convert.mesh_to_flexible_dual_grid_batch vs one mesh_to_flexible_dual_grid call per mesh"}
 
@@ -236,21 +296,157 @@ def replica_value(faces: int, world: int, ms_per_step: float) -> float:
     return world * faces / (ms_per_step / 1e3) / 1e6
 
 
+# ----------------------------------------------------------------------------- timing helpers
+def time_steps(fn, steps, stream, flush):
+    """Per-step device times (ms) of fn() with CUDA events on `stream`, the L2
+    flushed (a 256 MB write) before every step, outside the events."""
+    import torch
+
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def canonical(vox, dual, inter):
+    """Rows sorted by voxel coordinate (x slowest), for comparing outputs of different row orders."""
+    import torch
+
+    v = vox.long()
+    key = (v[:, 0] << 42) | (v[:, 1] << 21) | v[:, 2]
+    o = torch.argsort(key)
+    return vox[o], dual[o], inter[o]
+
+
+def compare_outputs(got, want, voxel_size):
+    """Parity of one conversion's outputs against another's: occupancy set,
+    flag mismatches, dual-vertex differences in voxel edges."""
+    import torch
+
+    gv, gd, gi = canonical(*got)
+    wv, wd, wi = canonical(*want)
+    if gv.shape != wv.shape or not torch.equal(gv, wv):
+        return {"occupancy_equal": False, "voxels": [int(gv.shape[0]), int(wv.shape[0])]}
+    vs = torch.tensor(voxel_size, dtype=torch.float64, device=gd.device)
+    d = (gd.double() - wd.double()) / vs
+    err = d.norm(dim=1)
+    return {"occupancy_equal": True, "flag_mismatches": int((gi != wi).sum().item()),
+            "dual_rms_voxel": float(err.square().mean().sqrt().item()), "dual_max_voxel": float(err.max().item()),
+            "dual_bit_identical_rows": float((gd.view(torch.int32) == wd.view(torch.int32)).all(1).float().mean().item())}
+
+
+class RefGpu:
+    """The reference's own CUDA implementation (baseline/_ref), called the way
+    its wrapper calls it: vertices already shifted by aabb[0] and int32 faces
+    (flexible_dual_grid.py:89-90,181,184); those input passes are done once,
+    outside the timed region."""
+
+    def __init__(self):
+        sys.path.insert(0, os.path.join(REPO, "baseline"))
+        import build_ref_gpu
+
+        self.mod = build_ref_gpu.load()
+
+    def available(self):
+        return self.mod is not None
+
+    def prepare(self, w, dev):
+        import numpy as np
+        import torch
+
+        origin, vs, gr = grid_args(w)
+        v = (torch.from_numpy(w.vertices).to(dev) - torch.from_numpy(np.asarray(origin)).to(dev)).contiguous()
+        f = torch.from_numpy(w.faces).to(dev).int().contiguous()
+        args = (v, f, [float(x) for x in vs], gr, float(w.face_weight), float(w.boundary_weight),
+                float(w.regularization_weight))
+        return lambda: self.mod.mesh_to_flexible_dual_grid_cuda(*args)
+
+
 # ----------------------------------------------------------------------------- our arm
+def measure_workload(name, w, dev, stream, flush, steps, ref_gpu=None, ours_out=None):
+    """Device-resident timing of one workload through a fresh C-ABI context
+    (cold first call, then warm steps), its roofline and memory; and, when
+    given, the reference's CUDA path on the same inputs."""
+    import torch
+
+    import ovx_fdg_abi as abi
+
+    F, V = w.num_faces, w.vertices.shape[0]
+    origin, vs, gr = grid_args(w)
+    vd = torch.from_numpy(w.vertices).to(dev)
+    fd = torch.from_numpy(w.faces).to(dev)
+    ctx = abi.Context(dev.index)
+    kw = (origin, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+    one = lambda: ctx.mesh_to_fdg(vd, fd, *kw, check=False)  # noqa: E731
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    out = one()
+    c1.record(stream)
+    c1.synchronize()
+    cold = c0.elapsed_time(c1)
+    for _ in range(3):
+        out = one()
+    ms = time_steps(one, steps, stream, flush)
+    ctx._check(abi.lib().ovx_fdg_sync_status(ctx.handle, abi.ctypes.c_void_p(stream.cuda_stream)), "status")
+    N = int(out[0].shape[0])
+    t = statistics.median(ms)
+    peak, peak_kind = peaks()
+    b_alg = algorithmic_bytes(V, F, N)
+    res = {"faces": F, "vertices": V, "voxels": N, "grid": int(gr[3]), "steps": steps, "ms": t,
+           "ms_spread": [min(ms), max(ms)], "mfaces_per_s": F / (t / 1e3) / 1e6, "cold_ms": cold,
+           "roofline": {"bound": "hbm", "algorithmic_bytes": b_alg, "achieved": b_alg / (t / 1e3) / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": b_alg / (t / 1e3) / 1e9 / peak, "peak_source": peak_kind},
+           "memory": {"workspace_bytes": int(ctx.workspace_bytes()), "output_bytes": 27 * N,
+                      "note": "the library's workspace after this workload on a fresh context, plus the outputs"}}
+    if ours_out is not None:
+        ours_out.append(out)
+    if ref_gpu is not None and ref_gpu.available():
+        fn = ref_gpu.prepare(w, dev)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats(dev)
+        base = torch.cuda.memory_allocated(dev)
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        rout = fn()
+        r1.record(stream)
+        r1.synchronize()
+        rcold = r0.elapsed_time(r1)
+        rpeak = torch.cuda.max_memory_allocated(dev) - base
+        for _ in range(3):
+            rout = fn()
+        rms = time_steps(fn, steps, stream, flush)
+        rt = statistics.median(rms)
+        res["reference_gpu"] = {
+            "ms": rt, "ms_spread": [min(rms), max(rms)], "mfaces_per_s": F / (rt / 1e3) / 1e6, "cold_ms": rcold,
+            "peak_allocated_bytes": int(rpeak), "speedup_of_this_library": rt / t,
+            "parity_vs_this_library": compare_outputs(rout, out, vs),
+            "note": "reference CUDA path (src/convert/mesh_to_flexible_dual_grid_gpu, sm_100 build) through its operator; "
+                    "parity is informational (its arithmetic deviates from its CPU path in known places)"}
+        del rout
+    ctx.close()
+    return res
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
 
     import ovx_fdg_abi as abi
     import o_voxel
-    from oracle import oracle as O
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     w = load_workload()
     F, V = w.num_faces, w.vertices.shape[0]
-    v_np, f_np, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
-    origin = np.asarray(w.aabb, np.float32)[0]
+    origin, vs, gr = grid_args(w)
     vd = torch.from_numpy(w.vertices).to(dev)
     fd = torch.from_numpy(w.faces).to(dev)  # int64, consumed as supplied
     ctx = abi.Context(dev.index)
@@ -281,16 +477,7 @@ def run_ours(args, rank, world):
     clocks = ClockSampler(dev.index)
     clocks.start()
     launches0 = ctx.kernel_launches()
-    ms = []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        out = one()
-        e1.record(stream)
-        e1.synchronize()
-        ms.append(e0.elapsed_time(e1))
+    ms = time_steps(one, args.steps, stream, flush)
     torch.cuda.synchronize()
     launches = ctx.kernel_launches() - launches0
     clk = clocks.stop()
@@ -299,8 +486,7 @@ def run_ours(args, rank, world):
         torch.distributed.barrier()
     ms_per_step = t_total / args.steps
     value = replica_value(F, world, ms_per_step)
-    if ctx.handle:
-        ctx._check(abi.lib().ovx_fdg_sync_status(ctx.handle, abi.ctypes.c_void_p(stream.cuda_stream)), "status")
+    ctx._check(abi.lib().ovx_fdg_sync_status(ctx.handle, abi.ctypes.c_void_p(stream.cuda_stream)), "status")
 
     # stage breakdown (separate, profiled conversion)
     ctx.set_profiling(True)
@@ -351,7 +537,7 @@ def run_ours(args, rank, world):
         ctx.close()
         return
     peak, peak_kind = peaks()
-    b_alg = 12 * V + 8 * 3 * F + 27 * N
+    b_alg = algorithmic_bytes(V, F, N)
     achieved = b_alg / (ms_per_step / 1e3) / 1e9
     traffic = None
     tf = os.path.join(REPO, "profiles", "fdg_traffic.json")
@@ -360,10 +546,36 @@ def run_ours(args, rank, world):
             traffic = json.load(fh_).get("dram_bytes_per_conversion")
     total_stage = sum(x for x in stages.values() if x > 0) or 1.0
     dom = max(stages.items(), key=lambda kv: kv[1]) if stages else ("", 0.0)
+    workspace = int(ctx.workspace_bytes())
+    ctx.close()
+    del out
+
+    # the other workloads and the reference's CUDA path, single GPU only
+    workloads, reference_gpu = {}, None
+    if world == 1 and not args.no_reference_gpu:
+        ref = RefGpu()
+        reference_gpu = {"available": ref.available()}
+        if not ref.available():
+            reference_gpu["why"] = "baseline/_ref not built (baseline/build_ref_gpu.py needs the reference source tree)"
+        else:
+            reference_gpu["build"] = "reference src/convert/mesh_to_flexible_dual_grid_gpu/*.cu, nvcc -O3 sm_100"
+    else:
+        ref = None
+    head = measure_workload(HEADLINE, w, dev, stream, flush, args.steps, ref_gpu=ref)
+    if ref is not None and "reference_gpu" in head:
+        reference_gpu[HEADLINE] = head["reference_gpu"]
+    if world == 1 and not args.no_large:
+        wl = load_workload(LARGE)
+        workloads[LARGE] = measure_workload(LARGE, wl, dev, stream, flush, max(3, min(args.steps, 10)), ref_gpu=ref)
+        if ref is not None and "reference_gpu" in workloads[LARGE]:
+            reference_gpu[LARGE] = workloads[LARGE].pop("reference_gpu")
+        del wl
+        torch.cuda.empty_cache()
+
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cb = CpuBaseline(w)
-        cpu_t = statistics.median([cb.step() for _ in range(2)])
+        cpu_t = cb.step()
         cb.close()
         cpu = cb.describe(cb.cores * cb.faces / cpu_t / 1e6)
     batched = None
@@ -374,7 +586,7 @@ def run_ours(args, rank, world):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED_MFACES, "dtype": "f64,f32",
         "data": "synthetic: seeded 48-primitive mesh (no dataset on the box)",
-        "config": {"workload": "primitives-282k-faces-grid512", "faces": F, "vertices": V, "voxels": N, "grid": 512,
+        "config": {"workload": HEADLINE, "faces": F, "vertices": V, "voxels": N, "grid": 512,
                    "weights": [w.face_weight, w.boundary_weight, w.regularization_weight], "faces_dtype": "int64",
                    "l2": "flushed between steps (256 MB write outside the timed events)", "parallelism": f"replicas x{world}"},
         "meshes_per_s": world / (ms_per_step / 1e3),
@@ -388,15 +600,69 @@ def run_ours(args, rank, world):
                      "dominant_stage": {"name": dom[0], "ms": dom[1], "share": dom[1] / total_stage}},
         "stage_ms": stages,
         "cold_ms": cold_ms,
-        "memory": {"workspace_bytes": int(ctx.workspace_bytes()), "torch_max_allocated_bytes": int(torch.cuda.max_memory_allocated(dev)),
+        "memory": {"workspace_bytes": workspace, "torch_max_allocated_bytes": int(torch.cuda.max_memory_allocated(dev)),
                    "note": "workspace: the conversion context's buffers (grown to the largest conversion); torch: outputs, inputs, "
-                           "the 256 MB L2 flush buffer and the batched leg"},
+                           "the 256 MB L2 flush buffer, the reference's CUDA path and the batched leg"},
+        "workloads": {HEADLINE: {k: v for k, v in head.items() if k != "reference_gpu"}, **workloads},
+        "reference_gpu": reference_gpu,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": int(launches),
     }
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- one workload
+def make_workload(name: str, grid: int = 0):
+    import fdg_workloads as W
+
+    if name == "ico_cap":
+        return W.ico_cap(0)
+    if name == "primitives":
+        return W.primitives(1)
+    if name == "subdivided":
+        return W.subdivided(1, grid_size=grid or 512)
+    if name == "sheets":
+        return W.sheets(3)
+    if name == "lowpoly":
+        return W.lowpoly(5, grid_size=grid or 512)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def run_one_workload(args):
+    """Runs one synthetic workload through the C ABI `--conversions` times and
+    prints its timings (ms per conversion, CUDA events), sizes and, with
+    --stages, the stage times of one more conversion."""
+    import torch
+
+    import ovx_fdg_abi as abi
+
+    w = make_workload(args.workload, args.grid)
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    origin, vs, gr = grid_args(w)
+    v = torch.from_numpy(w.vertices).to(dev)
+    f = torch.from_numpy(w.faces).to(dev)
+    ctx = abi.Context(0)
+    times, n = [], 0
+    for _ in range(max(1, args.conversions)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        vox, _, _ = ctx.mesh_to_fdg(v, f, origin, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        n = vox.shape[0]
+    out = {"workload": w.name, "faces": int(w.num_faces), "vertices": int(w.vertices.shape[0]),
+           "grid": int(gr[3]), "voxels": int(n), "ms": times,
+           "launches_per_conversion": ctx.kernel_launches() // max(1, args.conversions),
+           "workspace_bytes": ctx.workspace_bytes(), "counts": ctx.last_counts()}
+    if args.stages:
+        ctx.set_profiling(True)
+        ctx.mesh_to_fdg(v, f, origin, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+        out["stage_ms"] = ctx.stage_times()
     ctx.close()
+    print(json.dumps(out))
 
 
 def main():
@@ -407,7 +673,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-mesh batched measurement")
+    ap.add_argument("--no-large", action="store_true", help="skip the 10.3M-face workload")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference's CUDA path")
+    ap.add_argument("--workload", default=None, help="run one workload and print its timings instead (ico_cap, primitives, "
+                                                     "subdivided, sheets, lowpoly)")
+    ap.add_argument("--grid", type=int, default=0, help="grid size for --workload subdivided / lowpoly")
+    ap.add_argument("--conversions", type=int, default=3, help="conversions for --workload")
+    ap.add_argument("--stages", action="store_true", help="stage times for --workload")
     args = ap.parse_args()
+    if args.workload:
+        run_one_workload(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -225,10 +225,16 @@ int ovx_fdg_to_mesh_finish(ovx_fdg_mesh_context *ctx, void *stream, float *verti
  * calling thread's current device; voxel_indices has room for `capacity` rows.
  * *num_voxels receives N; if N > capacity nothing is written and
  * OVX_FDG_CAPACITY is returned.  The call waits once on `stream` (to read N)
- * and returns with the coordinate kernel enqueued on it.  The first call on a
- * device looks up the scratch address there (it should come before any stream
- * capture).  All calls on a device share the scratch array, so calls that
- * overlap on the GPU (different streams or threads) race; serialise them.
+ * and returns with the coordinate kernel enqueued on it; because of that wait
+ * it cannot run while `stream` is being captured into a CUDA graph, and
+ * returns OVX_FDG_INVALID_ARGUMENT without doing anything in that case.  Every
+ * call looks up the scratch array's address on the current device (so a
+ * cudaDeviceReset between calls is harmless).  All calls on a device share the
+ * scratch array, so calls that overlap on the GPU (different streams or
+ * threads) race; serialise them.  Each (triangle, axis) pair is scanned by one
+ * thread, so a mesh of a few large triangles on a fine grid runs serially
+ * inside those threads: the allocating entry points spread such work over
+ * whole warps and are the faster choice for low-poly meshes.
  */
 int ovx_fdg_occupancy_noalloc(void *stream, const float *triangles, int64_t num_triangles, const ovx_fdg_grid *grid,
                               int32_t *voxel_indices, int64_t capacity, int64_t *num_voxels);

@@ -73,7 +73,6 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
-#include <mutex>
 #include <cstring>
 #include <string>
 
@@ -2884,17 +2883,25 @@ __global__ void copy_word(const uint32_t *__restrict__ src, uint32_t *__restrict
     *dst = *src;
 }
 
-// Up to four device words/blocks to copy into the mapped readback words.
+// Up to kReadbackMax device words/blocks to copy into the mapped readback
+// words.  Adding more sets `overflow`, which the caller turns into an
+// OVX_FDG_INTERNAL error before launching (a dropped entry would leave a stale
+// host word to be read as a count).
+constexpr int kReadbackMax = 4;
 struct Readback
 {
-    const void *src[4];
-    int bytes[4]; // multiples of 4
-    int dst[4];   // index of the first 8-byte host word
+    const void *src[kReadbackMax];
+    int bytes[kReadbackMax]; // multiples of 4
+    int dst[kReadbackMax];   // index of the first 8-byte host word
     int n;
+    bool overflow;
     void add(const void *p, int nbytes, int word)
     {
-        if (n >= 4)
-            return; // the callers add at most four
+        if (n >= kReadbackMax)
+        {
+            overflow = true;
+            return;
+        }
         src[n] = p;
         bytes[n] = nbytes;
         dst[n] = word;
@@ -3205,6 +3212,8 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         if (full)
             r.add((unsigned long long *)ctx->roff.p + nb, 8, 2);
         r.add(ctx->counters.p, C_WORDS * 4, kHostCounters);
+        if (r.overflow)
+            return fail(ctx, OVX_FDG_INTERNAL, "readback list overflow");
         readback<<<1, 32, 0, st>>>(r, ctx->host_dev);
         ++ctx->launches;
     }
@@ -3628,6 +3637,8 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     {
         Readback r{};
         r.add(ctx->counters.p, C_WORDS * 4, kHostFinish);
+        if (r.overflow)
+            return fail(ctx, OVX_FDG_INTERNAL, "readback list overflow");
         readback<<<1, 32, 0, st>>>(r, ctx->host_dev);
         ++ctx->launches;
     }
@@ -3725,26 +3736,18 @@ int ovx_fdg_occupancy_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_
 // ---------------------------------------------------------------------------
 namespace
 {
-constexpr int kNoallocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[kNoallocMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up once per
-// device (the name itself is a host-side stand-in, not a device address).
-cudaError_t noalloc_scratch(int device, void **out)
+// Device address of the scratch array on the current device (the name itself
+// is a host-side stand-in, not a device address).  Looked up on every call: the
+// lookup is cheap, and a cached address would go stale if the caller reset the
+// device (cudaDeviceReset reloads the module, which can place the array
+// elsewhere).
+cudaError_t noalloc_scratch(void **out)
 {
-    if (device < 0 || device >= kNoallocMaxDevices)
-        return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[device])
-    {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            return e;
-        g_noalloc_ptr[device] = p;
-    }
-    *out = g_noalloc_ptr[device];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return e;
+    *out = p;
     return cudaSuccess;
 }
 } // namespace
@@ -3779,21 +3782,24 @@ extern "C" int ovx_fdg_occupancy_noalloc(void *stream, const float *triangles, i
     if (nb > kNoallocMaxBricks)
         return OVX_FDG_CAPACITY; // grid larger than the fixed scratch covers
     g.nbricks = nb;
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess)
+    cudaStream_t st = (cudaStream_t)stream;
+    // the call waits on the stream once (to read N), which a stream capture forbids
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess)
     {
         cudaGetLastError();
         return OVX_FDG_CUDA_ERROR;
     }
+    if (cap != cudaStreamCaptureStatusNone)
+        return OVX_FDG_INVALID_ARGUMENT;
     void *scratch = nullptr;
-    if (noalloc_scratch(device, &scratch) != cudaSuccess)
+    if (noalloc_scratch(&scratch) != cudaSuccess)
     {
         cudaGetLastError();
         return OVX_FDG_CUDA_ERROR;
     }
     uint32_t *bits = (uint32_t *)scratch;
     uint32_t *base = (uint32_t *)((unsigned char *)scratch + kNoallocBitsBytes);
-    cudaStream_t st = (cudaStream_t)stream;
     noalloc_clear<<<256, 256, 0, st>>>(bits, nb * kWordsPerBrick);
     if (num_triangles > 0)
         noalloc_mark<<<blocks_for(3 * num_triangles, kThreads), kThreads, 0, st>>>(triangles, num_triangles, g, bits);

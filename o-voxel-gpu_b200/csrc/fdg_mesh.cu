@@ -5,8 +5,8 @@
 // (o_voxel/convert/flexible_dual_grid.py:332-477):
 //   * active voxels are found by their flat key x*gy*gz + y*gz + z in a hash
 //     table, as the reference's hashmap does (src/hash/hash.cu:366-420,
-//     269-330); a neighbour one past the grid's last z or y therefore finds
-//     the voxel its key aliases, exactly as there;
+//     269-300); a neighbour outside [0, grid) on any axis is not looked up and
+//     counts as absent, as in the reference's lookup kernel (hash.cu:283-286);
 //   * every intersected edge (voxel, axis) whose four surrounding voxels are
 //     all active gives one quad, in (voxel, axis) order;
 //   * quads are split into two triangles by the larger normal alignment, or
@@ -128,7 +128,9 @@ __global__ void mesh_quads(const int32_t *__restrict__ coords, const uint8_t *__
 #pragma unroll
         for (int k = 0; k < 4; ++k)
         {
-            q[k] = mesh_hash_find(keys, vals, mask, flat_key(g, x + kEdgeNbr[a][k][0], y + kEdgeNbr[a][k][1], z + kEdgeNbr[a][k][2]));
+            const long long nx = x + kEdgeNbr[a][k][0], ny = y + kEdgeNbr[a][k][1], nz = z + kEdgeNbr[a][k][2];
+            const bool inside = nx >= 0 && nx < g.gx && ny >= 0 && ny < g.gy && nz >= 0 && nz < g.gz;
+            q[k] = inside ? mesh_hash_find(keys, vals, mask, flat_key(g, nx, ny, nz)) : kNoVoxel;
             ok = ok && q[k] != kNoVoxel;
         }
     }

@@ -278,14 +278,13 @@ def sheets(seed: int = 3, n_sheets: int = 2000, n_creases: int = 1000, grid_size
         ext = 0.5 * math.sqrt(2 * size * size + height * height) + 2 * vs
         centre = rng.uniform(-0.5 + ext, 0.5 - ext, size=3)
         for k in range(per_stack):
-            v, t = _grid_mesh(lambda u, w: np.stack([u - 0.5, w - 0.5, np.zeros_like(u)], 1), 4, 8, False, False, 64)
-            tilt = random_rotation(rng)
+            # 6 x 7 quads = 84 triangles a sheet: 2000 sheets and 1000 creases of 32 give 200k faces
+            v, t = _grid_mesh(lambda u, w: np.stack([u - 0.5, w - 0.5, np.zeros_like(u)], 1), 6, 7, False, False, 64)
             ang = 1e-5 * rng.normal(size=3)
             small = np.array([[1, -ang[2], ang[1]], [ang[2], 1, -ang[0]], [-ang[1], ang[0], 1]])
             v = (v * size) @ small.T
             v[:, 2] += (k - per_stack / 2) * 0.3 * vs
             v = v @ rot.T + centre
-            del tilt
             verts.append(v)
             tris.append(t + off)
             off += v.shape[0]

@@ -19,10 +19,16 @@ import sys
 import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_ROOT = os.environ.get("OVX_REFERENCE_ROOT", "/root/reference")
+# the reference source tree; without it nothing is rebuilt and existing builds are kept
+REFERENCE_ROOT = os.environ.get("OVX_REFERENCE_ROOT", "")
 ORACLE_SO = os.path.join(HERE, "libfdg_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_SO = os.path.join(REF_DIR, "fdg_ref" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def _ref_src(*parts):
+    """Path of a file of the reference source tree, or None when OVX_REFERENCE_ROOT is unset."""
+    return os.path.join(REFERENCE_ROOT, *parts) if REFERENCE_ROOT else None
 
 
 def _newer(target, sources):
@@ -42,8 +48,8 @@ def build_oracle(force=False):
 
 def build_ref(force=False):
     """Compile the reference CPU path; returns the .so path or None if the source is absent."""
-    ref_cpp = os.path.join(REFERENCE_ROOT, "src", "convert", "flexible_dual_grid.cpp")
-    if not os.path.exists(ref_cpp):
+    ref_cpp = _ref_src("src", "convert", "flexible_dual_grid.cpp")
+    if not ref_cpp or not os.path.exists(ref_cpp):
         return REF_SO if os.path.exists(REF_SO) else None
     binding = os.path.join(HERE, "ref_binding.cpp")
     shim = os.path.join(HERE, "eigen_shim")
@@ -75,8 +81,8 @@ def build_ref_zorder(force=False):
     """Compile the reference's z-order source (src/serialize/z_order.cu; its
     CPU functions are what the binding calls) into oracle/_ref; returns the .so
     path or None if the source is absent."""
-    src = os.path.join(REFERENCE_ROOT, "src", "serialize", "z_order.cu")
-    if not os.path.exists(src):
+    src = _ref_src("src", "serialize", "z_order.cu")
+    if not src or not os.path.exists(src):
         return REF_ZORDER_SO if os.path.exists(REF_ZORDER_SO) else None
     binding = os.path.join(HERE, "ref_zorder_binding.cu")
     if not (force or _newer(REF_ZORDER_SO, [src, binding])):
@@ -96,8 +102,8 @@ def build_ref_hilbert(force=False):
     """Compile the reference's Hilbert source (src/serialize/hilbert.cu; its CPU
     functions are what the binding calls) into oracle/_ref; returns the .so path
     or None if the source is absent."""
-    src = os.path.join(REFERENCE_ROOT, "src", "serialize", "hilbert.cu")
-    if not os.path.exists(src):
+    src = _ref_src("src", "serialize", "hilbert.cu")
+    if not src or not os.path.exists(src):
         return REF_HILBERT_SO if os.path.exists(REF_HILBERT_SO) else None
     binding = os.path.join(HERE, "ref_hilbert_binding.cu")
     if not (force or _newer(REF_HILBERT_SO, [src, binding])):
@@ -110,8 +116,53 @@ def build_ref_hilbert(force=False):
     return REF_HILBERT_SO
 
 
+REF_HASH_SO = os.path.join(REF_DIR, "hash_ref" + sysconfig.get_config_var("EXT_SUFFIX"))
+
+
+def build_ref_hash(force=False):
+    """Compile the reference's GPU hashmap (src/hash/hash.cu) with
+    ref_hash_binding.cpp into oracle/_ref, as a torch extension for sm_100
+    (the reference's generic build, setup.py:35-73); returns the .so path or
+    None if neither the source nor a build exists."""
+    src = _ref_src("src", "hash", "hash.cu")
+    if not src or not os.path.exists(src):
+        return REF_HASH_SO if os.path.exists(REF_HASH_SO) else None
+    binding = os.path.join(HERE, "ref_hash_binding.cpp")
+    if not (force or _newer(REF_HASH_SO, [src, binding])):
+        return REF_HASH_SO
+    import tempfile
+
+    import torch
+    from torch.utils import cpp_extension as ce
+
+    os.makedirs(REF_DIR, exist_ok=True)
+    cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    defs = [f"-D_GLIBCXX_USE_CXX11_ABI={abi}", "-DTORCH_EXTENSION_NAME=hash_ref", "-DTORCH_API_INCLUDE_EXTENSION_H"]
+    incs = ["-I", os.path.join(REFERENCE_ROOT, "src"), "-I", sysconfig.get_paths()["include"],
+            "-I", os.path.join(cuda_home, "include")]
+    for p in ce.include_paths(device_type="cuda"):
+        incs += ["-I", p]
+    with tempfile.TemporaryDirectory() as tmp:
+        o1, o2 = os.path.join(tmp, "hash.o"), os.path.join(tmp, "binding.o")
+        subprocess.check_call([os.path.join(cuda_home, "bin", "nvcc"), "-c", src, "-o", o1, "-O3", "-std=c++17",
+                               "-gencode", "arch=compute_100,code=sm_100", "--expt-relaxed-constexpr",
+                               "-D__CUDA_NO_HALF_OPERATORS__", "-D__CUDA_NO_HALF_CONVERSIONS__",
+                               "-D__CUDA_NO_BFLOAT16_CONVERSIONS__", "-D__CUDA_NO_HALF2_OPERATORS__",
+                               "-Xcompiler", "-fPIC", "-w", *defs, *incs])
+        subprocess.check_call(["g++", "-c", binding, "-o", o2, "-O3", "-std=c++17", "-fPIC", "-w", *defs, *incs])
+        cmd = ["g++", "-shared", "-o", REF_HASH_SO, o1, o2]
+        for p in ce.library_paths(device_type="cuda"):
+            cmd += ["-L", p, f"-Wl,-rpath,{p}"]
+        cmd += ["-L", os.path.join(cuda_home, "lib64"), "-lcudart",
+                "-lc10", "-lc10_cuda", "-ltorch", "-ltorch_cpu", "-ltorch_cuda", "-ltorch_python"]
+        subprocess.check_call(cmd)
+    return REF_HASH_SO
+
+
 if __name__ == "__main__":
     print(build_oracle(force="--force" in sys.argv))
     print(build_ref(force="--force" in sys.argv))
     print(build_ref_zorder(force="--force" in sys.argv))
     print(build_ref_hilbert(force="--force" in sys.argv))
+    print(build_ref_hash(force="--force" in sys.argv))

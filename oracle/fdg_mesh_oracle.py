@@ -1,14 +1,16 @@
 """CPU restatement of o_voxel.convert.flexible_dual_grid_to_mesh
 (o_voxel/convert/flexible_dual_grid.py:332-477; its voxel lookup follows
-src/hash/hash.cu:269-420) in numpy float32 -- test infrastructure only.
+src/hash/hash.cu:269-300 and :366-420) in numpy float32 -- test
+infrastructure only.
 
-Parity status: this restatement follows the reference's tensor operations one
-by one (each op rounded to float32).  The reference runs them as separate
-torch CUDA kernels; its cross product kernel may contract to FMA, so a split
-decision can differ from the reference's only where a quad's normal
-alignment is exactly zero in one evaluation and not in the other.  Not pinned
-against reference outputs: the reference path needs its CUDA hashmap, which is
-not run here.
+The restatement follows the reference's tensor operations one by one (each op
+rounded to float32).  A neighbour voxel outside [0, grid) on any axis is not
+looked up and counts as absent, as the reference's hashmap_lookup_3d kernel
+does (hash.cu:283-286).
+
+Pinned: it equals the golden outputs of the reference's own Python function
+(tests/golden/to_mesh.npz, made by tests/golden/make_to_mesh_golden.py) bit for
+bit on every case and mode there.
 """
 import numpy as np
 
@@ -52,6 +54,8 @@ def to_mesh(coords, dual, flags, split_weight, grid_size, voxel_size, aabb_min, 
     nbr = coords[:, None, None, :] + EDGE_NBR[None]  # [N,3,4,3]
     cand = nbr[flags]  # [M,4,3], (voxel, axis) order
     ck = cand[..., 0] * gy * gz + cand[..., 1] * gz + cand[..., 2]
+    inside = ((cand >= 0) & (cand < np.array([gx, gy, gz]))).all(-1)
+    ck = np.where(inside, ck, -1)
     idx = np.array([[table.get(k, -1) for k in row] for row in ck.tolist()], dtype=np.int64).reshape(-1, 4)
     quads = idx[(idx >= 0).all(1)]
     verts = (((coords.astype(np.float32) + dual).astype(np.float32) * vs).astype(np.float32) + amin).astype(np.float32)

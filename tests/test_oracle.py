@@ -10,9 +10,10 @@ import pytest
 import fdg_workloads as W
 from oracle import oracle as O
 
-# conversion fixtures (z_order.npz and hilbert.npz hold serialisation codes; test_serialize_cpu.py covers them)
+# conversion fixtures (z_order.npz and hilbert.npz hold serialisation codes, covered by
+# test_serialize_cpu.py; to_mesh.npz the inverse path, covered by test_to_mesh_cpu.py)
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if os.path.basename(p) not in ("z_order.npz", "hilbert.npz"))
+                if os.path.basename(p) not in ("z_order.npz", "hilbert.npz", "to_mesh.npz"))
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])

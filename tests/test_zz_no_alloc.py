@@ -68,3 +68,54 @@ def test_noalloc_grid_256_and_limits(cuda):
     big = np.array([1.0 / 512] * 3, np.float32)
     rc, n, _ = abi.occupancy_noalloc(t, big, [0, 0, 0, 512, 512, 512])
     assert rc == 5 and n == 0
+
+
+@pytest.mark.gpu
+def test_noalloc_brick_limit_exact_and_one_over(cuda):
+    """A non-cubic grid of exactly 32768 bricks (64 x 32 x 16, so the row-base
+    slot right after the bitmap is in use) matches the allocating entry point;
+    one brick more (3 x 11 x 993 = 32769) is refused with CAPACITY."""
+    import torch
+    import ovx_fdg_abi as abi
+
+    w = W.primitives(6, faces_total=20_000)
+    w = W.Workload(w.name, w.vertices, w.faces, [512, 256, 128], w.aabb)
+    tri, vs, gr = _soup(w)
+    assert (gr[3] // 8) * (gr[4] // 8) * (gr[5] // 8) == 32768
+    t = torch.from_numpy(tri).to(cuda)
+    ctx = abi.Context(cuda.index or 0)
+    try:
+        want = ctx.occupancy(t, vs, gr).cpu().numpy()
+    finally:
+        ctx.close()
+    assert want.shape[0] > 0
+    for _ in range(2):
+        rc, n, got = abi.occupancy_noalloc(t, vs, gr)
+        torch.cuda.synchronize()
+        assert rc == abi.OK and n == want.shape[0]
+        assert np.array_equal(got.cpu().numpy(), want)
+    rc, n, _ = abi.occupancy_noalloc(t, vs, [0, 0, 0, 24, 88, 7944])
+    assert rc == 5 and n == 0
+
+
+@pytest.mark.gpu
+def test_noalloc_lowpoly_grid_256(cuda):
+    """Large triangles (a low-poly soup on a 256^3 grid): each (triangle, axis)
+    pair is scanned by one thread here, so this is the slow case of this entry
+    point; results still equal the allocating entry point's."""
+    import torch
+    import ovx_fdg_abi as abi
+
+    w = W.lowpoly(5, faces_total=600, grid_size=256)
+    tri, vs, gr = _soup(w)
+    t = torch.from_numpy(tri).to(cuda)
+    ctx = abi.Context(cuda.index or 0)
+    try:
+        want = ctx.occupancy(t, vs, gr).cpu().numpy()
+    finally:
+        ctx.close()
+    for _ in range(2):
+        rc, n, got = abi.occupancy_noalloc(t, vs, gr)
+        torch.cuda.synchronize()
+        assert rc == abi.OK and n == want.shape[0]
+        assert np.array_equal(got.cpu().numpy(), want)
