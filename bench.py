@@ -52,6 +52,14 @@ LARGE = "subdivided-10.3M-faces-grid512"
 CPU_BUDGET_S = 150.0  # timed CPU reference steps stop once this much time has gone
 
 
+_T0 = time.perf_counter()
+
+
+def progress(msg):
+    """One timestamped progress line on stderr (the JSON result goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def load_workload(name=HEADLINE):
     import fdg_workloads as W
 
@@ -104,6 +112,22 @@ def _ref_worker(args):
     return time.perf_counter() - t0
 
 
+REF_PROCESS_BYTES = 2 << 30  # one full-mesh reference conversion peaks at about 1.6 GB of host memory
+
+
+def cpu_processes():
+    """Host cores to run reference conversions on: every core, at most 32, and
+    no more than the available host memory holds at REF_PROCESS_BYTES each."""
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+
+        n = min(n, max(1, int(psutil.virtual_memory().available // REF_PROCESS_BYTES)))
+    except Exception:
+        pass
+    return max(1, min(n, 32))
+
+
 class CpuBaseline:
     """The reference CPU implementation on all host cores.  The reference CPU
     path is single-threaded (flexible_dual_grid.cpp:660-992), so a step runs
@@ -117,7 +141,7 @@ class CpuBaseline:
         self.kind = "reference" if O.ref_module() is not None else "port"
         v, f, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
         self.faces = int(f.shape[0])
-        self.cores = cores or os.cpu_count() or 1
+        self.cores = cores or cpu_processes()
         self.job = (self.kind, v, f, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
         self.pool = mp.get_context("spawn").Pool(self.cores)
         self.latencies = []
@@ -198,6 +222,7 @@ def run_reference(args, rank):
     if rank != 0:
         return
     w = load_workload()
+    progress("reference arm: starting the CPU process pool")
     cb = CpuBaseline(w)
     warm = min(args.warmup, 1)
     for _ in range(warm):
@@ -207,6 +232,7 @@ def run_reference(args, rank):
     t_start = time.perf_counter()
     while len(times) < args.steps and (len(times) < 2 or time.perf_counter() - t_start < CPU_BUDGET_S):
         times.append(cb.step())
+        progress(f"reference arm: step {len(times)} took {times[-1]:.1f} s")
     cb.close()
     t = sum(times) / len(times)
     value = cb.cores * cb.faces / t / 1e6
@@ -395,6 +421,7 @@ def measure_workload(name, w, dev, stream, flush, steps, ref_gpu=None, ours_out=
     for _ in range(3):
         out = one()
     ms = time_steps(one, steps, stream, flush)
+    progress(f"{name}: this library {statistics.median(ms):.2f} ms")
     ctx._check(abi.lib().ovx_fdg_sync_status(ctx.handle, abi.ctypes.c_void_p(stream.cuda_stream)), "status")
     N = int(out[0].shape[0])
     t = statistics.median(ms)
@@ -409,6 +436,7 @@ def measure_workload(name, w, dev, stream, flush, steps, ref_gpu=None, ours_out=
     if ours_out is not None:
         ours_out.append(out)
     if ref_gpu is not None and ref_gpu.available():
+        progress(f"{name}: reference CUDA path, first call")
         fn = ref_gpu.prepare(w, dev)
         torch.cuda.synchronize()
         torch.cuda.reset_peak_memory_stats(dev)
@@ -422,6 +450,7 @@ def measure_workload(name, w, dev, stream, flush, steps, ref_gpu=None, ours_out=
         rpeak = torch.cuda.max_memory_allocated(dev) - base
         for _ in range(3):
             rout = fn()
+        progress(f"{name}: reference CUDA path, cold {rcold:.1f} ms; timing")
         rms = time_steps(fn, steps, stream, flush)
         rt = statistics.median(rms)
         res["reference_gpu"] = {
@@ -477,6 +506,7 @@ def run_ours(args, rank, world):
     clocks = ClockSampler(dev.index)
     clocks.start()
     launches0 = ctx.kernel_launches()
+    progress("headline: timed region")
     ms = time_steps(one, args.steps, stream, flush)
     torch.cuda.synchronize()
     launches = ctx.kernel_launches() - launches0
@@ -529,6 +559,7 @@ def run_ours(args, rank, world):
         e1.synchronize()
         return e0.elapsed_time(e1)
 
+    progress("end to end")
     e2e_run(2)
     e2e_ms = max_over_ranks(e2e_run(args.steps), world, dev) / args.steps
     e2e_value = replica_value(F, world, e2e_ms)
@@ -574,12 +605,14 @@ def run_ours(args, rank, world):
 
     cpu = None
     if not args.no_cpu_baseline and world == 1:
+        progress("CPU baseline")
         cb = CpuBaseline(w)
         cpu_t = cb.step()
         cb.close()
         cpu = cb.describe(cb.cores * cb.faces / cpu_t / 1e6)
     batched = None
     if not args.no_batch and world == 1:
+        progress("batched")
         batched = run_batched(dev)
     line = {
         "metric": METRIC, "value": value, "unit": "Mfaces/s", "n_gpus": world, "steps": args.steps,

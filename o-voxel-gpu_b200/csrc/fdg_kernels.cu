@@ -20,9 +20,12 @@
 //             boundary {e, 2<<30 | local voxel, 0}, e = index in the
 //                      boundary edge list, which is sorted by (v_min, v_max)
 //   qtab    plane quadric per triangle (10 floats)
-//   contrib per-voxel contribution lists, 16 B entries; brick b owns entries
+//   contrib per-voxel contribution lists of the bricks whose lists do not fit
+//           in shared memory, 16 B entries; brick b owns entries
 //           [4*roff[b], 4*roff[b+1]) (a record yields at most 4 contributions)
-//   vlist   per output row: first entry (40 bits) | entry count << 40 | sorted << 63
+//   vlist   per output row: first entry (40 bits) | entry count << 40, or 0
+//           for a row summed in brick_lists
+//   qreg    regularised quadric (10 floats) of each row summed in brick_lists
 //   estage, fstage  event and face records staged by the count pass (16 B,
 //           {brick, t, code, z} and {brick, t, code, rank in the brick})
 //   btab    line quadric per boundary edge (10 floats)
@@ -49,12 +52,14 @@
 //   boundary_records<FILL>
 //   brick_lists         one CTA per active brick: records -> per-voxel
 //                       contribution lists {key, payload} (a counting sort by
-//                       voxel), staged and the short ones sorted in shared
-//                       memory when the brick's lists fit there
-//   voxel_accumulate    one thread per voxel: sorts its list by key unless it is
-//                       marked sorted, sums it sequentially in FP32 in that order
-//                       (bit-identical to the reference CPU sums), regularises,
-//                       CPQR-solves
+//                       voxel).  When the brick's lists fit in shared memory
+//                       they are ordered there by key and each voxel's list is
+//                       summed sequentially in FP32 in that order (bit-identical
+//                       to the reference CPU sums) and regularised; otherwise
+//                       the lists go to global memory
+//   voxel_accumulate    one thread per voxel: solves the rows summed in
+//                       brick_lists; sorts, sums and regularises the others'
+//                       global lists first; CPQR solve
 //   constrained_solve   box-constrained search for the few voxels whose
 //                       unconstrained solution leaves the voxel
 //
@@ -86,13 +91,15 @@ constexpr int kUnitCells = 64;        // cells per unit of work of a large (tria
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
 constexpr int kListStage = 768; // contributions of a brick that brick_lists stages (and sorts) in shared memory
-// vlist word: first entry (bits 0-39) | count (bits 40-62) | sorted flag (bit 63)
+// vlist word: first entry (bits 0-39) | count (bits 40-62); 0 for a row that
+// brick_lists summed (every active voxel has at least one contribution)
 constexpr uint32_t kListCountMax = (1u << 23) - 1u;
-constexpr unsigned long long kListSorted = 1ull << 63;
 #ifndef OVX_FDG_WARP_SORT_MIN
 #define OVX_FDG_WARP_SORT_MIN 16
 #endif
 constexpr int kWarpSortMin = OVX_FDG_WARP_SORT_MIN; // lists this long or longer are ordered by the whole warp
+constexpr int kWarpSortPer = 2;                      // ... up to 2 entries per lane
+constexpr int kWarpSortMax = 32 * kWarpSortPer;      // longer lists go to voxel_accumulate_long
 
 // device counter words
 enum
@@ -1542,7 +1549,9 @@ struct SolveArgs
     uint32_t *longv;            // rows whose lists are too long for voxel_accumulate: up to kLongMidMax
                                 // entries from the front (counter C_LONG), longer ones from the back (C_HUGE)
     uint32_t longv_cap;
-    unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40 | sorted << 63
+    unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40;
+                                // 0: the row was summed by brick_lists and its quadric is in qreg
+    float *qreg;                // regularised quadric (10 floats) of the rows brick_lists summed
     float *clist; // deferred constrained searches, 16 words each
     uint32_t clist_cap;
 };
@@ -1764,8 +1773,9 @@ struct ListShared
     uint32_t scan_tmp[kConsumeThreads / 32 + 1]; // per-warp offsets, then the brick's total
     int nvox;
     uint32_t status;
+    uint32_t longest; // the brick's longest list
     // the brick's lists, when they fit (keys and payloads apart: 12 bytes an
-    // entry): filled, short lists sorted, copied out
+    // entry): filled, ordered by key and summed in place
     unsigned long long skey[kListStage];
     uint32_t spay[kListStage];
 };
@@ -1815,6 +1825,22 @@ struct ListStageFill
     }
 };
 
+// A voxel summed in brick_lists: its intersected flags go straight to the
+// output, its regularised quadric (flexible_dual_grid.cpp:780-792) to qreg for
+// the solve.
+__device__ __forceinline__ void voxel_sum_out(const SolveArgs &A, long long row, const Acc &a)
+{
+    float q[10];
+    regularize(a.q, a.mean, a.cnt, A.rw, q);
+    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
+    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
+    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
+    float *d = A.qreg + row * 10;
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        d[i] = q[i];
+}
+
 __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
 {
     __shared__ ListShared S;
@@ -1828,7 +1854,10 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     for (int i = tid; i < 512; i += blockDim.x)
         S.cnt[i] = 0;
     if (tid == 0)
+    {
         S.status = 0;
+        S.longest = 0;
+    }
     load_brick_ranks(S, A.bits, b, A.zorder);
     const int nvox = S.nvox;
     const unsigned long long vbase = A.bbase[b];
@@ -1853,14 +1882,17 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     {
         const int lane = tid & 31, warp = tid >> 5;
         constexpr int per = 512 / kConsumeThreads;
-        uint32_t v[per], sum = 0;
+        uint32_t v[per], sum = 0, mx = 0;
 #pragma unroll
         for (int k = 0; k < per; ++k)
         {
             const int j = tid * per + k;
             v[k] = j < nvox ? S.cnt[j] : 0u;
             sum += v[k];
+            mx = v[k] > mx ? v[k] : mx;
         }
+        if (mx > (uint32_t)kWarpSortMax)
+            atomicMax(&S.longest, mx);
         uint32_t incl = sum;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1)
@@ -1884,7 +1916,9 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
             S.scan_tmp[kConsumeThreads / 32] = r;
         }
         __syncthreads();
-        const bool staged = S.scan_tmp[kConsumeThreads / 32] <= (uint32_t)kListStage;
+        // the brick is summed here when its lists fit in shared memory and
+        // none is too long for a warp to order
+        const bool fused = S.scan_tmp[kConsumeThreads / 32] <= (uint32_t)kListStage && S.longest == 0u;
         uint32_t run = S.scan_tmp[warp] + incl - sum;
         const unsigned long long first = 4ull * A.roff[b];
 #pragma unroll
@@ -1895,8 +1929,7 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
             {
                 if (v[k] == 0u || v[k] > kListCountMax)
                     atomicOr(&S.status, (uint32_t)ST_REPLAY); // every active voxel has a scanline contribution
-                const bool sorted = staged && v[k] < (uint32_t)kWarpSortMin;
-                A.vlist[vbase + j] = (first + run) | ((unsigned long long)v[k] << 40) | (sorted ? kListSorted : 0ull);
+                A.vlist[vbase + j] = fused ? 0ull : (first + run) | ((unsigned long long)v[k] << 40);
             }
             S.off[j] = run;
             run += v[k];
@@ -1905,10 +1938,12 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     __syncthreads();
     const uint32_t total = S.scan_tmp[kConsumeThreads / 32];
     uint4 *out = A.contrib + 4ull * A.roff[b];
-    if (total <= (uint32_t)kListStage)
+    if (total <= (uint32_t)kListStage && S.longest == 0u)
     {
-        // the lists fit in shared memory: fill them there, sort the short ones
-        // (one thread per voxel), copy the brick's lists out in one sweep
+        // The lists fit in shared memory: fill them there, order each by key
+        // (short lists by one thread, the others by a warp), then sum every
+        // voxel's list in that order (the reference CPU order), regularise and
+        // leave the quadric for the solve; no list goes to global memory.
         {
             ListStageFill fs{S};
             for (unsigned long long r = tid; r < nrec; r += blockDim.x)
@@ -1937,11 +1972,70 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
                 P[y] = pv;
             }
         }
-        __syncthreads();
-        for (uint32_t i = tid; i < total; i += blockDim.x)
         {
-            const unsigned long long k = S.skey[i];
-            out[i] = make_uint4((uint32_t)k, (uint32_t)(k >> 32), S.spay[i], 0u);
+            // lists of kWarpSortMin..kWarpSortMax entries: each warp ranks one
+            // list at a time (keys are unique per voxel), all lanes read their
+            // entries before any lane stores
+            const int lane = tid & 31;
+            for (int j = tid >> 5; j < nvox; j += kConsumeThreads / 32)
+            {
+                const uint32_t c = S.cnt[j];
+                if (c < (uint32_t)kWarpSortMin)
+                    continue;
+                const uint32_t st = S.off[j] - c;
+                unsigned long long k[kWarpSortPer];
+                uint32_t pv[kWarpSortPer], r[kWarpSortPer];
+#pragma unroll
+                for (int q = 0; q < kWarpSortPer; ++q)
+                {
+                    const uint32_t idx = (uint32_t)(lane + 32 * q);
+                    k[q] = idx < c ? S.skey[st + idx] : ~0ull;
+                    pv[q] = idx < c ? S.spay[st + idx] : 0u;
+                    r[q] = 0;
+                }
+#pragma unroll
+                for (int sq = 0; sq < kWarpSortPer; ++sq)
+                {
+                    if ((uint32_t)(32 * sq) >= c)
+                        break;
+                    const uint32_t jn = c - 32u * sq < 32u ? c - 32u * sq : 32u;
+                    for (uint32_t jj = 0; jj < jn; ++jj)
+                    {
+                        const unsigned long long kj = S.skey[st + 32u * sq + jj];
+#pragma unroll
+                        for (int q = 0; q < kWarpSortPer; ++q)
+                            r[q] += kj < k[q];
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < kWarpSortPer; ++q)
+                    if ((uint32_t)(lane + 32 * q) < c)
+                    {
+                        S.skey[st + r[q]] = k[q];
+                        S.spay[st + r[q]] = pv[q];
+                    }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int lv = tid; lv < 512; lv += blockDim.x)
+        {
+            if (!((S.obits[lv >> 5] >> (lv & 31)) & 1u))
+                continue;
+            const int j = dense_index(S, lv);
+            const long long row = (long long)(vbase + j);
+            const uint32_t c = S.cnt[j], st = S.off[j] - c;
+            const int vc[3] = {o[0] + (lv & 7), o[1] + ((lv >> 3) & 7), o[2] + (lv >> 6)};
+            Acc a;
+            acc_init(a);
+            for (uint32_t x = 0; x < c; ++x)
+            {
+                Contrib cb;
+                contrib_load(A, vc, S.skey[st + x], S.spay[st + x], cb);
+                contrib_apply(cb, a);
+            }
+            voxel_sum_out(A, row, a);
         }
     }
     else
@@ -1966,17 +2060,13 @@ __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int
     return (unsigned long long)lo | ((unsigned long long)hi << 32);
 }
 
-// Regularise and solve one voxel (flexible_dual_grid.cpp:763-797); a voxel whose
-// unconstrained solution leaves its box goes to the constrained-search list.
-__device__ __forceinline__ void voxel_finish(const SolveArgs &A, long long row, const int vc[3], const Acc &a)
+// Solve one voxel from its regularised quadric (flexible_dual_grid.cpp:795-797);
+// a voxel whose unconstrained solution leaves its box goes to the
+// constrained-search list.
+__device__ __forceinline__ void voxel_solve(const SolveArgs &A, long long row, const int vc[3], const float q[10])
 {
-    float q[10];
-    regularize(a.q, a.mean, a.cnt, A.rw, q);
     float v[3];
     const bool inside = solve_unconstrained(vc, A.m.g, q, v);
-    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
-    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
-    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
     if (inside)
     {
         A.dual[row * 3 + 0] = v[0];
@@ -2000,8 +2090,17 @@ __device__ __forceinline__ void voxel_finish(const SolveArgs &A, long long row, 
         c[4 + i] = q[i];
 }
 
-constexpr int kWarpSortPer = 2;                      // ... up to 2 entries per lane
-constexpr int kWarpSortMax = 32 * kWarpSortPer;      // longer lists go to voxel_accumulate_long
+// Regularise and solve one voxel summed from its list (flexible_dual_grid.cpp:763-797).
+__device__ __forceinline__ void voxel_finish(const SolveArgs &A, long long row, const int vc[3], const Acc &a)
+{
+    float q[10];
+    regularize(a.q, a.mean, a.cnt, A.rw, q);
+    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
+    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
+    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
+    voxel_solve(A, row, vc, q);
+}
+
 constexpr int kLongMidMax = 1024;                    // ... one CTA of 128 threads, shared-memory sort
 constexpr int kLongHugeMax = 8192;                   // ... one CTA of 256 threads; longer: in-place insertion sort
 
@@ -2015,7 +2114,6 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
     const unsigned long long d = valid ? A.vlist[row] : 0ull;
     const unsigned long long first = d & ((1ull << 40) - 1ull);
     const uint32_t n = (uint32_t)(d >> 40) & kListCountMax;
-    const bool sorted = (d & kListSorted) != 0ull;
     // The warp orders the longer lists of its 32 voxels one after another: each
     // lane holds up to kWarpSortPer entries of the list and finds their ranks
     // among the list's (unique) keys, then stores the entries at those ranks.
@@ -2078,10 +2176,21 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
         return;
     }
     const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
-    uint4 *lst = A.contrib + first;
-    if (n < (uint32_t)kWarpSortMin && !sorted)
+    if (n == 0)
     {
-        // short lists that brick_lists could not sort in shared memory:
+        // summed by brick_lists: solve from the stored quadric
+        float q[10];
+        const float *qs = A.qreg + row * 10;
+#pragma unroll
+        for (int i = 0; i < 10; ++i)
+            q[i] = qs[i];
+        voxel_solve(A, row, vc, q);
+        return;
+    }
+    uint4 *lst = A.contrib + first;
+    if (n < (uint32_t)kWarpSortMin)
+    {
+        // short lists of bricks whose lists did not fit in shared memory:
         // insertion sort in place
         for (uint32_t x = 1; x < n; ++x)
         {
@@ -2601,7 +2710,7 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, scan_units, face_large, face_units, qtab;
     Buf vcnt, voff, emax, bkeys, blong, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, fstage, estage, longv, face_end;
+    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, qreg, fstage, estage, longv, face_end;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     unsigned long long *host = nullptr;     // readback words: pinned, mapped host memory
     unsigned long long *host_dev = nullptr; // the same words as the device addresses them
@@ -2645,7 +2754,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large, &c->scan_units,
                 &c->face_large, &c->face_units, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->blong, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv, &c->face_end,
+                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->qreg, &c->fstage, &c->estage, &c->longv, &c->face_end,
                 &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
@@ -3566,6 +3675,7 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(ensure(st, ctx, ctx->clist, (size_t)(n + 1) * 16 * 4));
     OVX_CUDA(ensure(st, ctx, ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
     OVX_CUDA(ensure(st, ctx, ctx->vlist, (size_t)n * 8));
+    OVX_CUDA(ensure(st, ctx, ctx->qreg, (size_t)n * 40));
     OVX_CUDA(ensure(st, ctx, ctx->longv, (size_t)(n + 1) * 4));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_LONG, 0, 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
@@ -3612,6 +3722,7 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.clist = (float *)ctx->clist.p;
     SA.contrib = (uint4 *)ctx->contrib.p;
     SA.vlist = (unsigned long long *)ctx->vlist.p;
+    SA.qreg = (float *)ctx->qreg.p;
     SA.longv = (uint32_t *)ctx->longv.p;
     SA.longv_cap = (uint32_t)(n + 1);
     SA.clist_cap = (uint32_t)(n + 1);

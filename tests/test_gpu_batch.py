@@ -78,3 +78,32 @@ def test_batch_error_is_raised(cuda):
     w = W.ico_cap(0)
     r = O.run_workload(w)
     assert_fdg_equal(tuple(t.cpu().numpy() for t in outs[0]), (r.voxels, r.dual, r.intersected), "after error")
+
+
+@pytest.mark.gpu
+@pytest.mark.slow
+def test_full_256_mesh_batch(cuda):
+    """The 256-mesh mixed batch that bench.py times (faces log-uniform 1k-500k,
+    grids 64-512, per-mesh aabb): every mesh equals the single-mesh API row for
+    row, and a seeded subset -- including every grid-512 mesh of 300k faces or
+    more, up to four -- equals the oracle."""
+    import torch
+    import o_voxel
+
+    ws = W.batch(4)
+    meshes = _upload(ws, cuda)
+    kw = dict(face_weight=1.0, boundary_weight=0.2, regularization_weight=1e-2)
+    outs = o_voxel.convert.mesh_to_flexible_dual_grid_batch(
+        meshes, grid_size=[w.grid_size for w in ws], aabb=[w.aabb for w in ws], **kw)
+    torch.cuda.synchronize()
+    assert len(outs) == len(ws)
+    big = [i for i, w in enumerate(ws) if w.grid_size == 512 and w.num_faces >= 300_000][:4]
+    assert big, "the batch has grid-512 meshes of 300k faces or more"
+    rng = np.random.default_rng(11)
+    subset = sorted(set(big) | set(rng.choice(len(ws), size=8, replace=False).tolist()))
+    for i, (w, (v, f), out) in enumerate(zip(ws, meshes, outs)):
+        single = o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=w.grid_size, aabb=w.aabb, **kw)
+        for a, b in zip(out, single):
+            assert torch.equal(a, b), (i, w.name)
+        if i in subset:
+            assert_fdg_equal(tuple(t.cpu().numpy() for t in out), _oracle(w, ("batch4", w.name)), w.name)
