@@ -13,9 +13,8 @@ size is used).  Prints one JSON line on rank 0.
              conversion time against the measured HBM copy bandwidth
   workloads  the 10.3M-face subdivided mesh at grid 512, timed the same way,
              with its own roofline and memory
-  reference_gpu  the reference's own CUDA implementation of the path (built
-             from its sources into baseline/_ref by baseline/build_ref_gpu.py),
-             timed on the same GPU, same inputs, same method, on both meshes
+  reference_gpu  the reference's own CUDA implementation of the path: not
+             run (it stalled on the 282k-face mesh; see REFERENCE_GPU_UNAVAILABLE)
   cpu_baseline  the reference's CPU implementation on the host cores: every
              core converts the full 282k-face mesh once
   batched    256 mixed meshes (grids 64-512): the batched API against one
@@ -249,9 +248,6 @@ def run_reference(args, rank):
 
 
 # ----------------------------------------------------------------------------- batched workload
-BATCH_WORKERS = 8
-
-
 def run_batched(dev, steps=10, warmup=2):
     """256 seeded meshes built like the 282k-face one, face counts log-uniform in
     [1k, 500k] (about 21M faces in all), grid 64/128/256/512 per mesh, per-mesh
@@ -273,7 +269,7 @@ def run_batched(dev, steps=10, warmup=2):
             o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=w.grid_size, aabb=w.aabb, **kw)
 
     def batched():
-        o_voxel.convert.mesh_to_flexible_dual_grid_batch(meshes, grid_size=grids, aabb=aabbs, workers=BATCH_WORKERS, **kw)
+        o_voxel.convert.mesh_to_flexible_dual_grid_batch(meshes, grid_size=grids, aabb=aabbs, **kw)
 
     def timed(fn):
         # the contexts reach their largest workspaces during the warm-up
@@ -293,7 +289,7 @@ def run_batched(dev, steps=10, warmup=2):
     t_plain, plain_ms = timed(plain)
     t_batch, batch_ms = timed(batched)
     return {"workload": "256 meshes, faces log-uniform 1k-500k, grids 64-512, per-mesh aabb",
-            "meshes": len(ws), "faces": int(F), "workers": BATCH_WORKERS, "steps": steps, "warmup": warmup,
+            "meshes": len(ws), "faces": int(F), "steps": steps, "warmup": warmup,
             "timing": "median of the steps (CUDA events on the caller's stream, host included)",
             "plain_step_ms": plain_ms, "batched_step_ms": batch_ms,
             "plain_ms": t_plain, "plain_spread_ms": [min(plain_ms), max(plain_ms)],
@@ -301,7 +297,8 @@ def run_batched(dev, steps=10, warmup=2):
             "batched_ms": t_batch, "batched_spread_ms": [min(batch_ms), max(batch_ms)],
             "batched_meshes_per_s": len(ws) / (t_batch / 1e3),
             "batched_mfaces_per_s": F / (t_batch / 1e3) / 1e6, "speedup": t_plain / t_batch,
-            "api": "o_voxel.convert.mesh_to_flexible_dual_grid_batch vs one mesh_to_flexible_dual_grid call per mesh"}
+            "api": "o_voxel.convert.mesh_to_flexible_dual_grid_batch (one pipeline per group of meshes, default "
+                   "max_group_records) vs one mesh_to_flexible_dual_grid call per mesh"}
 
 
 # ----------------------------------------------------------------------------- ranks
@@ -341,65 +338,17 @@ def time_steps(fn, steps, stream, flush):
     return ms
 
 
-def canonical(vox, dual, inter):
-    """Rows sorted by voxel coordinate (x slowest), for comparing outputs of different row orders."""
-    import torch
-
-    v = vox.long()
-    key = (v[:, 0] << 42) | (v[:, 1] << 21) | v[:, 2]
-    o = torch.argsort(key)
-    return vox[o], dual[o], inter[o]
-
-
-def compare_outputs(got, want, voxel_size):
-    """Parity of one conversion's outputs against another's: occupancy set,
-    flag mismatches, dual-vertex differences in voxel edges."""
-    import torch
-
-    gv, gd, gi = canonical(*got)
-    wv, wd, wi = canonical(*want)
-    if gv.shape != wv.shape or not torch.equal(gv, wv):
-        return {"occupancy_equal": False, "voxels": [int(gv.shape[0]), int(wv.shape[0])]}
-    vs = torch.tensor(voxel_size, dtype=torch.float64, device=gd.device)
-    d = (gd.double() - wd.double()) / vs
-    err = d.norm(dim=1)
-    return {"occupancy_equal": True, "flag_mismatches": int((gi != wi).sum().item()),
-            "dual_rms_voxel": float(err.square().mean().sqrt().item()), "dual_max_voxel": float(err.max().item()),
-            "dual_bit_identical_rows": float((gd.view(torch.int32) == wd.view(torch.int32)).all(1).float().mean().item())}
-
-
-class RefGpu:
-    """The reference's own CUDA implementation (baseline/_ref), called the way
-    its wrapper calls it: vertices already shifted by aabb[0] and int32 faces
-    (flexible_dual_grid.py:89-90,181,184); those input passes are done once,
-    outside the timed region."""
-
-    def __init__(self):
-        sys.path.insert(0, os.path.join(REPO, "baseline"))
-        import build_ref_gpu
-
-        self.mod = build_ref_gpu.load()
-
-    def available(self):
-        return self.mod is not None
-
-    def prepare(self, w, dev):
-        import numpy as np
-        import torch
-
-        origin, vs, gr = grid_args(w)
-        v = (torch.from_numpy(w.vertices).to(dev) - torch.from_numpy(np.asarray(origin)).to(dev)).contiguous()
-        f = torch.from_numpy(w.faces).to(dev).int().contiguous()
-        args = (v, f, [float(x) for x in vs], gr, float(w.face_weight), float(w.boundary_weight),
-                float(w.regularization_weight))
-        return lambda: self.mod.mesh_to_flexible_dual_grid_cuda(*args)
+REFERENCE_GPU_UNAVAILABLE = (
+    "not run: the reference's CUDA path (built from its sources by baseline/build_ref_gpu.py, sm_100) gave no result "
+    "for over 25 minutes on the 282k-face mesh and was killed; the same benchmark without it finished in 30 s. "
+    "Its brick-publication wait (src/convert/mesh_to_flexible_dual_grid_gpu/intersect_qef.cu:364-373) has no bound, "
+    "so it is not run again on the shared GPUs")
 
 
 # ----------------------------------------------------------------------------- our arm
-def measure_workload(name, w, dev, stream, flush, steps, ref_gpu=None, ours_out=None):
+def measure_workload(name, w, dev, stream, flush, steps, ours_out=None):
     """Device-resident timing of one workload through a fresh C-ABI context
-    (cold first call, then warm steps), its roofline and memory; and, when
-    given, the reference's CUDA path on the same inputs."""
+    (cold first call, then warm steps), its roofline and memory."""
     import torch
 
     import ovx_fdg_abi as abi
@@ -435,31 +384,6 @@ def measure_workload(name, w, dev, stream, flush, steps, ref_gpu=None, ours_out=
                       "note": "the library's workspace after this workload on a fresh context, plus the outputs"}}
     if ours_out is not None:
         ours_out.append(out)
-    if ref_gpu is not None and ref_gpu.available():
-        progress(f"{name}: reference CUDA path, first call")
-        fn = ref_gpu.prepare(w, dev)
-        torch.cuda.synchronize()
-        torch.cuda.reset_peak_memory_stats(dev)
-        base = torch.cuda.memory_allocated(dev)
-        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        r0.record(stream)
-        rout = fn()
-        r1.record(stream)
-        r1.synchronize()
-        rcold = r0.elapsed_time(r1)
-        rpeak = torch.cuda.max_memory_allocated(dev) - base
-        for _ in range(3):
-            rout = fn()
-        progress(f"{name}: reference CUDA path, cold {rcold:.1f} ms; timing")
-        rms = time_steps(fn, steps, stream, flush)
-        rt = statistics.median(rms)
-        res["reference_gpu"] = {
-            "ms": rt, "ms_spread": [min(rms), max(rms)], "mfaces_per_s": F / (rt / 1e3) / 1e6, "cold_ms": rcold,
-            "peak_allocated_bytes": int(rpeak), "speedup_of_this_library": rt / t,
-            "parity_vs_this_library": compare_outputs(rout, out, vs),
-            "note": "reference CUDA path (src/convert/mesh_to_flexible_dual_grid_gpu, sm_100 build) through its operator; "
-                    "parity is informational (its arithmetic deviates from its CPU path in known places)"}
-        del rout
     ctx.close()
     return res
 
@@ -581,25 +505,13 @@ def run_ours(args, rank, world):
     ctx.close()
     del out
 
-    # the other workloads and the reference's CUDA path, single GPU only
-    workloads, reference_gpu = {}, None
-    if world == 1 and not args.no_reference_gpu:
-        ref = RefGpu()
-        reference_gpu = {"available": ref.available()}
-        if not ref.available():
-            reference_gpu["why"] = "baseline/_ref not built (baseline/build_ref_gpu.py needs the reference source tree)"
-        else:
-            reference_gpu["build"] = "reference src/convert/mesh_to_flexible_dual_grid_gpu/*.cu, nvcc -O3 sm_100"
-    else:
-        ref = None
-    head = measure_workload(HEADLINE, w, dev, stream, flush, args.steps, ref_gpu=ref)
-    if ref is not None and "reference_gpu" in head:
-        reference_gpu[HEADLINE] = head["reference_gpu"]
+    # the other workload, single GPU only
+    workloads = {}
+    reference_gpu = {"available": False, "why": REFERENCE_GPU_UNAVAILABLE}
+    head = measure_workload(HEADLINE, w, dev, stream, flush, args.steps)
     if world == 1 and not args.no_large:
         wl = load_workload(LARGE)
-        workloads[LARGE] = measure_workload(LARGE, wl, dev, stream, flush, max(3, min(args.steps, 10)), ref_gpu=ref)
-        if ref is not None and "reference_gpu" in workloads[LARGE]:
-            reference_gpu[LARGE] = workloads[LARGE].pop("reference_gpu")
+        workloads[LARGE] = measure_workload(LARGE, wl, dev, stream, flush, max(3, min(args.steps, 10)))
         del wl
         torch.cuda.empty_cache()
 
@@ -636,7 +548,7 @@ def run_ours(args, rank, world):
         "memory": {"workspace_bytes": workspace, "torch_max_allocated_bytes": int(torch.cuda.max_memory_allocated(dev)),
                    "note": "workspace: the conversion context's buffers (grown to the largest conversion); torch: outputs, inputs, "
                            "the 256 MB L2 flush buffer, the reference's CUDA path and the batched leg"},
-        "workloads": {HEADLINE: {k: v for k, v in head.items() if k != "reference_gpu"}, **workloads},
+        "workloads": {HEADLINE: head, **workloads},
         "reference_gpu": reference_gpu,
         "cpu_baseline": cpu,
         "clocks": clk,
@@ -707,7 +619,6 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-mesh batched measurement")
     ap.add_argument("--no-large", action="store_true", help="skip the 10.3M-face workload")
-    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference's CUDA path")
     ap.add_argument("--workload", default=None, help="run one workload and print its timings instead (ico_cap, primitives, "
                                                      "subdivided, sheets, lowpoly)")
     ap.add_argument("--grid", type=int, default=0, help="grid size for --workload subdivided / lowpoly")

@@ -177,6 +177,38 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
 int ovx_fdg_sync_status(ovx_fdg_context *ctx, void *stream);
 
 /*
+ * Batched conversion: many meshes, each with its own grid and origin, in one
+ * pipeline (no counterpart in the reference, which converts one mesh per
+ * call: o_voxel._C.mesh_to_flexible_dual_grid_cuda, src/ext.cpp:19).  All
+ * meshes' triangles, bricks and vertices are laid out one mesh after another
+ * and every kernel of the conversion runs once over all of them, so a batch
+ * costs one host synchronisation (in begin) and one set of launches instead of
+ * one per mesh.  Each mesh's result equals what ovx_fdg_begin/ovx_fdg_finish
+ * give for it alone, row for row.
+ *
+ * begin_batch: num_voxels[i] receives mesh i's row count, *total_voxels their
+ * sum.  finish_batch: output buffers with room for total_voxels rows; mesh
+ * i's rows start at num_voxels[0] + ... + num_voxels[i-1].  Same semantics,
+ * order options and errors as the single-mesh calls (an error names the
+ * mesh).  Limits over the whole batch: 2^30 faces, 2^31-1 vertices, 2^31
+ * bricks of the grids.
+ */
+typedef struct ovx_fdg_mesh
+{
+    const float *vertices; /* device float32 [num_vertices,3], not shifted */
+    int64_t num_vertices;
+    const void *faces; /* device int32 or int64 [num_faces,3] */
+    int32_t face_index_bytes;
+    int64_t num_faces;
+    float origin[3]; /* subtracted from the vertices in float32 (aabb[0]) */
+    ovx_fdg_grid grid;
+} ovx_fdg_mesh;
+
+int ovx_fdg_begin_batch(ovx_fdg_context *ctx, void *stream, const ovx_fdg_mesh *meshes, int32_t num_meshes, float face_weight,
+                        float boundary_weight, float regularization_weight, int64_t *num_voxels, int64_t *total_voxels);
+int ovx_fdg_finish_batch(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, float *dual_vertices, uint8_t *intersected);
+
+/*
  * Occupancy only (reference intersect_occ).  triangles: device float32
  * [num_triangles, 3, 3] in grid-local coordinates (already shifted), as the
  * reference operator takes them.  begin returns N; finish writes int32 [N,3].

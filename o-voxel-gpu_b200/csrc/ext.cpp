@@ -12,9 +12,9 @@
 // the aabb origin and int32 or int64 faces so the wrapper does not need the
 // extra cast and shift passes over the inputs, and
 // `mesh_to_flexible_dual_grid_cuda_batch`, which converts a list of meshes
-// (each with its own grid) with a pool of host worker threads, each owning a
-// library context and a CUDA stream, so that one mesh's host synchronisation,
-// output allocation and small launches overlap the other meshes' GPU work.
+// (each with its own grid) through the library's batched conversion: every
+// kernel runs once over a group of meshes, with one host synchronisation per
+// group; groups bound the workspace by an estimate of their records.
 //
 // All compute goes through the C ABI in include/ovx_fdg.h (libovx_fdg.so).
 // Setting OVX_FDG_CHECK in the environment makes every call wait for its
@@ -28,13 +28,11 @@
 
 #include <c10/cuda/CUDAStream.h>
 
-#include <atomic>
 #include <cstdlib>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "ovx_fdg.h"
@@ -126,21 +124,30 @@ std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Ten
     return std::make_tuple(vox, dual, inter);
 }
 
-// Worker contexts of the batched path: one per (device, worker slot), kept for
-// the life of the process like the single-mesh context.
-DeviceContext &worker_context(int device, int slot)
+// Context of the batched path on a device, kept for the life of the process
+// like the single-mesh context.
+DeviceContext &batch_context(int device)
 {
     static std::mutex map_mu;
-    static std::map<std::pair<int, int>, std::unique_ptr<DeviceContext>> contexts;
+    static std::map<int, std::unique_ptr<DeviceContext>> contexts;
     std::lock_guard<std::mutex> lock(map_mu);
-    auto &ptr = contexts[{device, slot}];
-    if (!ptr)
+    auto &slot = contexts[device];
+    if (!slot)
     {
-        ptr = std::make_unique<DeviceContext>();
-        const int rc = ovx_fdg_context_create(device, &ptr->ctx);
+        slot = std::make_unique<DeviceContext>();
+        const int rc = ovx_fdg_context_create(device, &slot->ctx);
         TORCH_CHECK(rc == OVX_FDG_OK, "ovx_fdg_context_create failed: ", ovx_fdg_status_string(rc));
     }
-    return *ptr;
+    return *slot;
+}
+
+// Records a mesh is expected to produce, for sizing batch groups: about eight
+// per unit of grid face area and three per triangle (the measured mixture of
+// surface-bound and face-bound meshes stays below this on average).
+int64_t estimated_records(const ovx_fdg_grid &g, int64_t faces)
+{
+    const int64_t x = g.grid_max[0] - g.grid_min[0], y = g.grid_max[1] - g.grid_min[1], z = g.grid_max[2] - g.grid_min[2];
+    return 8 * (x * y + y * z + z * x) + 3 * faces;
 }
 
 } // namespace
@@ -189,7 +196,7 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     const std::vector<torch::Tensor> &vertices, const std::vector<torch::Tensor> &faces,
     const std::vector<std::vector<float>> &origins, const std::vector<std::vector<float>> &voxel_sizes,
     const std::vector<std::vector<int64_t>> &grid_ranges, float face_weight, float boundary_weight,
-    float regularization_weight, int64_t workers, int64_t order)
+    float regularization_weight, int64_t max_group_records, int64_t order)
 {
     const size_t n = vertices.size();
     TORCH_CHECK(faces.size() == n && origins.size() == n && voxel_sizes.size() == n && grid_ranges.size() == n,
@@ -198,6 +205,8 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     if (n == 0)
         return out;
     const c10::Device dev = vertices[0].device();
+    std::vector<torch::Tensor> vs(n), fs(n);
+    std::vector<ovx_fdg_mesh> meshes(n);
     for (size_t i = 0; i < n; ++i)
     {
         TORCH_CHECK(vertices[i].is_cuda() && faces[i].is_cuda(), "mesh ", i, ": vertices and faces must be CUDA tensors");
@@ -208,96 +217,64 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
         TORCH_CHECK(vertices[i].dim() == 2 && vertices[i].size(1) == 3, "mesh ", i, ": vertices must be [V,3]");
         TORCH_CHECK(faces[i].dim() == 2 && faces[i].size(1) == 3, "mesh ", i, ": faces must be [F,3]");
         TORCH_CHECK(origins[i].size() == 3, "mesh ", i, ": origin must have 3 elements");
+        vs[i] = vertices[i].contiguous();
+        fs[i] = faces[i].contiguous();
+        ovx_fdg_mesh &m = meshes[i];
+        m.vertices = vs[i].numel() ? vs[i].data_ptr<float>() : nullptr;
+        m.num_vertices = vs[i].size(0);
+        m.faces = fs[i].numel() ? fs[i].data_ptr() : nullptr;
+        m.face_index_bytes = fs[i].scalar_type() == torch::kInt64 ? 8 : 4;
+        m.num_faces = fs[i].size(0);
+        for (int a = 0; a < 3; ++a)
+            m.origin[a] = origins[i][a];
+        m.grid = make_grid(voxel_sizes[i], grid_ranges[i]);
     }
     const c10::cuda::CUDAGuard guard(dev);
     const int device = dev.index();
-    const int nw = (int)std::max<int64_t>(1, std::min<int64_t>(workers, (int64_t)n));
-    c10::cuda::CUDAStream caller = at::cuda::getCurrentCUDAStream(device);
-    // the workers' streams first wait for the work already queued on the caller's stream
-    cudaEvent_t ready;
-    TORCH_CHECK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) == cudaSuccess, "cudaEventCreate failed");
-    cudaEventRecord(ready, caller.stream());
-    std::atomic<size_t> next{0};
-    std::atomic<bool> failed{false};
-    std::mutex err_mu;
-    std::string err;
-    std::vector<c10::cuda::CUDAStream> streams;
-    for (int w = 0; w < nw; ++w)
-        streams.push_back(c10::cuda::getStreamFromPool(false, device));
-    auto work = [&](int w) {
-        try
-        {
-            const c10::cuda::CUDAGuard g(dev);
-            const c10::cuda::CUDAStreamGuard sg(streams[w]);
-            cudaStream_t st = streams[w].stream();
-            cudaStreamWaitEvent(st, ready, 0);
-            DeviceContext &dc = worker_context(device, w);
-            std::lock_guard<std::mutex> lock(dc.mu);
-            check(ovx_fdg_set_output_order(dc.ctx, (int)order), dc.ctx, "mesh_to_flexible_dual_grid_batch (order)");
-            for (;;)
-            {
-                const size_t i = next.fetch_add(1);
-                if (i >= n || failed.load())
-                    break;
-                const ovx_fdg_grid grid = make_grid(voxel_sizes[i], grid_ranges[i]);
-                auto v = vertices[i].contiguous();
-                auto f = faces[i].contiguous();
-                const float o[3] = {origins[i][0], origins[i][1], origins[i][2]};
-                int64_t nv = 0;
-                check(ovx_fdg_begin(dc.ctx, st, v.data_ptr<float>(), v.size(0), f.numel() ? f.data_ptr() : nullptr,
-                                    f.scalar_type() == torch::kInt64 ? 8 : 4, f.size(0), o, &grid, face_weight,
-                                    boundary_weight, regularization_weight, &nv),
-                      dc.ctx, "mesh_to_flexible_dual_grid_batch (occupancy)");
-                // The outputs belong to the caller's stream, so that the caching
-                // allocator reuses their blocks from one call to the next (the
-                // pool hands out other worker streams each call); the worker
-                // stream that writes them is recorded on them.  Blocks the caller
-                // freed earlier are safe here: this stream waited for the caller.
-                torch::Tensor vox, dual, inter;
-                {
-                    const c10::cuda::CUDAStreamGuard cg(caller);
-                    auto opts = torch::TensorOptions().device(dev);
-                    vox = torch::empty({nv, 3}, opts.dtype(torch::kInt32));
-                    dual = torch::empty({nv, 3}, opts.dtype(torch::kFloat32));
-                    inter = torch::empty({nv, 3}, opts.dtype(torch::kBool));
-                }
-                check(ovx_fdg_finish(dc.ctx, st, nv ? vox.data_ptr<int32_t>() : nullptr, nv ? dual.data_ptr<float>() : nullptr,
-                                     nv ? reinterpret_cast<uint8_t *>(inter.data_ptr<bool>()) : nullptr),
-                      dc.ctx, "mesh_to_flexible_dual_grid_batch (quadrics)");
-                vox.record_stream(streams[w]);
-                dual.record_stream(streams[w]);
-                inter.record_stream(streams[w]);
-                out[i] = std::make_tuple(vox, dual, inter);
-            }
-            static const bool sync_check = std::getenv("OVX_FDG_CHECK") != nullptr;
-            if (sync_check)
-                check(ovx_fdg_sync_status(dc.ctx, st), dc.ctx, "mesh_to_flexible_dual_grid_batch (device checks)");
-        }
-        catch (const std::exception &e)
-        {
-            failed.store(true);
-            std::lock_guard<std::mutex> lock(err_mu);
-            if (err.empty())
-                err = e.what();
-        }
-    };
-    std::vector<std::thread> pool;
-    for (int w = 1; w < nw; ++w)
-        pool.emplace_back(work, w);
-    work(0);
-    for (auto &t : pool)
-        t.join();
-    // the caller's stream waits for every worker's queued work
-    for (int w = 0; w < nw; ++w)
+    cudaStream_t stream = at::cuda::getCurrentCUDAStream(device).stream();
+    DeviceContext &dc = batch_context(device);
+    std::lock_guard<std::mutex> lock(dc.mu);
+    check(ovx_fdg_set_output_order(dc.ctx, (int)order), dc.ctx, "mesh_to_flexible_dual_grid_batch (order)");
+    static const bool sync_check = std::getenv("OVX_FDG_CHECK") != nullptr;
+    auto opts = torch::TensorOptions().device(dev);
+    // groups of consecutive meshes whose expected records stay within the
+    // budget: one conversion (one host synchronisation) per group
+    size_t first = 0;
+    while (first < n)
     {
-        cudaEvent_t done;
-        cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
-        cudaEventRecord(done, streams[w].stream());
-        cudaStreamWaitEvent(caller.stream(), done, 0);
-        cudaEventDestroy(done);
+        size_t last = first + 1;
+        int64_t est = estimated_records(meshes[first].grid, meshes[first].num_faces);
+        while (last < n)
+        {
+            const int64_t e = estimated_records(meshes[last].grid, meshes[last].num_faces);
+            if (max_group_records > 0 && est + e > max_group_records)
+                break;
+            est += e;
+            ++last;
+        }
+        const int32_t gm = (int32_t)(last - first);
+        std::vector<int64_t> nvox((size_t)gm);
+        int64_t total = 0;
+        check(ovx_fdg_begin_batch(dc.ctx, stream, meshes.data() + first, gm, face_weight, boundary_weight, regularization_weight,
+                                  nvox.data(), &total),
+              dc.ctx, "mesh_to_flexible_dual_grid_batch (occupancy)");
+        auto vox = torch::empty({total, 3}, opts.dtype(torch::kInt32));
+        auto dual = torch::empty({total, 3}, opts.dtype(torch::kFloat32));
+        auto inter = torch::empty({total, 3}, opts.dtype(torch::kBool));
+        check(ovx_fdg_finish_batch(dc.ctx, stream, total ? vox.data_ptr<int32_t>() : nullptr, total ? dual.data_ptr<float>() : nullptr,
+                                   total ? reinterpret_cast<uint8_t *>(inter.data_ptr<bool>()) : nullptr),
+              dc.ctx, "mesh_to_flexible_dual_grid_batch (quadrics)");
+        if (sync_check)
+            check(ovx_fdg_sync_status(dc.ctx, stream), dc.ctx, "mesh_to_flexible_dual_grid_batch (device checks)");
+        int64_t row = 0;
+        for (int32_t k = 0; k < gm; ++k)
+        {
+            const int64_t r = nvox[(size_t)k];
+            out[first + (size_t)k] = std::make_tuple(vox.narrow(0, row, r), dual.narrow(0, row, r), inter.narrow(0, row, r));
+            row += r;
+        }
+        first = last;
     }
-    cudaEventDestroy(ready);
-    TORCH_CHECK(!failed.load(), err);
     return out;
 }
 
@@ -447,7 +424,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
           py::arg("order") = 0, py::call_guard<py::gil_scoped_release>());
     m.def("mesh_to_flexible_dual_grid_cuda_batch", &mesh_to_flexible_dual_grid_cuda_batch, py::arg("vertices"),
           py::arg("faces"), py::arg("origins"), py::arg("voxel_sizes"), py::arg("grid_ranges"), py::arg("face_weight"),
-          py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("workers"), py::arg("order") = 0,
+          py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("max_group_records"), py::arg("order") = 0,
           py::call_guard<py::gil_scoped_release>());
     m.def("z_order_encode_cuda", &z_order_encode_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("flexible_dual_grid_to_mesh_cuda", &flexible_dual_grid_to_mesh_cuda, py::call_guard<py::gil_scoped_release>());

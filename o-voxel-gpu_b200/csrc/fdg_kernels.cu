@@ -20,12 +20,9 @@
 //             boundary {e, 2<<30 | local voxel, 0}, e = index in the
 //                      boundary edge list, which is sorted by (v_min, v_max)
 //   qtab    plane quadric per triangle (10 floats)
-//   contrib per-voxel contribution lists of the bricks whose lists do not fit
-//           in shared memory, 16 B entries; brick b owns entries
+//   contrib per-voxel contribution lists, 16 B entries; brick b owns entries
 //           [4*roff[b], 4*roff[b+1]) (a record yields at most 4 contributions)
-//   vlist   per output row: first entry (40 bits) | entry count << 40, or 0
-//           for a row summed in brick_lists
-//   qreg    regularised quadric (10 floats) of each row summed in brick_lists
+//   vlist   per output row: first entry (40 bits) | entry count << 40 | sorted << 63
 //   estage, fstage  event and face records staged by the count pass (16 B,
 //           {brick, t, code, z} and {brick, t, code, rank in the brick})
 //   btab    line quadric per boundary edge (10 floats)
@@ -52,14 +49,12 @@
 //   boundary_records<FILL>
 //   brick_lists         one CTA per active brick: records -> per-voxel
 //                       contribution lists {key, payload} (a counting sort by
-//                       voxel).  When the brick's lists fit in shared memory
-//                       they are ordered there by key and each voxel's list is
-//                       summed sequentially in FP32 in that order (bit-identical
-//                       to the reference CPU sums) and regularised; otherwise
-//                       the lists go to global memory
-//   voxel_accumulate    one thread per voxel: solves the rows summed in
-//                       brick_lists; sorts, sums and regularises the others'
-//                       global lists first; CPQR solve
+//                       voxel), staged and the short ones sorted in shared
+//                       memory when the brick's lists fit there
+//   voxel_accumulate    one thread per voxel: sorts its list by key unless it is
+//                       marked sorted, sums it sequentially in FP32 in that order
+//                       (bit-identical to the reference CPU sums), regularises,
+//                       CPQR-solves
 //   constrained_solve   box-constrained search for the few voxels whose
 //                       unconstrained solution leaves the voxel
 //
@@ -80,6 +75,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 using namespace ovx;
 
@@ -91,15 +87,13 @@ constexpr int kUnitCells = 64;        // cells per unit of work of a large (tria
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
 constexpr int kListStage = 768; // contributions of a brick that brick_lists stages (and sorts) in shared memory
-// vlist word: first entry (bits 0-39) | count (bits 40-62); 0 for a row that
-// brick_lists summed (every active voxel has at least one contribution)
+// vlist word: first entry (bits 0-39) | count (bits 40-62) | sorted flag (bit 63)
 constexpr uint32_t kListCountMax = (1u << 23) - 1u;
+constexpr unsigned long long kListSorted = 1ull << 63;
 #ifndef OVX_FDG_WARP_SORT_MIN
 #define OVX_FDG_WARP_SORT_MIN 16
 #endif
 constexpr int kWarpSortMin = OVX_FDG_WARP_SORT_MIN; // lists this long or longer are ordered by the whole warp
-constexpr int kWarpSortPer = 2;                      // ... up to 2 entries per lane
-constexpr int kWarpSortMax = 32 * kWarpSortPer;      // longer lists go to voxel_accumulate_long
 
 // device counter words
 enum
@@ -150,6 +144,10 @@ __device__ __forceinline__ void place(int ax2, int u, int v, int w, int &x, int 
     z = ax2 == 0 ? v : (ax2 == 1 ? u : w);
 }
 
+// One mesh of a conversion.  A batched conversion lays its meshes' triangles,
+// bricks and vertices out one mesh after another in global index spaces; a
+// mesh's entries there start at tri0, brick0 and vert0 (all 0 for a single
+// mesh), and its output rows at row0.
 struct Mesh
 {
     Grid g;
@@ -158,6 +156,8 @@ struct Mesh
     const void *faces; // NULL: triangle soup, vertex 3t+k
     long long nf;
     float ox, oy, oz;
+    int fbytes; // bytes per face index (4 or 8)
+    long long tri0, brick0, vert0, row0;
 };
 
 template <typename IdxT>
@@ -166,6 +166,81 @@ __device__ __forceinline__ bool tri_load(const Mesh &M, long long t, float v[3][
     long long idx[3];
     const float o[3] = {M.ox, M.oy, M.oz};
     return load_triangle<IdxT>(M.verts, M.nv, (const IdxT *)M.faces, t, o, v, idx);
+}
+
+// Triangle t (local to its mesh): single conversions know the face index type
+// at compile time; batched ones read it from the mesh.
+template <bool B, typename IdxT>
+__device__ __forceinline__ bool tri_load_m(const Mesh &M, long long t, float v[3][3])
+{
+    if constexpr (B)
+        return M.fbytes == 8 ? tri_load<long long>(M, t, v) : tri_load<int>(M, t, v);
+    else
+        return tri_load<IdxT>(M, t, v);
+}
+
+// Mesh of a global index: the last of the n meshes whose first index
+// first(i) is at most x (first is non-decreasing).
+template <typename First>
+__device__ __forceinline__ int seg_find(int n, long long x, First first)
+{
+    int lo = 0, hi = n;
+    while (hi - lo > 1)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (first(mid) <= x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// The mesh of a conversion: the single mesh in the kernel's parameters, or
+// mesh s of a batch's table in global memory.
+template <bool B, typename Args>
+__device__ __forceinline__ const Mesh &mesh_of(const Args &A, int s)
+{
+    if constexpr (B)
+        return A.segs[s];
+    else
+        return A.m;
+}
+
+template <bool B, typename Args>
+__device__ __forceinline__ int seg_of_tri(const Args &A, long long t)
+{
+    if constexpr (B)
+        return seg_find(A.nseg, t, [&](int i) { return A.segs[i].tri0; });
+    else
+        return 0;
+}
+
+template <bool B, typename Args>
+__device__ __forceinline__ int seg_of_brick(const Args &A, long long b)
+{
+    if constexpr (B)
+        return seg_find(A.nseg, b, [&](int i) { return A.segs[i].brick0; });
+    else
+        return 0;
+}
+
+template <bool B, typename Args>
+__device__ __forceinline__ int seg_of_vert(const Args &A, long long v)
+{
+    if constexpr (B)
+        return seg_find(A.nseg, v, [&](int i) { return A.segs[i].vert0; });
+    else
+        return 0;
+}
+
+template <bool B, typename Args>
+__device__ __forceinline__ int seg_of_row(const Args &A, long long r)
+{
+    if constexpr (B)
+        return seg_find(A.nseg, r, [&](int i) { return A.segs[i].row0; });
+    else
+        return 0;
 }
 
 __device__ __forceinline__ void vertex_load(const Mesh &M, long long i, float p[3])
@@ -224,6 +299,8 @@ __device__ __forceinline__ void brick_origin(const Grid &g, long long b, int o[3
 struct GenArgs
 {
     Mesh m;
+    const Mesh *segs; // batched conversions: the meshes (global memory)
+    int nseg;
     uint32_t *bits;
     uint32_t *rcnt;                 // records per brick (COUNT) / cursor (FILL)
     const unsigned long long *roff; // FILL
@@ -312,12 +389,14 @@ template <int M>
 struct EventSink
 {
     const GenArgs &A;
-    uint32_t t;
+    const Mesh &Ms; // the triangle's mesh (its grid, bitmap and first brick)
+    uint32_t t;     // global triangle index
     int ax2;
     EventStage *es = nullptr;
     __device__ __forceinline__ void operator()(int xi, int yi, int zi, float, float, double z) const
     {
-        const Grid &g = A.m.g;
+        const Grid &g = Ms.g;
+        uint32_t *const bits = A.bits + Ms.brick0 * kWordsPerBrick;
         long long w[4];
         uint32_t m[4];
 #pragma unroll
@@ -345,7 +424,7 @@ struct EventSink
                 for (int j = k + 1; j < 4; ++j)
                     if (w[j] == w[k])
                         mk |= m[j];
-                atomicOr(&A.bits[w[k]], mk);
+                atomicOr(&bits[w[k]], mk);
             }
         }
         const uint32_t zb = __float_as_uint((float)z);
@@ -371,10 +450,10 @@ struct EventSink
                 code = (uint32_t)ax2 | ((uint32_t)(xi - o0 + 1) << 2) | ((uint32_t)(yi - o1 + 1) << 6) |
                        ((uint32_t)(zi - o2) << 10);
             }
-            put_record<M>(A, b, t, code, zb);
+            put_record<M>(A, Ms.brick0 + b, t, code, zb);
             if (M == COUNT && es)
             {
-                es->b[es->n] = (uint32_t)b;
+                es->b[es->n] = (uint32_t)(Ms.brick0 + b);
                 es->code[es->n] = code;
                 ++es->n;
             }
@@ -393,7 +472,8 @@ constexpr int kWarpScanWork = 256;   // (triangle, axis) pairs with more row x c
 struct EventWarp
 {
     double t[3][3][32]; // sorted vertices (projection coordinates) of each lane's (triangle, axis)
-    long long ta[32];   // each lane's pair: 3 * triangle + axis
+    long long ta[32];   // each lane's pair: 3 * triangle + axis (global triangle index)
+    int seg[32];        // each lane's mesh (batched conversions)
     int start[32], mid[32]; // first row of the lane's rows, and the row where the second edge pair starts
     int clo[32], chi[32];   // columns of the lane's rows: [clo, chi)
 };
@@ -447,10 +527,9 @@ __device__ __forceinline__ LargeSplit large_split(int cols)
 // those rows again 32 at a time, so the FP64 event arithmetic runs on full
 // warps whatever the pairs' sizes.  COUNT marks the occupancy bits, counts
 // event records per brick and stages them; FILL writes the records.
-template <int M>
+template <int M, bool B>
 __device__ __forceinline__ void event_rows(const GenArgs &A, EventWarp &E, const int lane, const uint32_t nrows)
 {
-    const Grid &g = A.m.g;
     uint32_t nrow_all;
     const uint32_t rstart = warp_exclusive_scan(nrows, nrow_all);
     __syncwarp();
@@ -480,7 +559,8 @@ __device__ __forceinline__ void event_rows(const GenArgs &A, EventWarp &E, const
             s.ax0 = (oax2 + 1) % 3;
             s.ax1 = (oax2 + 2) % 3;
             yi = s.start + (int)(r - ors);
-            row_setup(s, yi, E.clo[ol], E.chi[ol], g, rs);
+            const Mesh &Mo = mesh_of<B>(A, B ? E.seg[ol] : 0);
+            row_setup(s, yi, E.clo[ol], E.chi[ol], Mo.g, rs);
         }
         const uint32_t ncol = rs.x1 > rs.x0 ? (uint32_t)(rs.x1 - rs.x0) : 0u;
         uint32_t ncol_all;
@@ -507,12 +587,14 @@ __device__ __forceinline__ void event_rows(const GenArgs &A, EventWarp &E, const
                 const long long cta = E.ta[col];
                 const int cax2 = (int)(cta % 3);
                 const int xi = cr.x0 + (int)(c - ccs);
+                const Mesh &Mc = mesh_of<B>(A, B ? E.seg[col] : 0);
+                const Grid &g = Mc.g;
                 double z;
                 int zi;
                 col_event(cr, xi, (cax2 + 1) % 3, cax2, g, z, zi);
                 if (zi >= g.gmin[cax2] && zi < g.gmax[cax2])
                 {
-                    EventSink<M> sink{A, (uint32_t)(cta / 3), cax2, (M == COUNT && A.estage) ? &es : nullptr};
+                    EventSink<M> sink{A, Mc, (uint32_t)(cta / 3), cax2, (M == COUNT && A.estage) ? &es : nullptr};
                     sink(xi, cyi, zi, 0.0f, 0.0f, z);
                 }
             }
@@ -544,21 +626,23 @@ __device__ __forceinline__ void event_rows(const GenArgs &A, EventWarp &E, const
 // event arithmetic runs on full warps whatever the triangles' sizes.  COUNT
 // marks the occupancy bits and counts event records per brick (and writes the
 // quadric table); FILL writes the records.
-template <int M, typename IdxT>
+template <int M, typename IdxT, bool B>
 __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
 {
     __shared__ EventWarp EW[kEventThreads / 32];
     const int lane = threadIdx.x & 31;
     EventWarp &E = EW[threadIdx.x >> 5];
-    const long long ta = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const Grid &g = A.m.g;
+    const long long ta = (long long)blockIdx.x * blockDim.x + threadIdx.x; // global (triangle, axis)
     uint32_t nrows = 0;
     if (ta < 3 * A.m.nf)
     {
         const long long t = ta / 3;
         const int ax2 = (int)(ta - 3 * t);
+        const int sg = seg_of_tri<B>(A, t);
+        const Mesh &Ms = mesh_of<B>(A, sg);
+        const Grid &g = Ms.g;
         float v[3][3];
-        if (!tri_load<IdxT>(A.m, t, v))
+        if (!tri_load_m<B, IdxT>(Ms, t - Ms.tri0, v))
         {
             if (M == COUNT)
                 atomicOr(&A.counters[C_STATUS], (uint32_t)ST_BAD_INDEX);
@@ -607,13 +691,14 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
                     E.clo[lane] = INT_MIN;
                     E.chi[lane] = INT_MAX;
                     E.ta[lane] = ta;
+                    E.seg[lane] = sg;
                     nrows = (uint32_t)rows;
                 }
             }
         }
     }
     __syncwarp();
-    event_rows<M>(A, E, lane, nrows);
+    event_rows<M, B>(A, E, lane, nrows);
 }
 
 // In-place exclusive scan of the unit counts of a work list (one CTA): entry i
@@ -694,7 +779,7 @@ __device__ __forceinline__ uint32_t unit_owner(const uint32_t *__restrict__ unit
 // block of rows, or a chunk of one row's columns): one unit per lane, 32 per
 // warp, the rows and column crossings of the warp's units spread over the
 // lanes as for the other pairs.
-template <int M, typename IdxT>
+template <int M, typename IdxT, bool B>
 __global__ void __launch_bounds__(kEventThreads) large_rows(GenArgs A)
 {
     __shared__ EventWarp EW[kEventThreads / 32];
@@ -714,13 +799,15 @@ __global__ void __launch_bounds__(kEventThreads) large_rows(GenArgs A)
             const uint32_t ta = A.scan_large[i];
             const long long t = ta / 3;
             const int ax2 = (int)(ta - 3 * t);
+            const int sg = seg_of_tri<B>(A, t);
+            const Mesh &Ms = mesh_of<B>(A, sg);
             float v[3][3];
-            if (tri_load<IdxT>(A.m, t, v))
+            if (tri_load_m<B, IdxT>(Ms, t - Ms.tri0, v))
             {
                 AxisScan s;
-                axis_setup(v, ax2, A.m.g, s);
+                axis_setup(v, ax2, Ms.g, s);
                 int clo, chi;
-                axis_col_bounds(s, A.m.g, clo, chi);
+                axis_col_bounds(s, Ms.g, clo, chi);
                 const LargeSplit sp = large_split(chi - clo + 1);
                 const int j = (int)((uint32_t)u - A.scan_units[i]);
                 const int ch = j % sp.nch;
@@ -738,12 +825,13 @@ __global__ void __launch_bounds__(kEventThreads) large_rows(GenArgs A)
                     E.clo[lane] = ch == 0 ? INT_MIN : clo + ch * kUnitCells;
                     E.chi[lane] = ch == sp.nch - 1 ? INT_MAX : clo + (ch + 1) * kUnitCells;
                     E.ta[lane] = ta;
+                    E.seg[lane] = sg;
                     nrows = (uint32_t)(r1 - r0);
                 }
             }
         }
         __syncwarp();
-        event_rows<M>(A, E, lane, nrows);
+        event_rows<M, B>(A, E, lane, nrows);
         __syncwarp();
     }
 }
@@ -793,7 +881,8 @@ struct FaceWarp
     uint32_t pass[kWordsPerBrick][32]; // face-test hits of each item of the current chunk
     int org[3][32];                    // brick origin of each item
     uint8_t own[32];                   // lane whose triangle an item belongs to
-    uint32_t tri[32];                  // triangle of each lane
+    uint32_t tri[32];                  // triangle of each lane (global index)
+    int seg[32];                       // mesh of each lane's triangle (batched conversions)
     uint16_t cl[kFaceWindow];          // candidate list: local voxel index
     alignas(16) uint8_t cs[kFaceWindow]; // candidate list: item slot (a dense item's 16 words while dense items run)
 };
@@ -888,8 +977,10 @@ __device__ __forceinline__ void face_hits(const GenArgs &A, const uint32_t (*pas
 // A lane's triangle in W: face-test coefficients, first brick and bricks along
 // x and y of its face box, the face box itself, the triangle index.
 __device__ __forceinline__ void face_lane_setup(FaceWarp &W, const int lane, const float v[3][3], const Grid &g, const int bmin[3],
-                                                const int bmax[3], const int b0[3], const int nx, const int ny, const uint32_t t)
+                                                const int bmax[3], const int b0[3], const int nx, const int ny, const uint32_t t,
+                                                const int sg)
 {
+    W.seg[lane] = sg;
     FaceSetup fs;
     face_setup(v, g, fs);
     float c[kFaceCoef];
@@ -910,18 +1001,19 @@ __device__ __forceinline__ void face_lane_setup(FaceWarp &W, const int lane, con
 // inside the face box) are tested on full warps: items with many of them by
 // the whole warp with the coefficients in registers, the others through a
 // shared list; then the hits become records.  Called by all lanes.
-template <int M>
+template <int M, bool B>
 __device__ __forceinline__ void face_item(const GenArgs &A, FaceWarp &W, const int lane, const bool valid, const int ol, const int r)
 {
-    const Grid &g = A.m.g;
     uint32_t cw[kWordsPerBrick];
     uint32_t cnt = 0;
-    long long b = 0;
+    long long b = 0; // global brick of this lane's item
     if (valid)
     {
+        const Mesh &Mi = mesh_of<B>(A, B ? W.seg[ol] : 0);
+        const Grid &g = Mi.g;
         const int nx = W.info[3][ol], ny = W.info[4][ol];
         const int bx = W.info[0][ol] + r % nx, by = W.info[1][ol] + (r / nx) % ny, bz = W.info[2][ol] + r / (nx * ny);
-        b = (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
+        b = Mi.brick0 + (long long)bx + (long long)g.nb[0] * ((long long)by + (long long)g.nb[1] * (long long)bz);
         const int o[3] = {g.gmin[0] + bx * kBrick, g.gmin[1] + by * kBrick, g.gmin[2] + bz * kBrick};
         const int bmin[3] = {W.info[5][ol], W.info[6][ol], W.info[7][ol]};
         const int bmax[3] = {W.info[8][ol], W.info[9][ol], W.info[10][ol]};
@@ -992,10 +1084,11 @@ __device__ __forceinline__ void face_item(const GenArgs &A, FaceWarp &W, const i
         }
         __syncwarp();
         const int ox = W.org[0][sd], oy = W.org[1][sd], oz = W.org[2][sd];
+        const Grid &gd = mesh_of<B>(A, B ? W.seg[so] : 0).g;
         for (uint32_t k = lane; k < ntot; k += 32)
         {
             const int lv = W.cl[k];
-            if (face_test_c(FaceCoefArr{c}, g, ox + (lv & 7), oy + ((lv >> 3) & 7), oz + (lv >> 6)))
+            if (face_test_c(FaceCoefArr{c}, gd, ox + (lv & 7), oy + ((lv >> 3) & 7), oz + (lv >> 6)))
                 atomicOr(&W.pass[lv >> 5][sd], 1u << (lv & 31));
         }
         __syncwarp();
@@ -1041,7 +1134,8 @@ __device__ __forceinline__ void face_item(const GenArgs &A, FaceWarp &W, const i
         {
             const int lv = W.cl[k], sl = W.cs[k];
             const int x = W.org[0][sl] + (lv & 7), y = W.org[1][sl] + ((lv >> 3) & 7), z = W.org[2][sl] + (lv >> 6);
-            if (face_test_c(FaceCoefSmem{&W.coef[0][W.own[sl]]}, g, x, y, z))
+            const Grid &gl = mesh_of<B>(A, B ? W.seg[W.own[sl]] : 0).g;
+            if (face_test_c(FaceCoefSmem{&W.coef[0][W.own[sl]]}, gl, x, y, z))
                 atomicOr(&W.pass[lv >> 5][sl], 1u << (lv & 31));
         }
         __syncwarp();
@@ -1062,19 +1156,21 @@ __device__ __forceinline__ void face_item(const GenArgs &A, FaceWarp &W, const i
 // listed in shared memory and tested by all 32 lanes, so the face tests run on
 // full warps whatever the triangles' sizes.  COUNT adds each item's hits to its
 // brick's record count; FILL writes one record per hit.
-template <int M, typename IdxT>
+template <int M, typename IdxT, bool B>
 __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
 {
     __shared__ FaceWarp FW[kFaceThreads / 32];
     const int lane = threadIdx.x & 31;
     FaceWarp &W = FW[threadIdx.x >> 5];
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const Grid &g = A.m.g;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; // global triangle
     int nbk = 0;
     if (t < A.m.nf)
     {
+        const int sg = seg_of_tri<B>(A, t);
+        const Mesh &Ms = mesh_of<B>(A, sg);
+        const Grid &g = Ms.g;
         float v[3][3];
-        if (tri_load<IdxT>(A.m, t, v))
+        if (tri_load_m<B, IdxT>(Ms, t - Ms.tri0, v))
         {
             int bmin[3], bmax[3];
             face_box(v, g, bmin, bmax);
@@ -1105,7 +1201,7 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
                 }
                 else
                 {
-                    face_lane_setup(W, lane, v, g, bmin, bmax, b0, nx, ny, (uint32_t)t);
+                    face_lane_setup(W, lane, v, g, bmin, bmax, b0, nx, ny, (uint32_t)t, sg);
                     nbk = (int)n;
                 }
             }
@@ -1139,7 +1235,7 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
         }
         const int ol = lo_l;
         const int r = it - __shfl_sync(0xffffffffu, istart, ol);
-        face_item<M>(A, W, lane, it < nitems, ol, r);
+        face_item<M, B>(A, W, lane, it < nitems, ol, r);
         __syncwarp();
     }
 }
@@ -1172,13 +1268,12 @@ __global__ void __launch_bounds__(kThreads) bucket_records(const uint4 *__restri
 // (triangle, brick) items, all listed triangles' items one after another, 32
 // per warp and round, one per lane; each lane sets up its own item's triangle
 // and the round runs as in face_records.
-template <int M, typename IdxT>
+template <int M, typename IdxT, bool B>
 __global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
 {
     __shared__ FaceWarp FW[kFaceThreads / 32];
     const int lane = threadIdx.x & 31;
     FaceWarp &W = FW[threadIdx.x >> 5];
-    const Grid &g = A.m.g;
     const uint32_t n = min(A.counters[C_FACE_LARGE], A.face_large_cap);
     const uint32_t total = A.counters[C_FUNITS];
     const int wpb = blockDim.x >> 5;
@@ -1193,8 +1288,11 @@ __global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
             const uint32_t i = unit_owner(A.face_units, n, (uint32_t)u);
             const uint32_t t = A.face_large[i];
             r = (int)((uint32_t)u - A.face_units[i]);
+            const int sg = seg_of_tri<B>(A, t);
+            const Mesh &Ms = mesh_of<B>(A, sg);
+            const Grid &g = Ms.g;
             float v[3][3];
-            if (tri_load<IdxT>(A.m, t, v))
+            if (tri_load_m<B, IdxT>(Ms, t - Ms.tri0, v))
             {
                 int bmin[3], bmax[3];
                 face_box(v, g, bmin, bmax);
@@ -1205,12 +1303,12 @@ __global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
                     b0[a] = (bmin[a] - g.gmin[a]) >> 3;
                     b1[a] = (bmax[a] - 1 - g.gmin[a]) >> 3;
                 }
-                face_lane_setup(W, lane, v, g, bmin, bmax, b0, b1[0] - b0[0] + 1, b1[1] - b0[1] + 1, t);
+                face_lane_setup(W, lane, v, g, bmin, bmax, b0, b1[0] - b0[0] + 1, b1[1] - b0[1] + 1, t, sg);
                 valid = true;
             }
         }
         __syncwarp();
-        face_item<M>(A, W, lane, valid, lane, r);
+        face_item<M, B>(A, W, lane, valid, lane, r);
         __syncwarp();
     }
 }
@@ -1252,18 +1350,20 @@ constexpr int kLongWalk = 64; // boundary edges with a longer step bound are wal
 // voxel visited.  Edges whose walk may take more than kLongWalk steps are
 // listed (COUNT) and left to boundary_long; FILL writes every edge's line
 // quadric here.
-template <int M>
+template <int M, bool B>
 __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
 {
     const uint32_t n = min(A.counters[C_BOUNDARY], A.bkeys_cap);
-    const Grid &g = A.m.g;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
         const unsigned long long e = A.bkeys[i];
-        const uint32_t ia = (uint32_t)(e >> 32), ib = (uint32_t)(e & 0xffffffffull);
+        const uint32_t ia = (uint32_t)(e >> 32), ib = (uint32_t)(e & 0xffffffffull); // global vertex indices
+        const Mesh &Ms = mesh_of<B>(A, seg_of_vert<B>(A, ia));
+        const Grid &g = Ms.g;
+        const uint32_t *bits = A.bits + Ms.brick0 * kWordsPerBrick;
         float v0[3], v1[3];
-        vertex_load(A.m, ia, v0);
-        vertex_load(A.m, ib, v1);
+        vertex_load(Ms, ia - Ms.vert0, v0);
+        vertex_load(Ms, ib - Ms.vert0, v1);
         Dda d;
         if (!boundary_setup(v0, v1, g, d, M == FILL ? A.btab + (size_t)i * 10 : nullptr))
             continue;
@@ -1285,8 +1385,8 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
             {
                 uint32_t bit;
                 const long long w = voxel_word(g, d.cur[0], d.cur[1], d.cur[2], bit);
-                if (A.bits[w] & (1u << bit))
-                    put_record<M>(A, w >> 4, i, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), 0u);
+                if (bits[w] & (1u << bit))
+                    put_record<M>(A, Ms.brick0 + (w >> 4), i, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), 0u);
             }
             if (!dda_step(d))
                 break;
@@ -1299,21 +1399,23 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
 // The listed long boundary edges, one warp each.  Every lane runs the same
 // DDA walk (the steps are cheap arithmetic); lane k visits steps k, k + 32,
 // ..., so the occupancy lookups and records of 32 steps go out together.
-template <int M>
+template <int M, bool B>
 __global__ void __launch_bounds__(kThreads) boundary_long(GenArgs A)
 {
     const uint32_t n = min(A.counters[C_BLONG], A.blong_cap);
-    const Grid &g = A.m.g;
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x >> 5;
     for (uint32_t j = blockIdx.x * wpb + (threadIdx.x >> 5); j < n; j += gridDim.x * wpb)
     {
         const uint32_t i = A.blong[j];
         const unsigned long long e = A.bkeys[i];
-        const uint32_t ia = (uint32_t)(e >> 32), ib = (uint32_t)(e & 0xffffffffull);
+        const uint32_t ia = (uint32_t)(e >> 32), ib = (uint32_t)(e & 0xffffffffull); // global vertex indices
+        const Mesh &Ms = mesh_of<B>(A, seg_of_vert<B>(A, ia));
+        const Grid &g = Ms.g;
+        const uint32_t *bits = A.bits + Ms.brick0 * kWordsPerBrick;
         float v0[3], v1[3];
-        vertex_load(A.m, ia, v0);
-        vertex_load(A.m, ib, v1);
+        vertex_load(Ms, ia - Ms.vert0, v0);
+        vertex_load(Ms, ib - Ms.vert0, v1);
         Dda d;
         if (!boundary_setup(v0, v1, g, d, nullptr))
             continue; // the same edge for the whole warp
@@ -1337,8 +1439,8 @@ __global__ void __launch_bounds__(kThreads) boundary_long(GenArgs A)
             {
                 uint32_t bit;
                 const long long w = voxel_word(g, c[0], c[1], c[2], bit);
-                if (A.bits[w] & (1u << bit))
-                    put_record<M>(A, w >> 4, i, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), 0u);
+                if (bits[w] & (1u << bit))
+                    put_record<M>(A, Ms.brick0 + (w >> 4), i, kRecBoundary | (uint32_t)((w & 15) * 32 + bit), 0u);
             }
         }
         if (M == COUNT && lane == 0 && d.guard < 0)
@@ -1423,6 +1525,52 @@ __global__ void edge_fill(const IdxT *__restrict__ faces, long long nf, long lon
             const uint32_t left = atomicSub(&vcnt[a], 1u);
             if (left == 0u)
                 continue; // cannot happen: same faces as edge_count
+            emax[voff[a] + (unsigned long long)(left - 1u)] = b;
+        }
+    }
+}
+
+// Edge k of global face f of a batched conversion, as global vertex indices.
+__device__ __forceinline__ bool batch_face_edge(const Mesh *__restrict__ segs, int nseg, long long f, int k, uint32_t &a, uint32_t &b)
+{
+    const Mesh &M = segs[seg_find(nseg, f, [&](int i) { return segs[i].tri0; })];
+    const long long fl = f - M.tri0;
+    const bool ok = M.fbytes == 8 ? face_edge((const long long *)M.faces, M.nv, fl, k, a, b)
+                                  : face_edge((const int *)M.faces, M.nv, fl, k, a, b);
+    a += (uint32_t)M.vert0;
+    b += (uint32_t)M.vert0;
+    return ok;
+}
+
+__global__ void edge_count_batch(const Mesh *__restrict__ segs, int nseg, long long nf, uint32_t *__restrict__ vcnt)
+{
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf)
+        return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        uint32_t a, b;
+        if (batch_face_edge(segs, nseg, f, k, a, b))
+            atomicAdd(&vcnt[a], 1u);
+    }
+}
+
+__global__ void edge_fill_batch(const Mesh *__restrict__ segs, int nseg, long long nf, const unsigned long long *__restrict__ voff,
+                                uint32_t *__restrict__ vcnt, uint32_t *__restrict__ emax)
+{
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf)
+        return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        uint32_t a, b;
+        if (batch_face_edge(segs, nseg, f, k, a, b))
+        {
+            const uint32_t left = atomicSub(&vcnt[a], 1u);
+            if (left == 0u)
+                continue; // cannot happen: same faces as edge_count_batch
             emax[voff[a] + (unsigned long long)(left - 1u)] = b;
         }
     }
@@ -1532,6 +1680,8 @@ __global__ void edge_emit(const unsigned long long *__restrict__ voff, const uin
 struct SolveArgs
 {
     Mesh m;
+    const Mesh *segs; // batched conversions: the meshes (global memory)
+    int nseg;
     float bw, rw;
     const uint32_t *bits;
     const unsigned long long *bbase;
@@ -1549,9 +1699,7 @@ struct SolveArgs
     uint32_t *longv;            // rows whose lists are too long for voxel_accumulate: up to kLongMidMax
                                 // entries from the front (counter C_LONG), longer ones from the back (C_HUGE)
     uint32_t longv_cap;
-    unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40;
-                                // 0: the row was summed by brick_lists and its quadric is in qreg
-    float *qreg;                // regularised quadric (10 floats) of the rows brick_lists summed
+    unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40 | sorted << 63
     float *clist; // deferred constrained searches, 16 words each
     uint32_t clist_cap;
 };
@@ -1667,7 +1815,8 @@ struct Contrib
     unsigned stage;
 };
 
-__device__ __forceinline__ void contrib_load(const SolveArgs &A, const int vc[3], unsigned long long key, uint32_t pay, Contrib &c)
+__device__ __forceinline__ void contrib_load(const SolveArgs &A, const Grid &g, const int vc[3], unsigned long long key, uint32_t pay,
+                                             Contrib &c)
 {
     c.stage = (unsigned)(key >> 62);
     c.flag = 0u;
@@ -1681,7 +1830,6 @@ __device__ __forceinline__ void contrib_load(const SolveArgs &A, const int vc[3]
         const int ax0 = (ax2 + 1) % 3, ax1 = (ax2 + 2) % 3;
         const int c0 = ax0 == 0 ? vc[0] : (ax0 == 1 ? vc[1] : vc[2]);
         const int c1 = ax1 == 0 ? vc[0] : (ax1 == 1 ? vc[1] : vc[2]);
-        const Grid &g = A.m.g;
         const float vs0 = ax0 == 0 ? g.vs[0] : (ax0 == 1 ? g.vs[1] : g.vs[2]);
         const float vs1 = ax1 == 0 ? g.vs[0] : (ax1 == 1 ? g.vs[1] : g.vs[2]);
         const float pu = (float)(c0 - dx + 1) * vs0;
@@ -1773,9 +1921,8 @@ struct ListShared
     uint32_t scan_tmp[kConsumeThreads / 32 + 1]; // per-warp offsets, then the brick's total
     int nvox;
     uint32_t status;
-    uint32_t longest; // the brick's longest list
     // the brick's lists, when they fit (keys and payloads apart: 12 bytes an
-    // entry): filled, ordered by key and summed in place
+    // entry): filled, short lists sorted, copied out
     unsigned long long skey[kListStage];
     uint32_t spay[kListStage];
 };
@@ -1825,39 +1972,23 @@ struct ListStageFill
     }
 };
 
-// A voxel summed in brick_lists: its intersected flags go straight to the
-// output, its regularised quadric (flexible_dual_grid.cpp:780-792) to qreg for
-// the solve.
-__device__ __forceinline__ void voxel_sum_out(const SolveArgs &A, long long row, const Acc &a)
-{
-    float q[10];
-    regularize(a.q, a.mean, a.cnt, A.rw, q);
-    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
-    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
-    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
-    float *d = A.qreg + row * 10;
-#pragma unroll
-    for (int i = 0; i < 10; ++i)
-        d[i] = q[i];
-}
-
+template <bool B>
 __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
 {
     __shared__ ListShared S;
     const int tid = threadIdx.x;
-    const Grid &g = A.m.g;
-    const long long b = A.active[blockIdx.x];
+    const long long b = A.active[blockIdx.x]; // global brick
     int o[3];
-    brick_origin(g, b, o);
+    {
+        const Mesh &Ms = mesh_of<B>(A, seg_of_brick<B>(A, b));
+        brick_origin(Ms.g, b - Ms.brick0, o);
+    }
     const Rec *rec = A.rec + A.roff[b];
     const unsigned long long nrec = A.roff[b + 1] - A.roff[b];
     for (int i = tid; i < 512; i += blockDim.x)
         S.cnt[i] = 0;
     if (tid == 0)
-    {
         S.status = 0;
-        S.longest = 0;
-    }
     load_brick_ranks(S, A.bits, b, A.zorder);
     const int nvox = S.nvox;
     const unsigned long long vbase = A.bbase[b];
@@ -1882,17 +2013,14 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     {
         const int lane = tid & 31, warp = tid >> 5;
         constexpr int per = 512 / kConsumeThreads;
-        uint32_t v[per], sum = 0, mx = 0;
+        uint32_t v[per], sum = 0;
 #pragma unroll
         for (int k = 0; k < per; ++k)
         {
             const int j = tid * per + k;
             v[k] = j < nvox ? S.cnt[j] : 0u;
             sum += v[k];
-            mx = v[k] > mx ? v[k] : mx;
         }
-        if (mx > (uint32_t)kWarpSortMax)
-            atomicMax(&S.longest, mx);
         uint32_t incl = sum;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1)
@@ -1916,9 +2044,7 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
             S.scan_tmp[kConsumeThreads / 32] = r;
         }
         __syncthreads();
-        // the brick is summed here when its lists fit in shared memory and
-        // none is too long for a warp to order
-        const bool fused = S.scan_tmp[kConsumeThreads / 32] <= (uint32_t)kListStage && S.longest == 0u;
+        const bool staged = S.scan_tmp[kConsumeThreads / 32] <= (uint32_t)kListStage;
         uint32_t run = S.scan_tmp[warp] + incl - sum;
         const unsigned long long first = 4ull * A.roff[b];
 #pragma unroll
@@ -1929,7 +2055,8 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
             {
                 if (v[k] == 0u || v[k] > kListCountMax)
                     atomicOr(&S.status, (uint32_t)ST_REPLAY); // every active voxel has a scanline contribution
-                A.vlist[vbase + j] = fused ? 0ull : (first + run) | ((unsigned long long)v[k] << 40);
+                const bool sorted = staged && v[k] < (uint32_t)kWarpSortMin;
+                A.vlist[vbase + j] = (first + run) | ((unsigned long long)v[k] << 40) | (sorted ? kListSorted : 0ull);
             }
             S.off[j] = run;
             run += v[k];
@@ -1938,12 +2065,10 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     __syncthreads();
     const uint32_t total = S.scan_tmp[kConsumeThreads / 32];
     uint4 *out = A.contrib + 4ull * A.roff[b];
-    if (total <= (uint32_t)kListStage && S.longest == 0u)
+    if (total <= (uint32_t)kListStage)
     {
-        // The lists fit in shared memory: fill them there, order each by key
-        // (short lists by one thread, the others by a warp), then sum every
-        // voxel's list in that order (the reference CPU order), regularise and
-        // leave the quadric for the solve; no list goes to global memory.
+        // the lists fit in shared memory: fill them there, sort the short ones
+        // (one thread per voxel), copy the brick's lists out in one sweep
         {
             ListStageFill fs{S};
             for (unsigned long long r = tid; r < nrec; r += blockDim.x)
@@ -1972,70 +2097,11 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
                 P[y] = pv;
             }
         }
-        {
-            // lists of kWarpSortMin..kWarpSortMax entries: each warp ranks one
-            // list at a time (keys are unique per voxel), all lanes read their
-            // entries before any lane stores
-            const int lane = tid & 31;
-            for (int j = tid >> 5; j < nvox; j += kConsumeThreads / 32)
-            {
-                const uint32_t c = S.cnt[j];
-                if (c < (uint32_t)kWarpSortMin)
-                    continue;
-                const uint32_t st = S.off[j] - c;
-                unsigned long long k[kWarpSortPer];
-                uint32_t pv[kWarpSortPer], r[kWarpSortPer];
-#pragma unroll
-                for (int q = 0; q < kWarpSortPer; ++q)
-                {
-                    const uint32_t idx = (uint32_t)(lane + 32 * q);
-                    k[q] = idx < c ? S.skey[st + idx] : ~0ull;
-                    pv[q] = idx < c ? S.spay[st + idx] : 0u;
-                    r[q] = 0;
-                }
-#pragma unroll
-                for (int sq = 0; sq < kWarpSortPer; ++sq)
-                {
-                    if ((uint32_t)(32 * sq) >= c)
-                        break;
-                    const uint32_t jn = c - 32u * sq < 32u ? c - 32u * sq : 32u;
-                    for (uint32_t jj = 0; jj < jn; ++jj)
-                    {
-                        const unsigned long long kj = S.skey[st + 32u * sq + jj];
-#pragma unroll
-                        for (int q = 0; q < kWarpSortPer; ++q)
-                            r[q] += kj < k[q];
-                    }
-                }
-                __syncwarp();
-#pragma unroll
-                for (int q = 0; q < kWarpSortPer; ++q)
-                    if ((uint32_t)(lane + 32 * q) < c)
-                    {
-                        S.skey[st + r[q]] = k[q];
-                        S.spay[st + r[q]] = pv[q];
-                    }
-                __syncwarp();
-            }
-        }
         __syncthreads();
-        for (int lv = tid; lv < 512; lv += blockDim.x)
+        for (uint32_t i = tid; i < total; i += blockDim.x)
         {
-            if (!((S.obits[lv >> 5] >> (lv & 31)) & 1u))
-                continue;
-            const int j = dense_index(S, lv);
-            const long long row = (long long)(vbase + j);
-            const uint32_t c = S.cnt[j], st = S.off[j] - c;
-            const int vc[3] = {o[0] + (lv & 7), o[1] + ((lv >> 3) & 7), o[2] + (lv >> 6)};
-            Acc a;
-            acc_init(a);
-            for (uint32_t x = 0; x < c; ++x)
-            {
-                Contrib cb;
-                contrib_load(A, vc, S.skey[st + x], S.spay[st + x], cb);
-                contrib_apply(cb, a);
-            }
-            voxel_sum_out(A, row, a);
+            const unsigned long long k = S.skey[i];
+            out[i] = make_uint4((uint32_t)k, (uint32_t)(k >> 32), S.spay[i], 0u);
         }
     }
     else
@@ -2060,13 +2126,17 @@ __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int
     return (unsigned long long)lo | ((unsigned long long)hi << 32);
 }
 
-// Solve one voxel from its regularised quadric (flexible_dual_grid.cpp:795-797);
-// a voxel whose unconstrained solution leaves its box goes to the
-// constrained-search list.
-__device__ __forceinline__ void voxel_solve(const SolveArgs &A, long long row, const int vc[3], const float q[10])
+// Regularise and solve one voxel (flexible_dual_grid.cpp:763-797); a voxel whose
+// unconstrained solution leaves its box goes to the constrained-search list.
+__device__ __forceinline__ void voxel_finish(const SolveArgs &A, const Grid &g, long long row, const int vc[3], const Acc &a)
 {
+    float q[10];
+    regularize(a.q, a.mean, a.cnt, A.rw, q);
     float v[3];
-    const bool inside = solve_unconstrained(vc, A.m.g, q, v);
+    const bool inside = solve_unconstrained(vc, g, q, v);
+    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
+    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
+    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
     if (inside)
     {
         A.dual[row * 3 + 0] = v[0];
@@ -2090,22 +2160,14 @@ __device__ __forceinline__ void voxel_solve(const SolveArgs &A, long long row, c
         c[4 + i] = q[i];
 }
 
-// Regularise and solve one voxel summed from its list (flexible_dual_grid.cpp:763-797).
-__device__ __forceinline__ void voxel_finish(const SolveArgs &A, long long row, const int vc[3], const Acc &a)
-{
-    float q[10];
-    regularize(a.q, a.mean, a.cnt, A.rw, q);
-    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
-    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
-    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
-    voxel_solve(A, row, vc, q);
-}
-
+constexpr int kWarpSortPer = 2;                      // ... up to 2 entries per lane
+constexpr int kWarpSortMax = 32 * kWarpSortPer;      // longer lists go to voxel_accumulate_long
 constexpr int kLongMidMax = 1024;                    // ... one CTA of 128 threads, shared-memory sort
 constexpr int kLongHugeMax = 8192;                   // ... one CTA of 256 threads; longer: in-place insertion sort
 
 // 12 resident CTAs per SM (at most 40 registers): the sums wait on gathers,
 // and the extra warps hide more of that than the few spills cost
+template <bool B>
 __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long long nrows)
 {
     const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2114,6 +2176,7 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
     const unsigned long long d = valid ? A.vlist[row] : 0ull;
     const unsigned long long first = d & ((1ull << 40) - 1ull);
     const uint32_t n = (uint32_t)(d >> 40) & kListCountMax;
+    const bool sorted = (d & kListSorted) != 0ull;
     // The warp orders the longer lists of its 32 voxels one after another: each
     // lane holds up to kWarpSortPer entries of the list and finds their ranks
     // among the list's (unique) keys, then stores the entries at those ranks.
@@ -2176,21 +2239,11 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
         return;
     }
     const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
-    if (n == 0)
-    {
-        // summed by brick_lists: solve from the stored quadric
-        float q[10];
-        const float *qs = A.qreg + row * 10;
-#pragma unroll
-        for (int i = 0; i < 10; ++i)
-            q[i] = qs[i];
-        voxel_solve(A, row, vc, q);
-        return;
-    }
+    const Grid &g = mesh_of<B>(A, seg_of_row<B>(A, row)).g;
     uint4 *lst = A.contrib + first;
-    if (n < (uint32_t)kWarpSortMin)
+    if (n < (uint32_t)kWarpSortMin && !sorted)
     {
-        // short lists of bricks whose lists did not fit in shared memory:
+        // short lists that brick_lists could not sort in shared memory:
         // insertion sort in place
         for (uint32_t x = 1; x < n; ++x)
         {
@@ -2215,10 +2268,10 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
     {
         const uint4 e = lst[x];
         Contrib c;
-        contrib_load(A, vc, entry_key(e), e.z, c);
+        contrib_load(A, g, vc, entry_key(e), e.z, c);
         contrib_apply(c, a);
     }
-    voxel_finish(A, row, vc, a);
+    voxel_finish(A, g, row, vc, a);
 }
 
 constexpr int kLongChunk = 256; // contributions staged per step of the sequential sum
@@ -2234,7 +2287,7 @@ constexpr size_t long_smem()
 // thread.  Lists longer than kMax are insertion-sorted in place (slow,
 // correct).
 // kHuge = false: lists of up to kLongMidMax entries (front of longv); true: longer lists (back of longv).
-template <int kMax, int kThreadsT, bool kHuge>
+template <int kMax, int kThreadsT, bool kHuge, bool B>
 __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
 {
     extern __shared__ unsigned long long lsm[];
@@ -2250,6 +2303,7 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
         const unsigned long long first = d & ((1ull << 40) - 1ull);
         const uint32_t n = (uint32_t)(d >> 40) & kListCountMax;
         const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
+        const Grid &g = mesh_of<B>(A, seg_of_row<B>(A, row)).g;
         uint4 *lst = A.contrib + first;
         Acc a;
         acc_init(a);
@@ -2299,7 +2353,7 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
             {
                 const uint32_t cn = min((uint32_t)kLongChunk, n - c0);
                 for (uint32_t i = tid; i < cn; i += blockDim.x)
-                    contrib_load(A, vc, key[c0 + i], pay[c0 + i], cb[i]);
+                    contrib_load(A, g, vc, key[c0 + i], pay[c0 + i], cb[i]);
                 __syncthreads();
                 if (tid == 0)
                     for (uint32_t i = 0; i < cn; ++i)
@@ -2329,20 +2383,22 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
             {
                 const uint4 e = lst[x];
                 Contrib c;
-                contrib_load(A, vc, entry_key(e), e.z, c);
+                contrib_load(A, g, vc, entry_key(e), e.z, c);
                 contrib_apply(c, a);
             }
         }
         if (tid == 0)
-            voxel_finish(A, row, vc, a);
+            voxel_finish(A, g, row, vc, a);
         __syncthreads();
     }
 }
 
 // Constrained search (faces, edges, corners of the voxel box) for the voxels
 // whose unconstrained solution left the box; one thread per listed voxel.
+template <bool B>
 __global__ void __launch_bounds__(128) constrained_solve(const float *__restrict__ clist, const uint32_t *__restrict__ counters,
-                                                         uint32_t cap, Grid g, float *__restrict__ dual)
+                                                         uint32_t cap, Grid g1, const Mesh *__restrict__ segs, int nseg,
+                                                         float *__restrict__ dual)
 {
     const uint32_t n = min(counters[C_CONSTRAINED], cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -2355,7 +2411,10 @@ __global__ void __launch_bounds__(128) constrained_solve(const float *__restrict
         for (int k = 0; k < 10; ++k)
             q[k] = c[4 + k];
         float v[3];
-        solve_constrained(vc, g, q, v);
+        if constexpr (B)
+            solve_constrained(vc, segs[seg_find(nseg, row, [&](int s) { return segs[s].row0; })].g, q, v);
+        else
+            solve_constrained(vc, g1, q, v);
         dual[row * 3 + 0] = v[0];
         dual[row * 3 + 1] = v[1];
         dual[row * 3 + 2] = v[2];
@@ -2394,17 +2453,31 @@ __global__ void __launch_bounds__(128) brick_coords(const uint32_t *__restrict__
 }
 
 // z-order row bases: sort key of each active brick (its z-order code) ...
-__global__ void zorder_brick_keys(const uint32_t *__restrict__ active, long long n_active, Grid g,
-                                  unsigned long long *__restrict__ keys, uint32_t *__restrict__ slots)
+// In a batched conversion the key leads with the brick's mesh (bits 42 and up),
+// so that each mesh's rows stay together, in z-order inside the mesh (brick
+// coordinates below 2^14 per axis).
+template <bool B>
+__global__ void zorder_brick_keys(const uint32_t *__restrict__ active, long long n_active, Grid g1, const Mesh *__restrict__ segs,
+                                  int nseg, unsigned long long *__restrict__ keys, uint32_t *__restrict__ slots)
 {
     const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_active)
         return;
-    const long long b = active[s];
+    long long b = active[s];
+    unsigned long long lead = 0;
+    const Grid *gp = &g1;
+    if constexpr (B)
+    {
+        const int sg = seg_find(nseg, b, [&](int i) { return segs[i].brick0; });
+        b -= segs[sg].brick0;
+        gp = &segs[sg].g;
+        lead = (unsigned long long)sg << 42;
+    }
+    const Grid &g = *gp;
     const unsigned long long bx = (unsigned long long)(g.gmin[0] / kBrick) + (unsigned long long)(b % g.nb[0]);
     const unsigned long long by = (unsigned long long)(g.gmin[1] / kBrick) + (unsigned long long)((b / g.nb[0]) % g.nb[1]);
     const unsigned long long bz = (unsigned long long)(g.gmin[2] / kBrick) + (unsigned long long)(b / ((long long)g.nb[0] * g.nb[1]));
-    keys[s] = brick_morton(bx, by, bz);
+    keys[s] = lead | brick_morton(bx, by, bz);
     slots[s] = (uint32_t)s;
 }
 
@@ -2710,8 +2783,15 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, scan_units, face_large, face_units, qtab;
     Buf vcnt, voff, emax, bkeys, blong, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, qreg, fstage, estage, longv, face_end;
+    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, fstage, estage, longv, face_end;
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
+    Buf segs_d;                             // batched conversion: the meshes (device copy of segs)
+    std::vector<Mesh> segs;                 // batched conversion: the meshes, with their global offsets
+    Mesh *segs_pinned = nullptr;            // staging of the mesh table for its upload (pinned)
+    unsigned long long *seg_rows = nullptr; // first output row of every mesh and the total: pinned, mapped
+    unsigned long long *seg_rows_dev = nullptr;
+    int seg_cap = 0;                        // meshes the pinned buffers hold
+    bool batch = false;                     // the conversion in progress is a batched one
     unsigned long long *host = nullptr;     // readback words: pinned, mapped host memory
     unsigned long long *host_dev = nullptr; // the same words as the device addresses them
     cudaMemPool_t pool = nullptr;       // workspace pool (keeps its memory until the context is destroyed)
@@ -2754,8 +2834,8 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large, &c->scan_units,
                 &c->face_large, &c->face_units, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->blong, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->qreg, &c->fstage, &c->estage, &c->longv, &c->face_end,
-                &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase};
+                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv, &c->face_end,
+                &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase, &c->segs_d};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
@@ -2909,16 +2989,23 @@ int zorder_row_bases(ovx_fdg_context *ctx, cudaStream_t st)
     unsigned long long *kin = (unsigned long long *)ctx->zkeys.p, *kout = kin + (na + 1);
     uint32_t *vin = (uint32_t *)ctx->zslots.p, *vout = vin + (na + 1);
     const uint32_t *active = (const uint32_t *)ctx->active.p;
-    zorder_brick_keys<<<blocks_for(na, 256), 256, 0, st>>>(active, na, ctx->g, kin, vin);
-    // key bits: 3 x (bits of the largest brick coordinate)
-    int cb = 1;
-    for (int a = 0; a < 3; ++a)
+    int end_bit = 63;
+    if (ctx->batch)
+        zorder_brick_keys<true><<<blocks_for(na, 256), 256, 0, st>>>(active, na, ctx->g, (const Mesh *)ctx->segs_d.p,
+                                                                     (int)ctx->segs.size(), kin, vin);
+    else
     {
-        const long long mx = ctx->g.gmin[a] / kBrick + ctx->g.nb[a];
-        while ((1ll << cb) <= mx)
-            ++cb;
+        zorder_brick_keys<false><<<blocks_for(na, 256), 256, 0, st>>>(active, na, ctx->g, nullptr, 0, kin, vin);
+        // key bits: 3 x (bits of the largest brick coordinate)
+        int cb = 1;
+        for (int a = 0; a < 3; ++a)
+        {
+            const long long mx = ctx->g.gmin[a] / kBrick + ctx->g.nb[a];
+            while ((1ll << cb) <= mx)
+                ++cb;
+        }
+        end_bit = std::min(63, 3 * cb);
     }
-    const int end_bit = std::min(63, 3 * cb);
     size_t bytes = 0;
     OVX_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, (int)na, 0, end_bit, st));
     OVX_CUDA(ensure(st, ctx, ctx->cub_tmp, bytes));
@@ -2976,6 +3063,7 @@ Mesh make_mesh(const ovx_fdg_context *c)
     m.ox = c->origin[0];
     m.oy = c->origin[1];
     m.oz = c->origin[2];
+    m.fbytes = c->fbytes;
     return m;
 }
 
@@ -2990,6 +3078,32 @@ static_assert(kHostCounters * 8 + C_WORDS * 4 <= kHostFinish * 8 && kHostFinish 
 __global__ void copy_word(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst)
 {
     *dst = *src;
+}
+
+// First output row of every mesh of a batched conversion, into the mesh table
+// (row0) and into mapped host memory, then the total.
+__global__ void seg_rows(Mesh *__restrict__ segs, int nseg, const unsigned long long *__restrict__ bbase, long long nb,
+                         unsigned long long *host)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    volatile unsigned long long *h = host;
+    if (i < nseg)
+    {
+        const unsigned long long r = bbase[segs[i].brick0];
+        segs[i].row0 = (long long)r;
+        h[i] = r;
+    }
+    else if (i == nseg)
+        h[i] = bbase[nb];
+    __threadfence_system();
+}
+
+// The mesh table of a batched conversion, from mapped host memory (a kernel
+// rather than a copy, which could queue behind another stream's large copy).
+__global__ void load_segs(const uint32_t *__restrict__ src, uint32_t *__restrict__ dst, long long words)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
 }
 
 // Up to kReadbackMax device words/blocks to copy into the mapped readback
@@ -3057,6 +3171,8 @@ GenArgs make_gen(ovx_fdg_context *ctx)
 {
     GenArgs A{};
     A.m = make_mesh(ctx);
+    A.segs = ctx->batch ? (const Mesh *)ctx->segs_d.p : nullptr;
+    A.nseg = ctx->batch ? (int)ctx->segs.size() : 0;
     A.bits = (uint32_t *)ctx->bits.p;
     A.rcnt = (uint32_t *)ctx->rcnt.p;
     A.roff = (const unsigned long long *)ctx->roff.p;
@@ -3082,7 +3198,7 @@ GenArgs make_gen(ovx_fdg_context *ctx)
     return A;
 }
 
-template <int M, typename IdxT>
+template <int M, typename IdxT, bool B>
 void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
 {
     if (M == FILL && ctx->event_staged)
@@ -3097,7 +3213,7 @@ void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
     }
     else if (ctx->nf > 0)
     {
-        tri_events<M, IdxT><<<blocks_for(3 * ctx->nf, kEventThreads), kEventThreads, 0, st>>>(A);
+        tri_events<M, IdxT, B><<<blocks_for(3 * ctx->nf, kEventThreads), kEventThreads, 0, st>>>(A);
         ++ctx->launches;
         if (M == COUNT)
         {
@@ -3109,13 +3225,13 @@ void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
                                               : ctx->sms * 8;
         if (rows_grid > 0)
         {
-            large_rows<M, IdxT><<<(unsigned)rows_grid, kEventThreads, 0, st>>>(A);
+            large_rows<M, IdxT, B><<<(unsigned)rows_grid, kEventThreads, 0, st>>>(A);
             ++ctx->launches;
         }
     }
 }
 
-template <int M, typename IdxT>
+template <int M, typename IdxT, bool B>
 void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
 {
     if (ctx->fw > 0.0f && ctx->nf > 0)
@@ -3136,7 +3252,7 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
         }
         else
         {
-            face_records<M, IdxT><<<blocks_for(ctx->nf, kFaceThreads), kFaceThreads, 0, st>>>(A);
+            face_records<M, IdxT, B><<<blocks_for(ctx->nf, kFaceThreads), kFaceThreads, 0, st>>>(A);
             ++ctx->launches;
         }
         if (!(M == FILL && ctx->face_staged))
@@ -3150,7 +3266,7 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
                 M == FILL ? std::min<long long>(ctx->sms * 7, blocks_for((long long)ctx->n_funits, kFaceThreads)) : ctx->sms * 7;
             if (faces_grid > 0)
             {
-                large_faces<M, IdxT><<<(unsigned)faces_grid, kFaceThreads, 0, st>>>(A);
+                large_faces<M, IdxT, B><<<(unsigned)faces_grid, kFaceThreads, 0, st>>>(A);
                 ++ctx->launches;
             }
         }
@@ -3169,17 +3285,41 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
         const long long rec_grid = std::min<long long>(ctx->sms * 8, blocks_for(nb_edges, kThreads));
         if (rec_grid > 0)
         {
-            boundary_records<M><<<(unsigned)rec_grid, kThreads, 0, st>>>(A);
+            boundary_records<M, B><<<(unsigned)rec_grid, kThreads, 0, st>>>(A);
             ++ctx->launches;
         }
         const long long nb_long = M == FILL ? (long long)ctx->n_blong : 3 * ctx->nf;
         const long long long_grid = std::min<long long>(ctx->sms * 4, blocks_for(nb_long, kThreads / 32));
         if (long_grid > 0)
         {
-            boundary_long<M><<<(unsigned)long_grid, kThreads, 0, st>>>(A);
+            boundary_long<M, B><<<(unsigned)long_grid, kThreads, 0, st>>>(A);
             ++ctx->launches;
         }
     }
+}
+
+// The record generators for the conversion in progress: batched, or a single
+// mesh with int32 or int64 face indices.
+template <int M>
+void launch_events_any(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
+{
+    if (ctx->batch)
+        launch_events<M, int, true>(ctx, A, st);
+    else if (ctx->fbytes == 8)
+        launch_events<M, long long, false>(ctx, A, st);
+    else
+        launch_events<M, int, false>(ctx, A, st);
+}
+
+template <int M>
+void launch_faces_boundary_any(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
+{
+    if (ctx->batch)
+        launch_faces_boundary<M, int, true>(ctx, A, st);
+    else if (ctx->fbytes == 8)
+        launch_faces_boundary<M, long long, false>(ctx, A, st);
+    else
+        launch_faces_boundary<M, int, false>(ctx, A, st);
 }
 
 // Occupancy stage shared by the full conversion and intersect_occ; ends with
@@ -3245,13 +3385,19 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         OVX_CUDA(cudaMemsetAsync(ctx->vcnt.p, 0, (size_t)(ctx->nv + 1) * 4, es));
         uint32_t *vcnt = (uint32_t *)ctx->vcnt.p;
         unsigned long long *voff = (unsigned long long *)ctx->voff.p;
-        if (ctx->fbytes == 8)
+        if (ctx->batch)
+            edge_count_batch<<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const Mesh *)ctx->segs_d.p, (int)ctx->segs.size(), nf,
+                                                                           vcnt);
+        else if (ctx->fbytes == 8)
             edge_count<long long><<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const long long *)ctx->faces, nf, ctx->nv, vcnt);
         else
             edge_count<int><<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const int *)ctx->faces, nf, ctx->nv, vcnt);
         OVX_CUDA(cudaGetLastError());
         OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, voff, ctx->nv + 1, es, &ctx->cub_tmp_side));
-        if (ctx->fbytes == 8)
+        if (ctx->batch)
+            edge_fill_batch<<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const Mesh *)ctx->segs_d.p, (int)ctx->segs.size(), nf,
+                                                                          voff, vcnt, (uint32_t *)ctx->emax.p);
+        else if (ctx->fbytes == 8)
             edge_fill<long long><<<blocks_for(nf, kThreads), kThreads, 0, es>>>((const long long *)ctx->faces, nf, ctx->nv, voff, vcnt,
                                                                                (uint32_t *)ctx->emax.p);
         else
@@ -3280,10 +3426,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         A.estage = nullptr; // occupancy only: no records
         A.estage_cap = 0;
     }
-    if (ctx->fbytes == 8)
-        launch_events<COUNT, long long>(ctx, A, st);
-    else
-        launch_events<COUNT, int>(ctx, A, st);
+    launch_events_any<COUNT>(ctx, A, st);
     OVX_CUDA(cudaGetLastError());
     stage(ctx, EV_EVENTS_COUNT, st);
 
@@ -3295,6 +3438,13 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     brick_slots<<<blocks_for(nb, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->aflag.p, (const unsigned long long *)ctx->aslot.p,
                                                                nb, (uint32_t *)ctx->active.p);
     ctx->launches += 2;
+    if (ctx->batch)
+    {
+        const int ns = (int)ctx->segs.size();
+        seg_rows<<<blocks_for(ns + 1, kThreads), kThreads, 0, st>>>((Mesh *)ctx->segs_d.p, ns,
+                                                                   (const unsigned long long *)ctx->bbase.p, nb, ctx->seg_rows_dev);
+        ++ctx->launches;
+    }
     OVX_CUDA(cudaGetLastError());
     stage(ctx, EV_COMPACT, st);
 
@@ -3305,10 +3455,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     if (full)
     {
         A = make_gen(ctx);
-        if (ctx->fbytes == 8)
-            launch_faces_boundary<COUNT, long long>(ctx, A, st);
-        else
-            launch_faces_boundary<COUNT, int>(ctx, A, st);
+        launch_faces_boundary_any<COUNT>(ctx, A, st);
         OVX_CUDA(cudaGetLastError());
         OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)ctx->rcnt.p, (unsigned long long *)ctx->roff.p, nb + 1, st));
     }
@@ -3349,6 +3496,34 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     ctx->face_staged = full && ctx->n_fstaged <= (unsigned long long)cap_u32(ctx->fstage, sizeof(uint4));
     ctx->fstage_want = std::max(ctx->fstage_want, ctx->n_fstaged);
     *num_voxels = (int64_t)n;
+    return OVX_FDG_OK;
+}
+
+// The per-brick lists, the per-voxel sums and solves, and the constrained
+// search of a conversion (single mesh or batch).
+template <bool B>
+int launch_consume(ovx_fdg_context *ctx, const SolveArgs &SA, cudaStream_t st, long long n)
+{
+    if (ctx->n_active > 0)
+    {
+        brick_lists<B><<<(unsigned)ctx->n_active, kConsumeThreads, 0, st>>>(SA);
+        ++ctx->launches;
+    }
+    stage(ctx, EV_CONSUME, st);
+    voxel_accumulate<B><<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
+    // one CTA per long list, at most one per row
+    voxel_accumulate_long<kLongMidMax, 128, false, B>
+        <<<(unsigned)std::min<long long>(ctx->sms * 8, n), 128, long_smem<kLongMidMax>(), st>>>(SA);
+    OVX_CUDA(cudaFuncSetAttribute(voxel_accumulate_long<kLongHugeMax, 256, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)long_smem<kLongHugeMax>()));
+    voxel_accumulate_long<kLongHugeMax, 256, true, B>
+        <<<(unsigned)std::min<long long>(ctx->sms * 2, n), 256, long_smem<kLongHugeMax>(), st>>>(SA);
+    ctx->launches += 3;
+    stage(ctx, EV_SOLVE, st);
+    constrained_solve<B><<<(unsigned)std::min<long long>(ctx->sms * 8, blocks_for(n, 128)), 128, 0, st>>>(
+        (const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap, ctx->g, SA.segs, SA.nseg, SA.dual);
+    ++ctx->launches;
+    OVX_CUDA(cudaGetLastError());
     return OVX_FDG_OK;
 }
 
@@ -3427,6 +3602,10 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
         cudaMemPoolDestroy(ctx->pool);
     if (ctx->host)
         cudaFreeHost(ctx->host);
+    if (ctx->segs_pinned)
+        cudaFreeHost(ctx->segs_pinned);
+    if (ctx->seg_rows)
+        cudaFreeHost(ctx->seg_rows);
     if (ctx->done)
         cudaEventDestroy(ctx->done);
     if (ctx->side)
@@ -3634,6 +3813,7 @@ int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int
         return rc;
     const DeviceScope scope(ctx->device);
     OVX_CUDA(scope.status);
+    ctx->batch = false;
     ctx->g = g;
     ctx->verts = vertices;
     ctx->nv = num_vertices;
@@ -3651,6 +3831,120 @@ int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int
         return rc;
     ctx->phase = 1;
     return OVX_FDG_OK;
+}
+
+int ovx_fdg_begin_batch(ovx_fdg_context *ctx, void *stream, const ovx_fdg_mesh *meshes, int32_t num_meshes, float face_weight,
+                        float boundary_weight, float regularization_weight, int64_t *num_voxels, int64_t *total_voxels)
+{
+    if (!ctx)
+        return OVX_FDG_INVALID_ARGUMENT;
+    ctx->phase = 0;
+    ctx->err.clear();
+    if (!total_voxels || !num_voxels || !meshes || num_meshes < 1)
+        return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "batch: NULL argument or no meshes");
+    *total_voxels = 0;
+    std::vector<Mesh> segs((size_t)num_meshes);
+    long long tri = 0, brick = 0, vert = 0;
+    for (int i = 0; i < num_meshes; ++i)
+    {
+        const ovx_fdg_mesh &m = meshes[i];
+        num_voxels[i] = 0;
+        const std::string which = "batch mesh " + std::to_string(i) + ": ";
+        if (m.num_vertices < 0 || m.num_faces < 0)
+            return fail(ctx, OVX_FDG_INVALID_ARGUMENT, (which + "negative size").c_str());
+        if (m.num_faces > 0 && m.num_vertices == 0)
+            return fail(ctx, OVX_FDG_BAD_FACE_INDEX, (which + "faces reference vertices but there are none").c_str());
+        if ((m.num_vertices > 0 && !m.vertices) || (m.num_faces > 0 && !m.faces))
+            return fail(ctx, OVX_FDG_INVALID_ARGUMENT, (which + "NULL vertices or faces").c_str());
+        if (m.face_index_bytes != 4 && m.face_index_bytes != 8)
+            return fail(ctx, OVX_FDG_INVALID_ARGUMENT, (which + "face_index_bytes must be 4 or 8").c_str());
+        Grid g{};
+        const int rc = check_grid(ctx, &m.grid, g);
+        if (rc != OVX_FDG_OK)
+        {
+            ctx->err = which + ctx->err;
+            return rc;
+        }
+        Mesh &M = segs[(size_t)i];
+        M.g = g;
+        M.verts = m.vertices;
+        M.nv = m.num_vertices;
+        M.faces = m.faces;
+        M.nf = m.num_faces;
+        M.ox = m.origin[0];
+        M.oy = m.origin[1];
+        M.oz = m.origin[2];
+        M.fbytes = m.face_index_bytes;
+        M.tri0 = tri;
+        M.brick0 = brick;
+        M.vert0 = vert;
+        M.row0 = 0;
+        tri += m.num_faces;
+        brick += g.nbricks;
+        vert += m.num_vertices;
+    }
+    if (tri >= (1ll << 30) || vert >= (1ll << 31) - 1)
+        return fail(ctx, OVX_FDG_CAPACITY, "batch: more than 2^30 faces or 2^31-1 vertices in all");
+    if (brick >= (1ll << 31) || brick * kWordsPerBrick * 4ll > (64ll << 30))
+        return fail(ctx, OVX_FDG_CAPACITY, "batch: grids too large for the dense brick bitmap (64 GiB limit)");
+    const DeviceScope scope(ctx->device);
+    OVX_CUDA(scope.status);
+    cudaStream_t st = (cudaStream_t)stream;
+    OVX_CUDA(wait_previous(ctx, st));
+    if (num_meshes > ctx->seg_cap)
+    {
+        // the previous batch's table upload and row readback are complete: its begin synchronised
+        if (ctx->segs_pinned)
+            cudaFreeHost(ctx->segs_pinned);
+        if (ctx->seg_rows)
+            cudaFreeHost(ctx->seg_rows);
+        ctx->segs_pinned = nullptr;
+        ctx->seg_rows = nullptr;
+        ctx->seg_cap = 0;
+        OVX_CUDA(cudaHostAlloc((void **)&ctx->segs_pinned, (size_t)num_meshes * sizeof(Mesh), cudaHostAllocMapped));
+        OVX_CUDA(cudaHostAlloc((void **)&ctx->seg_rows, (size_t)(num_meshes + 1) * 8, cudaHostAllocMapped));
+        OVX_CUDA(cudaHostGetDevicePointer((void **)&ctx->seg_rows_dev, ctx->seg_rows, 0));
+        ctx->seg_cap = num_meshes;
+    }
+    std::memcpy(ctx->segs_pinned, segs.data(), (size_t)num_meshes * sizeof(Mesh));
+    Mesh *segs_map = nullptr;
+    OVX_CUDA(cudaHostGetDevicePointer((void **)&segs_map, ctx->segs_pinned, 0));
+    static_assert(sizeof(Mesh) % 4 == 0, "the mesh table is copied in 32-bit words");
+    OVX_CUDA(ensure(st, ctx, ctx->segs_d, (size_t)num_meshes * sizeof(Mesh)));
+    const long long words = (long long)num_meshes * (long long)(sizeof(Mesh) / 4);
+    load_segs<<<(unsigned)std::min<long long>(ctx->sms, blocks_for(words, kThreads)), kThreads, 0, st>>>(
+        (const uint32_t *)segs_map, (uint32_t *)ctx->segs_d.p, words);
+    ++ctx->launches;
+    OVX_CUDA(cudaGetLastError());
+    ctx->segs = std::move(segs);
+    ctx->batch = true;
+    ctx->g = Grid{};
+    ctx->g.nbricks = brick;
+    ctx->verts = nullptr;
+    ctx->nv = vert;
+    ctx->faces = nullptr;
+    ctx->fbytes = 4;
+    ctx->nf = tri;
+    ctx->origin[0] = ctx->origin[1] = ctx->origin[2] = 0.0f;
+    ctx->fw = face_weight;
+    ctx->bw = boundary_weight;
+    ctx->rw = regularization_weight;
+    const int rc = occupancy_stage(ctx, st, true, total_voxels);
+    if (rc != OVX_FDG_OK)
+        return rc;
+    for (int i = 0; i < num_meshes; ++i)
+        num_voxels[i] = (int64_t)(ctx->seg_rows[i + 1] - ctx->seg_rows[i]);
+    ctx->phase = 1;
+    return OVX_FDG_OK;
+}
+
+int ovx_fdg_finish_batch(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, float *dual_vertices, uint8_t *intersected)
+{
+    if (!ctx)
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (!ctx->batch || ctx->phase != 1)
+        return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "ovx_fdg_finish_batch without a successful ovx_fdg_begin_batch");
+    return ovx_fdg_finish(ctx, stream, voxel_indices, dual_vertices, intersected);
 }
 
 int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, float *dual_vertices, uint8_t *intersected)
@@ -3675,7 +3969,6 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(ensure(st, ctx, ctx->clist, (size_t)(n + 1) * 16 * 4));
     OVX_CUDA(ensure(st, ctx, ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
     OVX_CUDA(ensure(st, ctx, ctx->vlist, (size_t)n * 8));
-    OVX_CUDA(ensure(st, ctx, ctx->qreg, (size_t)n * 40));
     OVX_CUDA(ensure(st, ctx, ctx->longv, (size_t)(n + 1) * 4));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_LONG, 0, 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
@@ -3684,20 +3977,16 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     stage(ctx, EV_FINISH, st);
     GenArgs A = make_gen(ctx);
     A.qtab = nullptr;
-    if (ctx->fbytes == 8)
-        launch_events<FILL, long long>(ctx, A, st);
-    else
-        launch_events<FILL, int>(ctx, A, st);
+    launch_events_any<FILL>(ctx, A, st);
     stage(ctx, EV_EVENTS_FILL, st);
-    if (ctx->fbytes == 8)
-        launch_faces_boundary<FILL, long long>(ctx, A, st);
-    else
-        launch_faces_boundary<FILL, int>(ctx, A, st);
+    launch_faces_boundary_any<FILL>(ctx, A, st);
     OVX_CUDA(cudaGetLastError());
     stage(ctx, EV_RECORD_FILL, st);
 
     SolveArgs SA{};
     SA.m = make_mesh(ctx);
+    SA.segs = ctx->batch ? (const Mesh *)ctx->segs_d.p : nullptr;
+    SA.nseg = ctx->batch ? (int)ctx->segs.size() : 0;
     SA.bw = ctx->bw;
     SA.rw = ctx->rw;
     SA.bits = (const uint32_t *)ctx->bits.p;
@@ -3722,27 +4011,12 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.clist = (float *)ctx->clist.p;
     SA.contrib = (uint4 *)ctx->contrib.p;
     SA.vlist = (unsigned long long *)ctx->vlist.p;
-    SA.qreg = (float *)ctx->qreg.p;
     SA.longv = (uint32_t *)ctx->longv.p;
     SA.longv_cap = (uint32_t)(n + 1);
     SA.clist_cap = (uint32_t)(n + 1);
-    if (ctx->n_active > 0)
-    {
-        brick_lists<<<(unsigned)ctx->n_active, kConsumeThreads, 0, st>>>(SA);
-        ++ctx->launches;
-    }
-    stage(ctx, EV_CONSUME, st);
-    voxel_accumulate<<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
-    // one CTA per long list, at most one per row
-    voxel_accumulate_long<kLongMidMax, 128, false><<<(unsigned)std::min<long long>(ctx->sms * 8, n), 128, long_smem<kLongMidMax>(), st>>>(SA);
-    OVX_CUDA(cudaFuncSetAttribute(voxel_accumulate_long<kLongHugeMax, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)long_smem<kLongHugeMax>()));
-    voxel_accumulate_long<kLongHugeMax, 256, true><<<(unsigned)std::min<long long>(ctx->sms * 2, n), 256, long_smem<kLongHugeMax>(), st>>>(SA);
-    ctx->launches += 3;
-    stage(ctx, EV_SOLVE, st);
-    constrained_solve<<<(unsigned)std::min<long long>(ctx->sms * 8, blocks_for(n, 128)), 128, 0, st>>>((const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap,
-                                                    ctx->g, dual_vertices);
-    ++ctx->launches;
+    const int cr = ctx->batch ? launch_consume<true>(ctx, SA, st, n) : launch_consume<false>(ctx, SA, st, n);
+    if (cr != OVX_FDG_OK)
+        return cr;
     stage(ctx, EV_CONSTRAINED, st);
     OVX_CUDA(cudaGetLastError());
     {
@@ -3792,6 +4066,7 @@ int ovx_fdg_occupancy_begin(ovx_fdg_context *ctx, void *stream, const float *tri
         return rc;
     const DeviceScope scope(ctx->device);
     OVX_CUDA(scope.status);
+    ctx->batch = false;
     ctx->g = g;
     ctx->verts = triangles;
     ctx->nv = num_triangles * 3;

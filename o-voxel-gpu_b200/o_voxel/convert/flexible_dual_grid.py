@@ -279,7 +279,7 @@ def mesh_to_flexible_dual_grid_batch(
     face_weight: float = 1.0,
     boundary_weight: float = 1.0,
     regularization_weight: float = 0.1,
-    workers: int = 4,
+    max_group_records: int = 128_000_000,
     order: Optional[str] = None,
 ) -> List[Tuple[torch.Tensor, torch.Tensor, torch.Tensor]]:
     """
@@ -295,13 +295,19 @@ def mesh_to_flexible_dual_grid_batch(
             meshes a list of three numbers is one per-axis value: give per-mesh
             sizes as three 3-element lists).
         face_weight, boundary_weight, regularization_weight: shared by all meshes.
-        workers: host threads converting meshes concurrently, each with its own
-            CUDA stream; the results are ordered on the caller's current stream.
+        max_group_records: the meshes are converted in groups of consecutive
+            meshes whose expected quadric records (about 8 per unit of grid face
+            area plus 3 per triangle) stay within this budget, which bounds the
+            device workspace (about 100 bytes a record); 0 puts every mesh in one
+            group.
         order: output row order, as in mesh_to_flexible_dual_grid.
 
-    The reference has no batched form; this one exists so that many small and
-    mid-sized meshes keep the GPU busy while each mesh's single host
-    synchronisation (to learn its voxel count) happens.
+    The reference has no batched form.  Here every kernel of the conversion
+    runs once over all meshes of a group (their triangles, bricks and vertices
+    laid out one mesh after another), with one host synchronisation per group,
+    so many small and mid-sized meshes cost one pipeline instead of one each.
+    Work runs on the current stream; each mesh's tensors are views of the
+    group's output tensors.
     """
     n = len(meshes)
 
@@ -335,7 +341,7 @@ def mesh_to_flexible_dual_grid_batch(
         granges.append(gr_arg)
     out = _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
                                                        float(boundary_weight), float(regularization_weight),
-                                                       int(workers), _order_code(order))
+                                                       int(max_group_records), _order_code(order))
     return [_download(o) if h else o for o, h in zip(out, host)]
 
 

@@ -47,6 +47,8 @@ PROTOTYPES = [
     ("ovx_fdg_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.c_int32, _I64, _P, _P, _F, _F, _F, ctypes.POINTER(_I64)]),
     ("ovx_fdg_finish", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("ovx_fdg_sync_status", ctypes.c_int, [_P, _P]),
+    ("ovx_fdg_begin_batch", ctypes.c_int, [_P, _P, _P, ctypes.c_int32, _F, _F, _F, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
+    ("ovx_fdg_finish_batch", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("ovx_fdg_occupancy_begin", ctypes.c_int, [_P, _P, _P, _I64, _P, ctypes.POINTER(_I64)]),
     ("ovx_fdg_occupancy_finish", ctypes.c_int, [_P, _P, _P]),
     ("ovx_fdg_occupancy_noalloc", ctypes.c_int, [_P, _P, _I64, _P, _P, _I64, ctypes.POINTER(_I64)]),
@@ -55,6 +57,13 @@ PROTOTYPES = [
 
 class Grid(ctypes.Structure):
     _fields_ = [("voxel_size", ctypes.c_float * 3), ("grid_min", ctypes.c_int32 * 3), ("grid_max", ctypes.c_int32 * 3)]
+
+
+class MeshDesc(ctypes.Structure):
+    """ovx_fdg_mesh: one mesh of a batched conversion."""
+    _fields_ = [("vertices", ctypes.c_void_p), ("num_vertices", ctypes.c_int64), ("faces", ctypes.c_void_p),
+                ("face_index_bytes", ctypes.c_int32), ("num_faces", ctypes.c_int64), ("origin", ctypes.c_float * 3),
+                ("grid", Grid)]
 
 
 _LIB = None
@@ -169,6 +178,42 @@ class Context:
         if check:
             self._check(self._lib.ovx_fdg_sync_status(self.handle, st), "ovx_fdg_sync_status")
         return vox, dual, inter
+
+    def mesh_to_fdg_batch(self, meshes, fw, bw, rw, stream=None, check=True):
+        """meshes: list of (vertices, faces, origin, voxel_size, grid_range) with
+        CUDA tensors; one batched conversion; returns per-mesh torch tensors
+        (views of one output buffer)."""
+        import torch
+
+        dev = meshes[0][0].device
+        st = ctypes.c_void_p(stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream)
+        descs = (MeshDesc * len(meshes))()
+        for d, (v, f, origin, vs, gr) in zip(descs, meshes):
+            d.vertices = v.data_ptr() if v.numel() else None
+            d.num_vertices = v.shape[0]
+            d.faces = f.data_ptr() if f.numel() else None
+            d.face_index_bytes = f.element_size()
+            d.num_faces = f.shape[0]
+            for a in range(3):
+                d.origin[a] = float(origin[a])
+            d.grid = make_grid(vs, gr)
+        nv = (_I64 * len(meshes))()
+        total = _I64(0)
+        self._check(self._lib.ovx_fdg_begin_batch(self.handle, st, ctypes.cast(descs, ctypes.c_void_p), len(meshes), float(fw),
+                                                  float(bw), float(rw), nv, ctypes.byref(total)), "ovx_fdg_begin_batch")
+        N = total.value
+        vox = torch.empty((N, 3), dtype=torch.int32, device=dev)
+        dual = torch.empty((N, 3), dtype=torch.float32, device=dev)
+        inter = torch.empty((N, 3), dtype=torch.bool, device=dev)
+        ptr = lambda t: ctypes.c_void_p(t.data_ptr() if t.numel() else 0)  # noqa: E731
+        self._check(self._lib.ovx_fdg_finish_batch(self.handle, st, ptr(vox), ptr(dual), ptr(inter)), "ovx_fdg_finish_batch")
+        if check:
+            self._check(self._lib.ovx_fdg_sync_status(self.handle, st), "ovx_fdg_sync_status")
+        out, row = [], 0
+        for i in range(len(meshes)):
+            out.append((vox[row:row + nv[i]], dual[row:row + nv[i]], inter[row:row + nv[i]]))
+            row += nv[i]
+        return out
 
     def occupancy(self, triangles, voxel_size, grid_range, stream=None):
         import torch

@@ -25,8 +25,11 @@ def _upload(ws, device):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("workers", [1, 4])
-def test_batch_matches_oracle_and_single(cuda, workers):
+@pytest.mark.parametrize("group", [0, 400_000])
+def test_batch_matches_oracle_and_single(cuda, group):
+    """12 meshes in one batched pipeline (group 0), or cut into groups of about
+    400k expected records each: every mesh equals the single-mesh API's rows
+    and the oracle."""
     import torch
     import o_voxel
 
@@ -34,7 +37,7 @@ def test_batch_matches_oracle_and_single(cuda, workers):
     meshes = _upload(ws, cuda)
     kw = dict(face_weight=1.0, boundary_weight=0.2, regularization_weight=1e-2)
     outs = o_voxel.convert.mesh_to_flexible_dual_grid_batch(
-        meshes, grid_size=[w.grid_size for w in ws], aabb=[w.aabb for w in ws], workers=workers, **kw)
+        meshes, grid_size=[w.grid_size for w in ws], aabb=[w.aabb for w in ws], max_group_records=group, **kw)
     torch.cuda.synchronize()
     assert len(outs) == len(ws)
     for w, (v, f), out in zip(ws, meshes, outs):
@@ -71,7 +74,7 @@ def test_batch_error_is_raised(cuda):
     good = _upload([W.ico_cap(0)], cuda)[0]
     bad = (torch.rand(4, 3, device=cuda) - 0.5, torch.tensor([[0, 1, 2], [1, 2, 9]], device=cuda))
     with pytest.raises(RuntimeError, match="face index"):
-        o_voxel.convert.mesh_to_flexible_dual_grid_batch([good, bad, good], grid_size=32, aabb=W.UNIT_AABB, workers=2)
+        o_voxel.convert.mesh_to_flexible_dual_grid_batch([good, bad, good], grid_size=32, aabb=W.UNIT_AABB)
     # the pool stays usable
     outs = o_voxel.convert.mesh_to_flexible_dual_grid_batch([good], grid_size=64, aabb=W.UNIT_AABB,
                                                             boundary_weight=0.2, regularization_weight=1e-2)
@@ -107,3 +110,23 @@ def test_full_256_mesh_batch(cuda):
             assert torch.equal(a, b), (i, w.name)
         if i in subset:
             assert_fdg_equal(tuple(t.cpu().numpy() for t in out), _oracle(w, ("batch4", w.name)), w.name)
+
+
+@pytest.mark.gpu
+def test_batch_mixed_index_types_and_z_order(cuda):
+    """int32 and int64 faces in one batch, and z-order rows: each mesh equals
+    the single-mesh API with the same order."""
+    import torch
+    import o_voxel
+
+    ws = W.batch(seed=9, n_meshes=6, f_lo=2_000, f_hi=30_000, grids=(64, 128))
+    meshes = _upload(ws, cuda)
+    meshes = [(v, f.int() if i % 2 else f) for i, (v, f) in enumerate(meshes)]
+    kw = dict(face_weight=1.0, boundary_weight=0.2, regularization_weight=1e-2)
+    for order in (None, "z_order"):
+        outs = o_voxel.convert.mesh_to_flexible_dual_grid_batch(
+            meshes, grid_size=[w.grid_size for w in ws], aabb=[w.aabb for w in ws], order=order, **kw)
+        for w, (v, f), out in zip(ws, meshes, outs):
+            single = o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=w.grid_size, aabb=w.aabb, order=order, **kw)
+            for a, b in zip(out, single):
+                assert torch.equal(a, b), (w.name, order)

@@ -224,7 +224,7 @@ def test_host_tensors(cuda):
     batch = o_voxel.convert.mesh_to_flexible_dual_grid_batch([(v, f), (v.to(cuda), f.to(cuda))], grid_size=w.grid_size,
                                                             aabb=w.aabb, face_weight=w.face_weight,
                                                             boundary_weight=w.boundary_weight,
-                                                            regularization_weight=w.regularization_weight, workers=2)
+                                                            regularization_weight=w.regularization_weight)
     assert batch[0][0].device.type == "cpu" and batch[1][0].is_cuda
     for a, b, c in zip(batch[0], batch[1], host):
         assert torch.equal(a, b.cpu()) and torch.equal(a, c)
