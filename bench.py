@@ -81,6 +81,15 @@ def grid_args(w):
     return ab[0], vs, [0, 0, 0, int(g[0]), int(g[1]), int(g[2])]
 
 
+def apply_tuned_shapes(ctx, w):
+    """The library's tuned work shapes (o_voxel/tuning.json) for this workload's
+    grid, as the o_voxel wrapper applies them, on a C-ABI context."""
+    from o_voxel.convert import _tuning
+
+    values = _tuning.values_for(max(grid_args(w)[2][3:]))
+    ctx.set_tuning(dict(zip(_tuning.FIELDS, values)) if values else None)
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -358,6 +367,7 @@ def measure_workload(name, w, dev, stream, flush, steps, ours_out=None):
     vd = torch.from_numpy(w.vertices).to(dev)
     fd = torch.from_numpy(w.faces).to(dev)
     ctx = abi.Context(dev.index)
+    apply_tuned_shapes(ctx, w)
     kw = (origin, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
     one = lambda: ctx.mesh_to_fdg(vd, fd, *kw, check=False)  # noqa: E731
     torch.cuda.synchronize()
@@ -403,6 +413,7 @@ def run_ours(args, rank, world):
     vd = torch.from_numpy(w.vertices).to(dev)
     fd = torch.from_numpy(w.faces).to(dev)  # int64, consumed as supplied
     ctx = abi.Context(dev.index)
+    apply_tuned_shapes(ctx, w)
     kw = (origin, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
@@ -589,6 +600,7 @@ def run_one_workload(args):
     v = torch.from_numpy(w.vertices).to(dev)
     f = torch.from_numpy(w.faces).to(dev)
     ctx = abi.Context(0)
+    apply_tuned_shapes(ctx, w)
     times, n = [], 0
     for _ in range(max(1, args.conversions)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -107,6 +107,34 @@ enum ovx_fdg_order
 int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order);
 
 /*
+ * Work shapes of a context's following conversions (no counterpart in the
+ * reference, whose shapes are constants: 16x16 scan tiles,
+ * intersect_qef.cu:27-28, and 8^3 bricks, types.cuh:50).  Results do not
+ * depend on them; speed does, with the mesh and grid.  NULL restores the
+ * defaults (64, 256, 8, 32, 64).  o_voxel picks them per grid size from a
+ * table written by the project's tuner (fdg_tune.py).
+ *   unit_cells          cells (rows x columns) per unit of work of a large
+ *                       (triangle, projection axis) pair, 8..4096
+ *   warp_scan_cells     pairs with more cells than this are cut into units, 1..2^20
+ *   inline_face_bricks  triangles whose face box spans more 8^3 bricks go to
+ *                       the large-triangle face pass, 1..4096
+ *   dense_candidates    (triangle, brick) items with more candidate voxels are
+ *                       tested by a whole warp, the others through a shared list, 0..512
+ *   long_walk           boundary edges whose walk may take more steps are
+ *                       walked by a whole warp, 1..2^20
+ */
+typedef struct ovx_fdg_tuning
+{
+    int32_t unit_cells;
+    int32_t warp_scan_cells;
+    int32_t inline_face_bricks;
+    int32_t dense_candidates;
+    int32_t long_walk;
+} ovx_fdg_tuning;
+int ovx_fdg_set_tuning(ovx_fdg_context *ctx, const ovx_fdg_tuning *tuning);
+int ovx_fdg_get_tuning(const ovx_fdg_context *ctx, ovx_fdg_tuning *tuning);
+
+/*
  * z-order (Morton) codes, o_voxel.serialize.encode_seq / decode_seq with
  * mode='z_order' (serialize.py:7-36, src/serialize/z_order.cu:33-97,
  * src/ext.cpp:28-29): code = interleave of the low 10 bits of x, y, z with x

@@ -278,6 +278,27 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     return out;
 }
 
+// Work shapes (ovx_fdg_tuning, in field order) of the device's single-mesh and
+// batch contexts; an empty list restores the defaults.
+void set_tuning_cuda(int64_t device, const std::vector<int64_t> &values)
+{
+    TORCH_CHECK(values.empty() || values.size() == 5, "set_tuning: 5 values (or none) expected");
+    ovx_fdg_tuning t{};
+    if (!values.empty())
+    {
+        t.unit_cells = (int32_t)values[0];
+        t.warp_scan_cells = (int32_t)values[1];
+        t.inline_face_bricks = (int32_t)values[2];
+        t.dense_candidates = (int32_t)values[3];
+        t.long_walk = (int32_t)values[4];
+    }
+    for (DeviceContext *dc : {&context_for((int)device), &batch_context((int)device)})
+    {
+        std::lock_guard<std::mutex> lock(dc->mu);
+        check(ovx_fdg_set_tuning(dc->ctx, values.empty() ? nullptr : &t), dc->ctx, "set_tuning");
+    }
+}
+
 // flexible dual grid -> mesh (reference o_voxel/convert/flexible_dual_grid.py:332-477)
 std::tuple<torch::Tensor, torch::Tensor> flexible_dual_grid_to_mesh_cuda(
     const torch::Tensor &coords, const torch::Tensor &dual_vertices, const torch::Tensor &intersected,
@@ -426,6 +447,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
           py::arg("faces"), py::arg("origins"), py::arg("voxel_sizes"), py::arg("grid_ranges"), py::arg("face_weight"),
           py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("max_group_records"), py::arg("order") = 0,
           py::call_guard<py::gil_scoped_release>());
+    m.def("set_tuning_cuda", &set_tuning_cuda, py::arg("device"), py::arg("values"), py::call_guard<py::gil_scoped_release>());
     m.def("z_order_encode_cuda", &z_order_encode_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("flexible_dual_grid_to_mesh_cuda", &flexible_dual_grid_to_mesh_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("pack_flexible_dual_grid_cuda", &pack_flexible_dual_grid_cuda, py::call_guard<py::gil_scoped_release>());

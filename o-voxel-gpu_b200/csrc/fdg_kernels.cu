@@ -82,6 +82,7 @@ using namespace ovx;
 namespace
 {
 
+// Work shapes (defaults; a context may be tuned, ovx_fdg_set_tuning):
 constexpr int kInlineFaceBricks = 8; // triangles whose face box spans more bricks go to large_faces
 constexpr int kUnitCells = 64;        // cells per unit of work of a large (triangle, axis) pair
 constexpr int kThreads = 256;
@@ -296,8 +297,15 @@ __device__ __forceinline__ void brick_origin(const Grid &g, long long b, int o[3
 // ===========================================================================
 // record generation
 // ===========================================================================
+// Work shapes of the record generators (ovx_fdg_tuning).
+struct Tuning
+{
+    int unit_cells, scan_work, inline_face_bricks, dense_candidates, long_walk;
+};
+
 struct GenArgs
 {
+    Tuning tune;
     Mesh m;
     const Mesh *segs; // batched conversions: the meshes (global memory)
     int nseg;
@@ -468,6 +476,7 @@ struct EventSink
 
 constexpr int kEventThreads = 128;   // scanline pass: one (triangle, axis) per lane
 constexpr int kWarpScanWork = 256;   // (triangle, axis) pairs with more row x column work go to large_rows
+constexpr int kDenseCandidates = 32; // (triangle, brick) items with more candidates are tested by the whole warp
 
 struct EventWarp
 {
@@ -508,18 +517,18 @@ __device__ __forceinline__ uint32_t warp_exclusive_scan(uint32_t x, uint32_t &to
     return incl - x;
 }
 
-// A large (triangle, axis) pair is cut into units of about kUnitCells cells:
+// A large (triangle, axis) pair is cut into units of about `unit` cells:
 // blocks of rb rows of narrow pairs, column chunks (nch per row) of wide ones.
 struct LargeSplit
 {
     int rb, nch;
 };
 
-__device__ __forceinline__ LargeSplit large_split(int cols)
+__device__ __forceinline__ LargeSplit large_split(int cols, int unit)
 {
-    if (cols >= kUnitCells)
-        return {1, (cols + kUnitCells - 1) / kUnitCells};
-    return {kUnitCells / cols, 1};
+    if (cols >= unit)
+        return {1, (cols + unit - 1) / unit};
+    return {unit / cols, 1};
 }
 
 // The rows of the warp's (triangle, axis) pairs (lane l: nrows rows from
@@ -664,14 +673,14 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
             {
                 int clo, chi;
                 axis_col_bounds(s, g, clo, chi);
-                if ((long long)rows * (long long)(chi - clo + 1) > kWarpScanWork)
+                if ((long long)rows * (long long)(chi - clo + 1) > A.tune.scan_work)
                 {
                     if (M == COUNT)
                     {
                         const uint32_t slot = atomicAdd(&A.counters[C_SCAN_LARGE], 1u);
                         if (slot < A.scan_large_cap)
                         {
-                            const LargeSplit sp = large_split(chi - clo + 1);
+                            const LargeSplit sp = large_split(chi - clo + 1, A.tune.unit_cells);
                             A.scan_large[slot] = (uint32_t)ta;
                             A.scan_units[slot] = (uint32_t)((rows + sp.rb - 1) / sp.rb * sp.nch);
                         }
@@ -775,7 +784,7 @@ __device__ __forceinline__ uint32_t unit_owner(const uint32_t *__restrict__ unit
     return lo;
 }
 
-// Large (triangle, axis) pairs, cut into units of about kUnitCells cells (a
+// Large (triangle, axis) pairs, cut into units of about tune.unit_cells cells (a
 // block of rows, or a chunk of one row's columns): one unit per lane, 32 per
 // warp, the rows and column crossings of the warp's units spread over the
 // lanes as for the other pairs.
@@ -808,7 +817,7 @@ __global__ void __launch_bounds__(kEventThreads) large_rows(GenArgs A)
                 axis_setup(v, ax2, Ms.g, s);
                 int clo, chi;
                 axis_col_bounds(s, Ms.g, clo, chi);
-                const LargeSplit sp = large_split(chi - clo + 1);
+                const LargeSplit sp = large_split(chi - clo + 1, A.tune.unit_cells);
                 const int j = (int)((uint32_t)u - A.scan_units[i]);
                 const int ch = j % sp.nch;
                 const int r0 = s.start + (j / sp.nch) * sp.rb;
@@ -822,8 +831,8 @@ __global__ void __launch_bounds__(kEventThreads) large_rows(GenArgs A)
                             E.t[k][c][lane] = s.t[k][c];
                     E.start[lane] = r0;
                     E.mid[lane] = s.mid;
-                    E.clo[lane] = ch == 0 ? INT_MIN : clo + ch * kUnitCells;
-                    E.chi[lane] = ch == sp.nch - 1 ? INT_MAX : clo + (ch + 1) * kUnitCells;
+                    E.clo[lane] = ch == 0 ? INT_MIN : clo + ch * A.tune.unit_cells;
+                    E.chi[lane] = ch == sp.nch - 1 ? INT_MAX : clo + (ch + 1) * A.tune.unit_cells;
                     E.ta[lane] = ta;
                     E.seg[lane] = sg;
                     nrows = (uint32_t)(r1 - r0);
@@ -1048,7 +1057,7 @@ __device__ __forceinline__ void face_item(const GenArgs &A, FaceWarp &W, const i
         W.pass[w][lane] = 0u;
     // items with many candidates are tested by the whole warp with the
     // triangle's coefficients in registers; the others go through the list
-    const bool dense = cnt > 32u;
+    const bool dense = cnt > (uint32_t)A.tune.dense_candidates;
     const uint32_t dmask = __ballot_sync(0xffffffffu, dense);
     __syncwarp();
     for (uint32_t dm = dmask; dm; dm &= dm - 1u)
@@ -1185,7 +1194,7 @@ __global__ void __launch_bounds__(kFaceThreads) face_records(GenArgs A)
                 }
                 const int nx = b1[0] - b0[0] + 1, ny = b1[1] - b0[1] + 1;
                 const long long n = (long long)nx * ny * (b1[2] - b0[2] + 1);
-                if (n > kInlineFaceBricks)
+                if (n > A.tune.inline_face_bricks)
                 {
                     if (M == COUNT)
                     {
@@ -1264,7 +1273,7 @@ __global__ void __launch_bounds__(kThreads) bucket_records(const uint4 *__restri
     rec[base + k] = o;
 }
 
-// Triangles whose face box spans more than kInlineFaceBricks bricks: their
+// Triangles whose face box spans more than tune.inline_face_bricks bricks: their
 // (triangle, brick) items, all listed triangles' items one after another, 32
 // per warp and round, one per lane; each lane sets up its own item's triangle
 // and the round runs as in face_records.
@@ -1344,10 +1353,10 @@ __global__ void copy_words(const uint32_t *__restrict__ src, uint32_t *__restric
         dst[i] = src[i];
 }
 
-constexpr int kLongWalk = 64; // boundary edges with a longer step bound are walked by a whole warp
+constexpr int kLongWalk = 64; // boundary edges with a longer step bound are walked by a whole warp (default)
 
 // One thread per boundary edge: the reference DDA walk; one record per active
-// voxel visited.  Edges whose walk may take more than kLongWalk steps are
+// voxel visited.  Edges whose walk may take more than tune.long_walk steps are
 // listed (COUNT) and left to boundary_long; FILL writes every edge's line
 // quadric here.
 template <int M, bool B>
@@ -1367,7 +1376,7 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
         Dda d;
         if (!boundary_setup(v0, v1, g, d, M == FILL ? A.btab + (size_t)i * 10 : nullptr))
             continue;
-        if (d.guard > kLongWalk)
+        if (d.guard > A.tune.long_walk)
         {
             if (M == COUNT)
             {
@@ -2792,6 +2801,7 @@ struct ovx_fdg_context
     unsigned long long *seg_rows_dev = nullptr;
     int seg_cap = 0;                        // meshes the pinned buffers hold
     bool batch = false;                     // the conversion in progress is a batched one
+    Tuning tune{kUnitCells, kWarpScanWork, kInlineFaceBricks, kDenseCandidates, kLongWalk};
     unsigned long long *host = nullptr;     // readback words: pinned, mapped host memory
     unsigned long long *host_dev = nullptr; // the same words as the device addresses them
     cudaMemPool_t pool = nullptr;       // workspace pool (keeps its memory until the context is destroyed)
@@ -3170,6 +3180,7 @@ int status_to_error(ovx_fdg_context *ctx, uint32_t st)
 GenArgs make_gen(ovx_fdg_context *ctx)
 {
     GenArgs A{};
+    A.tune = ctx->tune;
     A.m = make_mesh(ctx);
     A.segs = ctx->batch ? (const Mesh *)ctx->segs_d.p : nullptr;
     A.nseg = ctx->batch ? (int)ctx->segs.size() : 0;
@@ -3619,6 +3630,35 @@ void ovx_fdg_context_destroy(ovx_fdg_context *ctx)
             cudaEventDestroy(ctx->ev[i]);
     cudaSetDevice(prev);
     delete ctx;
+}
+
+int ovx_fdg_set_tuning(ovx_fdg_context *ctx, const ovx_fdg_tuning *t)
+{
+    if (!ctx)
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (!t)
+    {
+        ctx->tune = Tuning{kUnitCells, kWarpScanWork, kInlineFaceBricks, kDenseCandidates, kLongWalk};
+        return OVX_FDG_OK;
+    }
+    if (t->unit_cells < 8 || t->unit_cells > 4096 || t->warp_scan_cells < 1 || t->warp_scan_cells > (1 << 20) ||
+        t->inline_face_bricks < 1 || t->inline_face_bricks > 4096 || t->dense_candidates < 0 ||
+        t->dense_candidates > kFaceWindow || t->long_walk < 1 || t->long_walk > (1 << 20))
+        return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "tuning value out of range");
+    ctx->tune = Tuning{t->unit_cells, t->warp_scan_cells, t->inline_face_bricks, t->dense_candidates, t->long_walk};
+    return OVX_FDG_OK;
+}
+
+int ovx_fdg_get_tuning(const ovx_fdg_context *ctx, ovx_fdg_tuning *t)
+{
+    if (!ctx || !t)
+        return OVX_FDG_INVALID_ARGUMENT;
+    t->unit_cells = ctx->tune.unit_cells;
+    t->warp_scan_cells = ctx->tune.scan_work;
+    t->inline_face_bricks = ctx->tune.inline_face_bricks;
+    t->dense_candidates = ctx->tune.dense_candidates;
+    t->long_walk = ctx->tune.long_walk;
+    return OVX_FDG_OK;
 }
 
 int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order)

@@ -24,6 +24,8 @@ from typing import Any, List, Optional, Sequence, Tuple, Union
 import numpy as np
 import torch
 
+from . import _tuning
+
 FloatArrayLike = Union[float, List[Any], Tuple[Any, ...], np.ndarray, torch.Tensor]
 IntArrayLike = Union[int, List[Any], Tuple[Any, ...], np.ndarray, torch.Tensor]
 ArrayLike = Union[List[Any], Tuple[Any, ...], np.ndarray, torch.Tensor]
@@ -82,7 +84,7 @@ def _grid_setup(vertices, faces, voxel_size, grid_size, aabb):
             assert not voxel_size.is_cuda, "voxel_size Tensor metadata must be on CPU; pass Python values to avoid implicit CUDA sync"
             voxel_size_cpu = voxel_size.to(dtype=torch.float32).contiguous()
         assert isinstance(voxel_size, torch.Tensor), f"voxel_size must be a float, list, tuple, np.ndarray, or torch.Tensor, but got {type(voxel_size)}"
-        voxel_size = voxel_size_cpu.to(device=device).contiguous()
+        voxel_size = voxel_size_cpu  # host metadata; moved to the device only for an aabb derived there
         assert voxel_size.dim() == 1, f"voxel_size must be a 1D tensor, but got {voxel_size.shape}"
         assert voxel_size.size(0) == 3, f"voxel_size must have 3 elements, but got {voxel_size.size(0)}"
 
@@ -99,7 +101,7 @@ def _grid_setup(vertices, faces, voxel_size, grid_size, aabb):
             assert not grid_size.is_cuda, "grid_size Tensor metadata must be on CPU; pass Python values to avoid implicit CUDA sync"
             grid_size_cpu = grid_size.to(dtype=torch.int32).contiguous()
         assert isinstance(grid_size, torch.Tensor), f"grid_size must be an int, list, tuple, np.ndarray, or torch.Tensor, but got {type(grid_size)}"
-        grid_size = grid_size_cpu.to(device=device).contiguous()
+        grid_size = grid_size_cpu  # host metadata; moved to the device only for an aabb derived there
         assert grid_size.dim() == 1, f"grid_size must be a 1D tensor, but got {grid_size.shape}"
         assert grid_size.size(0) == 3, f"grid_size must have 3 elements, but got {grid_size.size(0)}"
 
@@ -114,7 +116,7 @@ def _grid_setup(vertices, faces, voxel_size, grid_size, aabb):
             assert not aabb.is_cuda, "aabb Tensor metadata must be on CPU; pass Python values to avoid implicit CUDA sync"
             aabb_cpu = aabb.to(dtype=torch.float32).contiguous()
         assert isinstance(aabb, torch.Tensor), f"aabb must be a list, tuple, np.ndarray, or torch.Tensor, but got {type(aabb)}"
-        aabb = aabb_cpu.to(device=device).contiguous()
+        aabb = aabb_cpu  # host metadata: the conversion takes aabb[0] and the voxel size as host values
         assert aabb.dim() == 2, f"aabb must be a 2D tensor, but got {aabb.shape}"
         assert aabb.size(0) == 2, f"aabb must have 2 rows, but got {aabb.size(0)}"
         assert aabb.size(1) == 3, f"aabb must have 3 columns, but got {aabb.size(1)}"
@@ -123,10 +125,12 @@ def _grid_setup(vertices, faces, voxel_size, grid_size, aabb):
         min_xyz = vertices.min(dim=0).values
         max_xyz = vertices.max(dim=0).values
         if voxel_size is not None:
+            voxel_size = voxel_size.to(device=device)
             padding = torch.ceil((max_xyz - min_xyz) / voxel_size) * voxel_size - (max_xyz - min_xyz)
             min_xyz -= padding * 0.5
             max_xyz += padding * 0.5
         if grid_size is not None:
+            grid_size = grid_size.to(device=device)
             padding = (max_xyz - min_xyz) / (grid_size - 1)
             min_xyz -= padding * 0.5
             max_xyz += padding * 0.5
@@ -231,6 +235,7 @@ def mesh_to_flexible_dual_grid(
         if aabb_cpu is None:
             aabb_cpu = aabb.detach()
         vertices, faces = _upload(vertices, dev), _upload(faces, dev)
+    _tuning.apply(_ext(), vertices.device.index, max(grid_range_arg[3:]))
     if aabb_cpu is not None:
         origin = [float(x) for x in aabb_cpu[0].tolist()]
         out = _ext().mesh_to_flexible_dual_grid_cuda_ex(vertices, faces, origin, voxel_size_arg, grid_range_arg,
@@ -264,8 +269,9 @@ def intersect_occ(
     if host:
         dev = _host_device(vertices, "intersect_occ")
         vertices, faces, aabb = _upload(vertices, dev), _upload(faces, dev), aabb.to(dev)
-    vertices = vertices - aabb[0].reshape(1, 3)
+    vertices = vertices - aabb.to(vertices.device)[0].reshape(1, 3)
     triangles = vertices[faces.to(dtype=torch.long)].contiguous()
+    _tuning.apply(_ext(), vertices.device.index, max(grid_range_arg[3:]))
     out = _ext().intersect_occ_cuda(triangles, voxel_size_arg, grid_range_arg, _order_code(order))
     return _download((out,))[0] if host else out
 
@@ -339,6 +345,9 @@ def mesh_to_flexible_dual_grid_batch(
         origins.append([float(x) for x in ab_cpu[0].tolist()])
         vsizes.append(vs_arg)
         granges.append(gr_arg)
+    if verts:
+        # one set of shapes for the whole batch: the bucket of its largest grid, whose meshes dominate the work
+        _tuning.apply(_ext(), verts[0].device.index, max(max(g[3:]) for g in granges))
     out = _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
                                                        float(boundary_weight), float(regularization_weight),
                                                        int(max_group_records), _order_code(order))

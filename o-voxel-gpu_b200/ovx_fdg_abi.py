@@ -33,6 +33,8 @@ PROTOTYPES = [
     ("ovx_fdg_kernel_launches", _I64, [_P]),
     ("ovx_fdg_last_counts", ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.c_int]),
     ("ovx_fdg_set_output_order", ctypes.c_int, [_P, ctypes.c_int]),
+    ("ovx_fdg_set_tuning", ctypes.c_int, [_P, _P]),
+    ("ovx_fdg_get_tuning", ctypes.c_int, [_P, _P]),
     ("ovx_z_order_encode", ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
     ("ovx_z_order_decode", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
     ("ovx_hilbert_encode", ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
@@ -57,6 +59,14 @@ PROTOTYPES = [
 
 class Grid(ctypes.Structure):
     _fields_ = [("voxel_size", ctypes.c_float * 3), ("grid_min", ctypes.c_int32 * 3), ("grid_max", ctypes.c_int32 * 3)]
+
+
+TUNING_FIELDS = ("unit_cells", "warp_scan_cells", "inline_face_bricks", "dense_candidates", "long_walk")
+
+
+class Tuning(ctypes.Structure):
+    """ovx_fdg_tuning: work shapes of a context's conversions."""
+    _fields_ = [(name, ctypes.c_int32) for name in TUNING_FIELDS]
 
 
 class MeshDesc(ctypes.Structure):
@@ -141,6 +151,24 @@ class Context:
 
     def kernel_launches(self) -> int:
         return int(self._lib.ovx_fdg_kernel_launches(self.handle))
+
+    def set_tuning(self, tuning=None):
+        """tuning: dict of ovx_fdg_tuning fields (missing ones keep their
+        defaults), or None for the defaults."""
+        if tuning is None:
+            self._check(self._lib.ovx_fdg_set_tuning(self.handle, None), "ovx_fdg_set_tuning")
+            return
+        t = Tuning()
+        self._check(self._lib.ovx_fdg_set_tuning(self.handle, None), "ovx_fdg_set_tuning")
+        self._check(self._lib.ovx_fdg_get_tuning(self.handle, ctypes.byref(t)), "ovx_fdg_get_tuning")
+        for k, v in tuning.items():
+            setattr(t, k, int(v))
+        self._check(self._lib.ovx_fdg_set_tuning(self.handle, ctypes.byref(t)), "ovx_fdg_set_tuning")
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        self._check(self._lib.ovx_fdg_get_tuning(self.handle, ctypes.byref(t)), "ovx_fdg_get_tuning")
+        return {k: int(getattr(t, k)) for k in TUNING_FIELDS}
 
     def set_output_order(self, order: int):
         """0: brick order (default), 1: ascending z-order code."""
