@@ -107,6 +107,27 @@ enum ovx_fdg_order
 int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order);
 
 /*
+ * Arithmetic of the following full conversions (no counterpart in the
+ * reference, whose CPU path sums and solves in FP32 and whose GPU path sums
+ * with FP32 atomics).
+ * OVX_FDG_PRECISION_EXACT (default): bit-identical to the reference CPU path.
+ * OVX_FDG_PRECISION_COMPENSATED: each voxel's quadric, mass point and count
+ * are summed in FP32 with two-sum error terms (in the same order) and merged
+ * in FP64; regularisation in FP64; the FP32 solve of the rounded quadric is
+ * kept unless its error estimate -- the pivoted QR's condition estimate
+ * |R00|/|R22| x FLT_EPSILON x the voxel's distance from the grid origin in
+ * voxel edges -- exceeds route_tolerance voxel edges, in which case the voxel
+ * is solved (and box-constrained) in FP64.  Occupancy and flags are the same
+ * in both modes; dual vertices move toward the FP64 result.
+ */
+enum ovx_fdg_precision
+{
+    OVX_FDG_PRECISION_EXACT = 0,
+    OVX_FDG_PRECISION_COMPENSATED = 1
+};
+int ovx_fdg_set_precision(ovx_fdg_context *ctx, int precision, float route_tolerance);
+
+/*
  * Work shapes of a context's following conversions (no counterpart in the
  * reference, whose shapes are constants: 16x16 scan tiles,
  * intersect_qef.cu:27-28, and 8^3 bricks, types.cuh:50).  Results do not
@@ -167,8 +188,10 @@ int ovx_fdg_pack(void *stream, const int32_t *voxel_indices, const float *dual_v
 
 /* Sizes of the last conversion, known after ovx_fdg_begin: out[0] voxel rows,
  * out[1] occupied 8^3 bricks, out[2] quadric records bucketed by brick,
- * out[3] boundary edges, out[4] bricks of the grid.  Writes min(capacity, 5)
- * values and returns how many it wrote (negative status on error). */
+ * out[3] boundary edges, out[4] bricks of the grid; and, after
+ * ovx_fdg_sync_status, out[5] voxels the compensated precision mode solved
+ * in FP64.  Writes min(capacity, 6) values and returns how many it wrote
+ * (negative status on error). */
 int ovx_fdg_last_counts(const ovx_fdg_context *ctx, int64_t *out, int capacity);
 
 /*

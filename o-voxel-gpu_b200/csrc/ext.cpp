@@ -88,7 +88,8 @@ ovx_fdg_grid make_grid(const std::vector<float> &voxel_size, const std::vector<i
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Tensor &vertices, const torch::Tensor &faces,
                                                                  const float *origin, const std::vector<float> &voxel_size,
                                                                  const std::vector<int64_t> &grid_range, float face_weight,
-                                                                 float boundary_weight, float regularization_weight, int64_t order)
+                                                                 float boundary_weight, float regularization_weight, int64_t order,
+                                                                 int64_t precision, double route_tolerance)
 {
     TORCH_CHECK(vertices.is_cuda(), "vertices must be a CUDA tensor");
     TORCH_CHECK(faces.is_cuda(), "faces must be a CUDA tensor");
@@ -106,6 +107,7 @@ std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> run_fdg(const torch::Ten
     DeviceContext &dc = context_for(device);
     std::lock_guard<std::mutex> lock(dc.mu);
     check(ovx_fdg_set_output_order(dc.ctx, (int)order), dc.ctx, "mesh_to_flexible_dual_grid (order)");
+    check(ovx_fdg_set_precision(dc.ctx, (int)precision, (float)route_tolerance), dc.ctx, "mesh_to_flexible_dual_grid (precision)");
     int64_t n = 0;
     check(ovx_fdg_begin(dc.ctx, stream, v.data_ptr<float>(), v.size(0), f.numel() ? f.data_ptr() : nullptr,
                         f.scalar_type() == torch::kInt64 ? 8 : 4, f.size(0), origin, &grid, face_weight, boundary_weight,
@@ -155,19 +157,21 @@ int64_t estimated_records(const ovx_fdg_grid &g, int64_t faces)
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> mesh_to_flexible_dual_grid_cuda(
     const torch::Tensor &vertices, const torch::Tensor &faces, const std::vector<float> &voxel_size,
     const std::vector<int64_t> &grid_range, float face_weight, float boundary_weight, float regularization_weight,
-    int64_t order)
+    int64_t order, int64_t precision, double route_tolerance)
 {
-    return run_fdg(vertices, faces, nullptr, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight, order);
+    return run_fdg(vertices, faces, nullptr, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight, order,
+                   precision, route_tolerance);
 }
 
 std::tuple<torch::Tensor, torch::Tensor, torch::Tensor> mesh_to_flexible_dual_grid_cuda_ex(
     const torch::Tensor &vertices, const torch::Tensor &faces, const std::vector<float> &origin,
     const std::vector<float> &voxel_size, const std::vector<int64_t> &grid_range, float face_weight, float boundary_weight,
-    float regularization_weight, int64_t order)
+    float regularization_weight, int64_t order, int64_t precision, double route_tolerance)
 {
     TORCH_CHECK(origin.size() == 3, "origin must have 3 elements");
     const float o[3] = {origin[0], origin[1], origin[2]};
-    return run_fdg(vertices, faces, o, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight, order);
+    return run_fdg(vertices, faces, o, voxel_size, grid_range, face_weight, boundary_weight, regularization_weight, order,
+                   precision, route_tolerance);
 }
 
 torch::Tensor intersect_occ_cuda(const torch::Tensor &triangles, const std::vector<float> &voxel_size,
@@ -196,7 +200,7 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     const std::vector<torch::Tensor> &vertices, const std::vector<torch::Tensor> &faces,
     const std::vector<std::vector<float>> &origins, const std::vector<std::vector<float>> &voxel_sizes,
     const std::vector<std::vector<int64_t>> &grid_ranges, float face_weight, float boundary_weight,
-    float regularization_weight, int64_t max_group_records, int64_t order)
+    float regularization_weight, int64_t max_group_records, int64_t order, int64_t precision, double route_tolerance)
 {
     const size_t n = vertices.size();
     TORCH_CHECK(faces.size() == n && origins.size() == n && voxel_sizes.size() == n && grid_ranges.size() == n,
@@ -235,6 +239,8 @@ std::vector<std::tuple<torch::Tensor, torch::Tensor, torch::Tensor>> mesh_to_fle
     DeviceContext &dc = batch_context(device);
     std::lock_guard<std::mutex> lock(dc.mu);
     check(ovx_fdg_set_output_order(dc.ctx, (int)order), dc.ctx, "mesh_to_flexible_dual_grid_batch (order)");
+    check(ovx_fdg_set_precision(dc.ctx, (int)precision, (float)route_tolerance), dc.ctx,
+          "mesh_to_flexible_dual_grid_batch (precision)");
     static const bool sync_check = std::getenv("OVX_FDG_CHECK") != nullptr;
     auto opts = torch::TensorOptions().device(dev);
     // groups of consecutive meshes whose expected records stay within the
@@ -436,17 +442,18 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m)
     // first seven arguments are the reference operator's
     m.def("mesh_to_flexible_dual_grid_cuda", &mesh_to_flexible_dual_grid_cuda, py::arg("vertices"), py::arg("faces"),
           py::arg("voxel_size"), py::arg("grid_range"), py::arg("face_weight"), py::arg("boundary_weight"),
-          py::arg("regularization_weight"), py::arg("order") = 0, py::call_guard<py::gil_scoped_release>());
+          py::arg("regularization_weight"), py::arg("order") = 0, py::arg("precision") = 0, py::arg("route_tolerance") = 1e-3,
+          py::call_guard<py::gil_scoped_release>());
     m.def("mesh_to_flexible_dual_grid_cuda_ex", &mesh_to_flexible_dual_grid_cuda_ex, py::arg("vertices"), py::arg("faces"),
           py::arg("origin"), py::arg("voxel_size"), py::arg("grid_range"), py::arg("face_weight"),
-          py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("order") = 0,
-          py::call_guard<py::gil_scoped_release>());
+          py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("order") = 0, py::arg("precision") = 0,
+          py::arg("route_tolerance") = 1e-3, py::call_guard<py::gil_scoped_release>());
     m.def("intersect_occ_cuda", &intersect_occ_cuda, py::arg("triangles"), py::arg("voxel_size"), py::arg("grid_range"),
           py::arg("order") = 0, py::call_guard<py::gil_scoped_release>());
     m.def("mesh_to_flexible_dual_grid_cuda_batch", &mesh_to_flexible_dual_grid_cuda_batch, py::arg("vertices"),
           py::arg("faces"), py::arg("origins"), py::arg("voxel_sizes"), py::arg("grid_ranges"), py::arg("face_weight"),
           py::arg("boundary_weight"), py::arg("regularization_weight"), py::arg("max_group_records"), py::arg("order") = 0,
-          py::call_guard<py::gil_scoped_release>());
+          py::arg("precision") = 0, py::arg("route_tolerance") = 1e-3, py::call_guard<py::gil_scoped_release>());
     m.def("set_tuning_cuda", &set_tuning_cuda, py::arg("device"), py::arg("values"), py::call_guard<py::gil_scoped_release>());
     m.def("z_order_encode_cuda", &z_order_encode_cuda, py::call_guard<py::gil_scoped_release>());
     m.def("flexible_dual_grid_to_mesh_cuda", &flexible_dual_grid_to_mesh_cuda, py::call_guard<py::gil_scoped_release>());

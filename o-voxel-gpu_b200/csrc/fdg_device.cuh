@@ -570,10 +570,48 @@ __device__ __forceinline__ bool dda_step(Dda &d)
 // Per-voxel solve (flexible_dual_grid.cpp:766-983)
 // ---------------------------------------------------------------------------
 // Column-pivoting Householder QR solve, A row-major n x n (n = 2 or 3).
-template <int N>
-__device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float *x)
+// Scalar arithmetic of the solves: the float members are the exact path's
+// operations (Eigen's fixed-size reduction orders), the double ones serve the
+// compensated-precision mode.
+template <typename T>
+struct Arith;
+
+template <>
+struct Arith<float>
 {
-    float qr[N * N], c[N], h[N], nu[N], nd[N];
+    static __device__ __forceinline__ float eps() { return FLT_EPSILON; }
+    static __device__ __forceinline__ float tiny() { return FLT_MIN; }
+    static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float abs(float x) { return fabsf(x); }
+    static __device__ __forceinline__ float dot3(float a0, float a1, float a2, float b0, float b1, float b2)
+    {
+        return dot3f(a0, a1, a2, b0, b1, b2);
+    }
+    static __device__ __forceinline__ float dot4(const float a[4], const float b[4]) { return dot4v(a, b); }
+};
+
+template <>
+struct Arith<double>
+{
+    static __device__ __forceinline__ double eps() { return DBL_EPSILON; }
+    static __device__ __forceinline__ double tiny() { return DBL_MIN; }
+    static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double abs(double x) { return fabs(x); }
+    static __device__ __forceinline__ double dot3(double a0, double a1, double a2, double b0, double b1, double b2)
+    {
+        return (a0 * b0 + a1 * b1) + a2 * b2;
+    }
+    static __device__ __forceinline__ double dot4(const double a[4], const double b[4])
+    {
+        return ((a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]) + a[3] * b[3];
+    }
+};
+
+template <typename T, int N>
+__device__ __forceinline__ void cpqr_solve_t(const T *A, const T *b, T *x, T *rdiag = nullptr)
+{
+    using Ar = Arith<T>;
+    T qr[N * N], c[N], h[N], nu[N], nd[N];
     int perm[N];
 #pragma unroll
     for (int i = 0; i < N * N; ++i)
@@ -583,31 +621,31 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
     {
         c[i] = b[i];
         perm[i] = i;
-        x[i] = 0.0f;
+        x[i] = T(0);
     }
 #pragma unroll
     for (int j = 0; j < N; ++j)
     {
-        float s;
+        T s;
         if (N == 3)
             s = qr[0 * N + j] * qr[0 * N + j] + (qr[1 * N + j] * qr[1 * N + j] + qr[2 * N + j] * qr[2 * N + j]);
         else
             s = qr[0 * N + j] * qr[0 * N + j] + qr[1 * N + j] * qr[1 * N + j];
-        nd[j] = nu[j] = sqrtf(s);
+        nd[j] = nu[j] = Ar::sqrt(s);
     }
-    float maxn = nu[0];
+    T maxn = nu[0];
 #pragma unroll
     for (int j = 1; j < N; ++j)
         if (nu[j] > maxn)
             maxn = nu[j];
-    const float th = (maxn * FLT_EPSILON) * (maxn * FLT_EPSILON) / (float)N;
-    const float downdate_th = sqrtf(FLT_EPSILON);
+    const T th = (maxn * Ar::eps()) * (maxn * Ar::eps()) / (T)N;
+    const T downdate_th = Ar::sqrt(Ar::eps());
     int nz = N;
 #pragma unroll
     for (int k = 0; k < N; ++k)
     {
         int bi = k;
-        float bv = nu[k];
+        T bv = nu[k];
 #pragma unroll
         for (int j = k + 1; j < N; ++j)
             if (nu[j] > bv)
@@ -615,14 +653,14 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
                 bv = nu[j];
                 bi = j;
             }
-        if (nz == N && bv * bv < th * (float)(N - k))
+        if (nz == N && bv * bv < th * (T)(N - k))
             nz = k;
         if (bi != k)
         {
 #pragma unroll
             for (int r = 0; r < N; ++r)
             {
-                const float t = qr[r * N + k];
+                const T t = qr[r * N + k];
                 // bi is data dependent; select instead of dynamic indexing keeps arrays in registers
 #pragma unroll
                 for (int j = k + 1; j < N; ++j)
@@ -636,7 +674,7 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
             for (int j = k + 1; j < N; ++j)
                 if (j == bi)
                 {
-                    float t = nu[k];
+                    T t = nu[k];
                     nu[k] = nu[j];
                     nu[j] = t;
                     t = nd[k];
@@ -648,29 +686,29 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
                 }
         }
         const int len = N - k - 1;
-        const float c0 = qr[k * N + k];
-        float tsq = 0.0f;
+        const T c0 = qr[k * N + k];
+        T tsq = T(0);
 #pragma unroll
         for (int i = 0; i < len; ++i)
         {
-            const float e = qr[(k + 1 + i) * N + k];
+            const T e = qr[(k + 1 + i) * N + k];
             tsq = (i == 0) ? e * e : tsq + e * e;
         }
-        float tau, beta;
-        if (tsq <= FLT_MIN)
+        T tau, beta;
+        if (tsq <= Ar::tiny())
         {
-            tau = 0.0f;
+            tau = T(0);
             beta = c0;
 #pragma unroll
             for (int i = 0; i < len; ++i)
-                qr[(k + 1 + i) * N + k] = 0.0f;
+                qr[(k + 1 + i) * N + k] = T(0);
         }
         else
         {
-            beta = sqrtf(c0 * c0 + tsq);
-            if (c0 >= 0.0f)
+            beta = Ar::sqrt(c0 * c0 + tsq);
+            if (c0 >= T(0))
                 beta = -beta;
-            const float den = c0 - beta;
+            const T den = c0 - beta;
 #pragma unroll
             for (int i = 0; i < len; ++i)
                 qr[(k + 1 + i) * N + k] = qr[(k + 1 + i) * N + k] / den;
@@ -678,16 +716,16 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
         }
         qr[k * N + k] = beta;
         h[k] = tau;
-        if (len > 0 && tau != 0.0f)
+        if (len > 0 && tau != T(0))
         {
 #pragma unroll
             for (int j = k + 1; j < N; ++j)
             {
-                float tmp = 0.0f;
+                T tmp = T(0);
 #pragma unroll
                 for (int i = 0; i < len; ++i)
                 {
-                    const float p = qr[(k + 1 + i) * N + k] * qr[(k + 1 + i) * N + j];
+                    const T p = qr[(k + 1 + i) * N + k] * qr[(k + 1 + i) * N + j];
                     tmp = (i == 0) ? p : tmp + p;
                 }
                 tmp = tmp + qr[k * N + j];
@@ -700,30 +738,36 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
 #pragma unroll
         for (int j = k + 1; j < N; ++j)
         {
-            if (nu[j] != 0.0f)
+            if (nu[j] != T(0))
             {
-                float temp = fabsf(qr[k * N + j]) / nu[j];
-                temp = (1.0f + temp) * (1.0f - temp);
-                temp = temp < 0.0f ? 0.0f : temp;
-                const float ratio = nu[j] / nd[j];
-                const float temp2 = temp * (ratio * ratio);
+                T temp = Ar::abs(qr[k * N + j]) / nu[j];
+                temp = (T(1) + temp) * (T(1) - temp);
+                temp = temp < T(0) ? T(0) : temp;
+                const T ratio = nu[j] / nd[j];
+                const T temp2 = temp * (ratio * ratio);
                 if (temp2 <= downdate_th)
                 {
-                    float s = 0.0f;
+                    T s = T(0);
 #pragma unroll
                     for (int r = k + 1; r < N; ++r)
                     {
-                        const float e = qr[r * N + j];
+                        const T e = qr[r * N + j];
                         s = (r == k + 1) ? e * e : s + e * e;
                     }
-                    nd[j] = nu[j] = sqrtf(s);
+                    nd[j] = nu[j] = Ar::sqrt(s);
                 }
                 else
                 {
-                    nu[j] = nu[j] * sqrtf(temp);
+                    nu[j] = nu[j] * Ar::sqrt(temp);
                 }
             }
         }
+    }
+    if (rdiag)
+    {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            rdiag[k] = qr[k * N + k];
     }
     if (nz == 0)
         return;
@@ -733,18 +777,18 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
         if (k >= nz)
             break;
         const int len = N - k - 1;
-        const float tau = h[k];
+        const T tau = h[k];
         if (len == 0)
         {
-            c[k] = c[k] * (1.0f - tau);
+            c[k] = c[k] * (T(1) - tau);
         }
-        else if (tau != 0.0f)
+        else if (tau != T(0))
         {
-            float tmp = 0.0f;
+            T tmp = T(0);
 #pragma unroll
             for (int i = 0; i < len; ++i)
             {
-                const float p = qr[(k + 1 + i) * N + k] * c[k + 1 + i];
+                const T p = qr[(k + 1 + i) * N + k] * c[k + 1 + i];
                 tmp = (i == 0) ? p : tmp + p;
             }
             tmp = tmp + c[k];
@@ -757,7 +801,7 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
 #pragma unroll
     for (int i = N - 1; i >= 0; --i)
     {
-        if (i < nz && c[i] != 0.0f)
+        if (i < nz && c[i] != T(0))
         {
             c[i] = c[i] / qr[i * N + i];
 #pragma unroll
@@ -768,7 +812,7 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
 #pragma unroll
     for (int i = 0; i < N; ++i)
     {
-        const float val = (i < nz) ? c[i] : 0.0f;
+        const T val = (i < nz) ? c[i] : T(0);
 #pragma unroll
         for (int j = 0; j < N; ++j)
             if (perm[i] == j)
@@ -776,93 +820,115 @@ __device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float
     }
 }
 
-__device__ __forceinline__ float qef_err4(const float Q[16], const float p[4])
+
+template <int N>
+__device__ __forceinline__ void cpqr_solve(const float *A, const float *b, float *x)
 {
-    float r[4];
+    cpqr_solve_t<float, N>(A, b, x);
+}
+
+template <typename T>
+__device__ __forceinline__ T qef_err4_t(const T Q[16], const T p[4])
+{
+    T r[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
     {
-        const float col[4] = {Q[0 * 4 + j], Q[1 * 4 + j], Q[2 * 4 + j], Q[3 * 4 + j]};
-        r[j] = dot4v(p, col);
+        const T col[4] = {Q[0 * 4 + j], Q[1 * 4 + j], Q[2 * 4 + j], Q[3 * 4 + j]};
+        r[j] = Arith<T>::dot4(p, col);
     }
-    return dot4v(r, p);
+    return Arith<T>::dot4(r, p);
 }
 
 // Regularisation toward the mass point (flexible_dual_grid.cpp:780-792): Q += (rw*cnt) * Qreg.
-__device__ __forceinline__ void regularize(const float q_in[10], const float mean[3], float cnt, float rw, float q[10])
+template <typename T>
+__device__ __forceinline__ void regularize_t(const T q_in[10], const T mean[3], T cnt, T rw, T q[10])
 {
 #pragma unroll
     for (int i = 0; i < 10; ++i)
         q[i] = q_in[i];
-    if (rw > 0.0f)
+    if (rw > T(0))
     {
-        const float p0 = mean[0] / cnt, p1 = mean[1] / cnt, p2 = mean[2] / cnt;
-        const float s = rw * cnt;
-        const float pp = dot3f(p0, p1, p2, p0, p1, p2);
-        q[0] = q[0] + s * 1.0f;
-        q[1] = q[1] + s * 0.0f;
-        q[2] = q[2] + s * 0.0f;
+        const T p0 = mean[0] / cnt, p1 = mean[1] / cnt, p2 = mean[2] / cnt;
+        const T s = rw * cnt;
+        const T pp = Arith<T>::dot3(p0, p1, p2, p0, p1, p2);
+        q[0] = q[0] + s * T(1);
+        q[1] = q[1] + s * T(0);
+        q[2] = q[2] + s * T(0);
         q[3] = q[3] + s * (-p0);
-        q[4] = q[4] + s * 1.0f;
-        q[5] = q[5] + s * 0.0f;
+        q[4] = q[4] + s * T(1);
+        q[5] = q[5] + s * T(0);
         q[6] = q[6] + s * (-p1);
-        q[7] = q[7] + s * 1.0f;
+        q[7] = q[7] + s * T(1);
         q[8] = q[8] + s * (-p2);
         q[9] = q[9] + s * pp;
     }
 }
 
-__device__ __forceinline__ void voxel_box(const int coord[3], const Grid &g, float mn[3], float mx[3])
+__device__ __forceinline__ void regularize(const float q_in[10], const float mean[3], float cnt, float rw, float q[10])
+{
+    regularize_t<float>(q_in, mean, cnt, rw, q);
+}
+
+template <typename T>
+__device__ __forceinline__ void voxel_box_t(const int coord[3], const Grid &g, T mn[3], T mx[3])
 {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
     {
-        mn[i] = (float)coord[i] * g.vs[i];
-        mx[i] = (float)(coord[i] + 1) * g.vs[i];
+        mn[i] = (T)((float)coord[i] * g.vs[i]);
+        mx[i] = (T)((float)(coord[i] + 1) * g.vs[i]);
     }
 }
 
 // Unconstrained minimiser A v = -b (flexible_dual_grid.cpp:795-797); true if it lies in the voxel box.
+template <typename T>
+__device__ __forceinline__ bool solve_unconstrained_t(const int coord[3], const Grid &g, const T q[10], T v[3], T *rdiag = nullptr)
+{
+    const T A[9] = {q[0], q[1], q[2], q[1], q[4], q[5], q[2], q[5], q[7]};
+    const T bb[3] = {-q[3], -q[6], -q[8]};
+    cpqr_solve_t<T, 3>(A, bb, v, rdiag);
+    T mn[3], mx[3];
+    voxel_box_t<T>(coord, g, mn, mx);
+    return v[0] >= mn[0] && v[0] <= mx[0] && v[1] >= mn[1] && v[1] <= mx[1] && v[2] >= mn[2] && v[2] <= mx[2];
+}
+
 __device__ __forceinline__ bool solve_unconstrained(const int coord[3], const Grid &g, const float q[10], float v[3])
 {
-    const float A[9] = {q[0], q[1], q[2], q[1], q[4], q[5], q[2], q[5], q[7]};
-    const float bb[3] = {-q[3], -q[6], -q[8]};
-    cpqr_solve<3>(A, bb, v);
-    float mn[3], mx[3];
-    voxel_box(coord, g, mn, mx);
-    return v[0] >= mn[0] && v[0] <= mx[0] && v[1] >= mn[1] && v[1] <= mx[1] && v[2] >= mn[2] && v[2] <= mx[2];
+    return solve_unconstrained_t<float>(coord, g, q, v);
 }
 
 // Constrained search over the box faces, edges and corners (flexible_dual_grid.cpp:799-979),
 // starting from the unconstrained solution, strict `<` in the reference order.
-__device__ __forceinline__ void solve_constrained(const int coord[3], const Grid &g, const float q[10], float v[3])
+template <typename T>
+__device__ __forceinline__ void solve_constrained_t(const int coord[3], const Grid &g, const T q[10], T v[3])
 {
-    solve_unconstrained(coord, g, q, v);
-    float mn[3], mx[3];
-    voxel_box(coord, g, mn, mx);
-    const float Q[16] = {q[0], q[1], q[2], q[3], q[1], q[4], q[5], q[6], q[2], q[5], q[7], q[8], q[3], q[6], q[8], q[9]};
-    float best = __int_as_float(0x7f800000);
+    solve_unconstrained_t<T>(coord, g, q, v);
+    T mn[3], mx[3];
+    voxel_box_t<T>(coord, g, mn, mx);
+    const T Q[16] = {q[0], q[1], q[2], q[3], q[1], q[4], q[5], q[6], q[2], q[5], q[7], q[8], q[3], q[6], q[8], q[9]};
+    T best = (T)__int_as_float(0x7f800000);
 #pragma unroll 1
     for (int fa = 0; fa < 3; ++fa)
     {
         const int a1 = (fa + 1) % 3, a2 = (fa + 2) % 3;
-        const float A2[4] = {Q[a1 * 4 + a1], Q[a1 * 4 + a2], Q[a2 * 4 + a1], Q[a2 * 4 + a2]};
-        const float B2[4] = {Q[a1 * 4 + fa], Q[a1 * 4 + 3], Q[a2 * 4 + fa], Q[a2 * 4 + 3]};
+        const T A2[4] = {Q[a1 * 4 + a1], Q[a1 * 4 + a2], Q[a2 * 4 + a1], Q[a2 * 4 + a2]};
+        const T B2[4] = {Q[a1 * 4 + fa], Q[a1 * 4 + 3], Q[a2 * 4 + fa], Q[a2 * 4 + 3]};
 #pragma unroll 1
         for (int bound = 0; bound < 2; ++bound)
         {
-            const float fv = bound == 0 ? mn[fa] : mx[fa];
-            const float rhs[2] = {(-B2[0]) * fv + (-B2[1]) * 1.0f, (-B2[2]) * fv + (-B2[3]) * 1.0f};
-            float x2[2];
-            cpqr_solve<2>(A2, rhs, x2);
+            const T fv = bound == 0 ? mn[fa] : mx[fa];
+            const T rhs[2] = {(-B2[0]) * fv + (-B2[1]) * T(1), (-B2[2]) * fv + (-B2[3]) * T(1)};
+            T x2[2];
+            cpqr_solve_t<T, 2>(A2, rhs, x2);
             if (x2[0] >= mn[a1] && x2[0] <= mx[a1] && x2[1] >= mn[a2] && x2[1] <= mx[a2])
             {
-                float p[4];
+                T p[4];
                 p[fa] = fv;
                 p[a1] = x2[0];
                 p[a2] = x2[1];
-                p[3] = 1.0f;
-                const float err = qef_err4(Q, p);
+                p[3] = T(1);
+                const T err = qef_err4_t<T>(Q, p);
                 if (err < best)
                 {
                     best = err;
@@ -877,22 +943,22 @@ __device__ __forceinline__ void solve_constrained(const int coord[3], const Grid
     for (int fr = 0; fr < 3; ++fr)
     {
         const int a1 = (fr + 1) % 3, a2 = (fr + 2) % 3;
-        const float a = Q[fr * 4 + fr];
-        const float b0 = Q[fr * 4 + a1], b1 = Q[fr * 4 + a2], b2 = Q[fr * 4 + 3];
+        const T a = Q[fr * 4 + fr];
+        const T b0 = Q[fr * 4 + a1], b1 = Q[fr * 4 + a2], b2 = Q[fr * 4 + 3];
 #pragma unroll 1
         for (int cc = 0; cc < 4; ++cc)
         {
-            const float u1 = (cc >> 1) == 0 ? mn[a1] : mx[a1];
-            const float u2 = (cc & 1) == 0 ? mn[a2] : mx[a2];
-            const float xf = -(dot3f(b0, b1, b2, u1, u2, 1.0f)) / a;
+            const T u1 = (cc >> 1) == 0 ? mn[a1] : mx[a1];
+            const T u2 = (cc & 1) == 0 ? mn[a2] : mx[a2];
+            const T xf = -(Arith<T>::dot3(b0, b1, b2, u1, u2, T(1))) / a;
             if (xf >= mn[fr] && xf <= mx[fr])
             {
-                float p[4];
+                T p[4];
                 p[fr] = xf;
                 p[a1] = u1;
                 p[a2] = u2;
-                p[3] = 1.0f;
-                const float err = qef_err4(Q, p);
+                p[3] = T(1);
+                const T err = qef_err4_t<T>(Q, p);
                 if (err < best)
                 {
                     best = err;
@@ -906,12 +972,12 @@ __device__ __forceinline__ void solve_constrained(const int coord[3], const Grid
 #pragma unroll 1
     for (int cn = 0; cn < 8; ++cn)
     {
-        float p[4];
+        T p[4];
         p[0] = (cn & 4) ? mn[0] : mx[0];
         p[1] = (cn & 2) ? mn[1] : mx[1];
         p[2] = (cn & 1) ? mn[2] : mx[2];
-        p[3] = 1.0f;
-        const float err = qef_err4(Q, p);
+        p[3] = T(1);
+        const T err = qef_err4_t<T>(Q, p);
         if (err < best)
         {
             best = err;
@@ -920,6 +986,11 @@ __device__ __forceinline__ void solve_constrained(const int coord[3], const Grid
             v[2] = p[2];
         }
     }
+}
+
+__device__ __forceinline__ void solve_constrained(const int coord[3], const Grid &g, const float q[10], float v[3])
+{
+    solve_constrained_t<float>(coord, g, q, v);
 }
 
 } // namespace ovx

@@ -76,6 +76,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <type_traits>
 
 using namespace ovx;
 
@@ -111,7 +112,8 @@ enum
     C_LUNITS = 9,  // units of work of the large (triangle, axis) pairs
     C_FUNITS = 10, // units of work of the large triangles' face boxes
     C_BLONG = 11,  // boundary edges walked by a whole warp
-    C_WORDS = 12
+    C_ROUTED = 12, // compensated precision: voxels solved in FP64
+    C_WORDS = 13
 };
 enum
 {
@@ -1711,6 +1713,7 @@ struct SolveArgs
     unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40 | sorted << 63
     float *clist; // deferred constrained searches, 16 words each
     uint32_t clist_cap;
+    float route_tol; // compensated precision: FP32 solve error (voxel edges) above which a voxel is solved in FP64
 };
 
 // Rank of active voxel lv among the brick's voxels in output order.
@@ -2137,6 +2140,115 @@ __device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int
 
 // Regularise and solve one voxel (flexible_dual_grid.cpp:763-797); a voxel whose
 // unconstrained solution leaves its box goes to the constrained-search list.
+// Compensated sums (precision mode "compensated"): each of the 14 running sums
+// (quadric, mass point, count) keeps its float value and the float error of
+// its additions (Knuth's TwoSum, exact without contraction), merged in double
+// at the end.
+struct AccC
+{
+    float s[14], e[14];
+    uint32_t flags;
+};
+
+__device__ __forceinline__ void acc_init(AccC &a)
+{
+#pragma unroll
+    for (int i = 0; i < 14; ++i)
+        a.s[i] = a.e[i] = 0.0f;
+    a.flags = 0;
+}
+
+__device__ __forceinline__ void two_sum_add(float &s, float &e, float x)
+{
+    const float t = s + x;
+    const float bp = t - s;
+    e = e + ((s - (t - bp)) + (x - bp));
+    s = t;
+}
+
+__device__ __forceinline__ void contrib_apply(const Contrib &c, AccC &a)
+{
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        two_sum_add(a.s[i], a.e[i], c.q[i]);
+    if (c.stage == 0)
+    {
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            two_sum_add(a.s[10 + i], a.e[10 + i], c.p[i]);
+        two_sum_add(a.s[13], a.e[13], 1.0f);
+        a.flags |= c.flag;
+    }
+}
+
+__device__ __forceinline__ void voxel_finish(const SolveArgs &A, const Grid &g, long long row, const int vc[3], const Acc &a);
+
+// Compensated precision: sums merged and regularised in double; the FP32
+// solve of the rounded quadric is kept unless its error estimate -- the
+// pivoted QR's condition estimate |R00|/|R22| times FLT_EPSILON times the
+// voxel's distance from the grid origin in voxel edges -- exceeds
+// A.route_tol voxel edges, in which case the voxel is solved (and, if
+// needed, box-constrained) in double.
+__device__ __forceinline__ void voxel_finish(const SolveArgs &A, const Grid &g, long long row, const int vc[3], const AccC &a)
+{
+    double qd[10], md[3];
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        qd[i] = (double)a.s[i] + (double)a.e[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        md[i] = (double)a.s[10 + i] + (double)a.e[10 + i];
+    const double cd = (double)a.s[13] + (double)a.e[13];
+    double qr[10];
+    regularize_t<double>(qd, md, cd, (double)A.rw, qr);
+    A.flags[row * 3 + 0] = (uint8_t)(a.flags & 1u);
+    A.flags[row * 3 + 1] = (uint8_t)((a.flags >> 1) & 1u);
+    A.flags[row * 3 + 2] = (uint8_t)((a.flags >> 2) & 1u);
+    float qf[10];
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        qf[i] = (float)qr[i];
+    float v[3], rd[3];
+    const bool inside = solve_unconstrained_t<float>(vc, g, qf, v, rd);
+    float ext = 1.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        ext = fmaxf(ext, fabsf((float)vc[i]) + 1.0f);
+    const float r0 = fabsf(rd[0]), r2 = fabsf(rd[2]);
+    if (!(r2 > 0.0f) || (r0 / r2) * FLT_EPSILON * ext > A.route_tol)
+    {
+        atomicAdd(&A.counters[C_ROUTED], 1u);
+        double vd[3];
+        if (!solve_unconstrained_t<double>(vc, g, qr, vd))
+            solve_constrained_t<double>(vc, g, qr, vd);
+        A.dual[row * 3 + 0] = (float)vd[0];
+        A.dual[row * 3 + 1] = (float)vd[1];
+        A.dual[row * 3 + 2] = (float)vd[2];
+        return;
+    }
+    if (inside)
+    {
+        A.dual[row * 3 + 0] = v[0];
+        A.dual[row * 3 + 1] = v[1];
+        A.dual[row * 3 + 2] = v[2];
+        return;
+    }
+    const uint32_t slot = atomicAdd(&A.counters[C_CONSTRAINED], 1u);
+    if (slot >= A.clist_cap)
+    {
+        atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+        return;
+    }
+    float *c = A.clist + (size_t)slot * 16;
+    c[0] = __int_as_float((int)row);
+    c[1] = __int_as_float(vc[0]);
+    c[2] = __int_as_float(vc[1]);
+    c[3] = __int_as_float(vc[2]);
+#pragma unroll
+    for (int i = 0; i < 10; ++i)
+        c[4 + i] = qf[i];
+}
+
 __device__ __forceinline__ void voxel_finish(const SolveArgs &A, const Grid &g, long long row, const int vc[3], const Acc &a)
 {
     float q[10];
@@ -2175,9 +2287,11 @@ constexpr int kLongMidMax = 1024;                    // ... one CTA of 128 threa
 constexpr int kLongHugeMax = 8192;                   // ... one CTA of 256 threads; longer: in-place insertion sort
 
 // 12 resident CTAs per SM (at most 40 registers): the sums wait on gathers,
-// and the extra warps hide more of that than the few spills cost
-template <bool B>
-__global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long long nrows)
+// and the extra warps hide more of that than the few spills cost; the
+// compensated-precision variant, with twice the running sums and an FP64
+// solve, gets 4 (128 registers)
+template <bool B, int P>
+__global__ void __launch_bounds__(128, P == 0 ? 12 : 4) voxel_accumulate(SolveArgs A, long long nrows)
 {
     const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -2271,7 +2385,7 @@ __global__ void __launch_bounds__(128, 12) voxel_accumulate(SolveArgs A, long lo
                 lst[j] = e;
         }
     }
-    Acc a;
+    std::conditional_t<P == 0, Acc, AccC> a;
     acc_init(a);
     for (uint32_t x = 0; x < n; ++x)
     {
@@ -2296,7 +2410,7 @@ constexpr size_t long_smem()
 // thread.  Lists longer than kMax are insertion-sorted in place (slow,
 // correct).
 // kHuge = false: lists of up to kLongMidMax entries (front of longv); true: longer lists (back of longv).
-template <int kMax, int kThreadsT, bool kHuge, bool B>
+template <int kMax, int kThreadsT, bool kHuge, bool B, int P>
 __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
 {
     extern __shared__ unsigned long long lsm[];
@@ -2314,7 +2428,7 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
         const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
         const Grid &g = mesh_of<B>(A, seg_of_row<B>(A, row)).g;
         uint4 *lst = A.contrib + first;
-        Acc a;
+        std::conditional_t<P == 0, Acc, AccC> a;
         acc_init(a);
         if (n <= (uint32_t)kMax)
         {
@@ -2802,6 +2916,8 @@ struct ovx_fdg_context
     int seg_cap = 0;                        // meshes the pinned buffers hold
     bool batch = false;                     // the conversion in progress is a batched one
     Tuning tune{kUnitCells, kWarpScanWork, kInlineFaceBricks, kDenseCandidates, kLongWalk};
+    int precision = 0;       // OVX_FDG_PRECISION_*
+    float route_tol = 1e-3f; // compensated precision: FP32 solve error estimate (voxel edges) that routes a voxel to FP64
     unsigned long long *host = nullptr;     // readback words: pinned, mapped host memory
     unsigned long long *host_dev = nullptr; // the same words as the device addresses them
     cudaMemPool_t pool = nullptr;       // workspace pool (keeps its memory until the context is destroyed)
@@ -3512,7 +3628,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
 
 // The per-brick lists, the per-voxel sums and solves, and the constrained
 // search of a conversion (single mesh or batch).
-template <bool B>
+template <bool B, int P>
 int launch_consume(ovx_fdg_context *ctx, const SolveArgs &SA, cudaStream_t st, long long n)
 {
     if (ctx->n_active > 0)
@@ -3521,13 +3637,13 @@ int launch_consume(ovx_fdg_context *ctx, const SolveArgs &SA, cudaStream_t st, l
         ++ctx->launches;
     }
     stage(ctx, EV_CONSUME, st);
-    voxel_accumulate<B><<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
+    voxel_accumulate<B, P><<<blocks_for(n, 128), 128, 0, st>>>(SA, n);
     // one CTA per long list, at most one per row
-    voxel_accumulate_long<kLongMidMax, 128, false, B>
+    voxel_accumulate_long<kLongMidMax, 128, false, B, P>
         <<<(unsigned)std::min<long long>(ctx->sms * 8, n), 128, long_smem<kLongMidMax>(), st>>>(SA);
-    OVX_CUDA(cudaFuncSetAttribute(voxel_accumulate_long<kLongHugeMax, 256, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    OVX_CUDA(cudaFuncSetAttribute(voxel_accumulate_long<kLongHugeMax, 256, true, B, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)long_smem<kLongHugeMax>()));
-    voxel_accumulate_long<kLongHugeMax, 256, true, B>
+    voxel_accumulate_long<kLongHugeMax, 256, true, B, P>
         <<<(unsigned)std::min<long long>(ctx->sms * 2, n), 256, long_smem<kLongHugeMax>(), st>>>(SA);
     ctx->launches += 3;
     stage(ctx, EV_SOLVE, st);
@@ -3661,6 +3777,19 @@ int ovx_fdg_get_tuning(const ovx_fdg_context *ctx, ovx_fdg_tuning *t)
     return OVX_FDG_OK;
 }
 
+int ovx_fdg_set_precision(ovx_fdg_context *ctx, int precision, float route_tolerance)
+{
+    if (!ctx)
+        return OVX_FDG_INVALID_ARGUMENT;
+    if (precision != OVX_FDG_PRECISION_EXACT && precision != OVX_FDG_PRECISION_COMPENSATED)
+        return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "unknown precision mode");
+    if (!(route_tolerance >= 0.0f) || !(route_tolerance < 3.0e38f))
+        return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "route tolerance must be finite and not negative");
+    ctx->precision = precision;
+    ctx->route_tol = route_tolerance;
+    return OVX_FDG_OK;
+}
+
 int ovx_fdg_set_output_order(ovx_fdg_context *ctx, int order)
 {
     if (!ctx)
@@ -3779,8 +3908,9 @@ int ovx_fdg_last_counts(const ovx_fdg_context *ctx, int64_t *out, int capacity)
 {
     if (!ctx || (!out && capacity > 0) || capacity < 0)
         return -OVX_FDG_INVALID_ARGUMENT;
-    const int64_t v[5] = {ctx->n_vox, ctx->n_active, ctx->n_rec, ctx->n_boundary, ctx->g.nbricks};
-    const int n = capacity < 5 ? capacity : 5;
+    const int64_t routed = (int64_t)((const uint32_t *)&ctx->host[kHostFinish])[C_ROUTED];
+    const int64_t v[6] = {ctx->n_vox, ctx->n_active, ctx->n_rec, ctx->n_boundary, ctx->g.nbricks, routed};
+    const int n = capacity < 6 ? capacity : 6;
     for (int i = 0; i < n; ++i)
         out[i] = v[i];
     return n;
@@ -4013,6 +4143,7 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_LONG, 0, 4, st));
     OVX_CUDA(cudaMemsetAsync(ctx->rcnt.p, 0, (size_t)(nb + 1) * 4, st));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONSTRAINED, 0, 4, st));
+    OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_ROUTED, 0, 4, st));
 
     stage(ctx, EV_FINISH, st);
     GenArgs A = make_gen(ctx);
@@ -4054,7 +4185,9 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.longv = (uint32_t *)ctx->longv.p;
     SA.longv_cap = (uint32_t)(n + 1);
     SA.clist_cap = (uint32_t)(n + 1);
-    const int cr = ctx->batch ? launch_consume<true>(ctx, SA, st, n) : launch_consume<false>(ctx, SA, st, n);
+    SA.route_tol = ctx->route_tol;
+    const int cr = ctx->batch ? (ctx->precision ? launch_consume<true, 1>(ctx, SA, st, n) : launch_consume<true, 0>(ctx, SA, st, n))
+                              : (ctx->precision ? launch_consume<false, 1>(ctx, SA, st, n) : launch_consume<false, 0>(ctx, SA, st, n));
     if (cr != OVX_FDG_OK)
         return cr;
     stage(ctx, EV_CONSTRAINED, st);

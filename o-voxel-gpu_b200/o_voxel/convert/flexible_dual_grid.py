@@ -161,6 +161,14 @@ def _order_code(order: Optional[str]) -> int:
     raise ValueError(f"order must be None, 'brick' or 'z_order', got {order!r}")
 
 
+def _precision_code(precision: Optional[str]) -> int:
+    if precision is None or precision == "exact":
+        return 0
+    if precision == "compensated":
+        return 1
+    raise ValueError(f"precision must be None, 'exact' or 'compensated', got {precision!r}")
+
+
 def _require_cuda(t: torch.Tensor, name: str):
     if not t.is_cuda:
         raise RuntimeError(f"{name}: this implementation runs on CUDA tensors only (got a {t.device} tensor)")
@@ -200,6 +208,8 @@ def mesh_to_flexible_dual_grid(
     regularization_weight: float = 0.1,
     timing: bool = False,
     order: Optional[str] = None,
+    precision: Optional[str] = None,
+    route_tolerance: float = 1e-3,
 ) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
     """
     Convert a triangle mesh into a sparse flexible dual grid.
@@ -219,6 +229,13 @@ def mesh_to_flexible_dual_grid(
             arbitrary): None or 'brick' -- 8x8x8 bricks then voxels, x-fastest;
             'z_order' -- ascending o_voxel.serialize.encode_seq code, the order the
             reference's examples obtain by sorting on it.
+        precision (str): arithmetic of the quadric sums and solves (not in the
+            reference): None or 'exact' -- bit-identical to the reference CPU path;
+            'compensated' -- FP32 sums with two-sum error terms merged in FP64,
+            FP64 regularisation, and an FP64 solve for the voxels whose FP32 solve
+            error estimate exceeds route_tolerance voxel edges.  Occupancy and flags
+            do not change; dual vertices move toward an FP64 evaluation.
+        route_tolerance (float): see precision.
 
     Returns:
         voxel_indices (torch.Tensor): [N, 3] int32 occupied voxel coordinates.
@@ -228,6 +245,7 @@ def mesh_to_flexible_dual_grid(
             starting at its min corner crosses the surface.
     """
     oc = _order_code(order)
+    pc = _precision_code(precision)
     vertices, faces, aabb, aabb_cpu, voxel_size_arg, grid_range_arg = _grid_setup(vertices, faces, voxel_size, grid_size, aabb)
     host = not vertices.is_cuda
     if host:
@@ -240,12 +258,13 @@ def mesh_to_flexible_dual_grid(
         origin = [float(x) for x in aabb_cpu[0].tolist()]
         out = _ext().mesh_to_flexible_dual_grid_cuda_ex(vertices, faces, origin, voxel_size_arg, grid_range_arg,
                                                         float(face_weight), float(boundary_weight),
-                                                        float(regularization_weight), oc)
+                                                        float(regularization_weight), oc, pc, float(route_tolerance))
     else:
         # aabb derived on the device: shift with torch, exactly like the reference wrapper
         vertices = vertices - aabb[0].reshape(1, 3)
         out = _ext().mesh_to_flexible_dual_grid_cuda(vertices, faces, voxel_size_arg, grid_range_arg, float(face_weight),
-                                                     float(boundary_weight), float(regularization_weight), oc)
+                                                     float(boundary_weight), float(regularization_weight), oc, pc,
+                                                     float(route_tolerance))
     return _download(out) if host else out
 
 
@@ -287,6 +306,8 @@ def mesh_to_flexible_dual_grid_batch(
     regularization_weight: float = 0.1,
     max_group_records: int = 128_000_000,
     order: Optional[str] = None,
+    precision: Optional[str] = None,
+    route_tolerance: float = 1e-3,
 ) -> List[Tuple[torch.Tensor, torch.Tensor, torch.Tensor]]:
     """
     Convert many meshes at once; returns one (voxel_indices, dual_vertices,
@@ -306,7 +327,7 @@ def mesh_to_flexible_dual_grid_batch(
             area plus 3 per triangle) stay within this budget, which bounds the
             device workspace (about 100 bytes a record); 0 puts every mesh in one
             group.
-        order: output row order, as in mesh_to_flexible_dual_grid.
+        order, precision, route_tolerance: as in mesh_to_flexible_dual_grid.
 
     The reference has no batched form.  Here every kernel of the conversion
     runs once over all meshes of a group (their triangles, bricks and vertices
@@ -350,7 +371,8 @@ def mesh_to_flexible_dual_grid_batch(
         _tuning.apply(_ext(), verts[0].device.index, max(max(g[3:]) for g in granges))
     out = _ext().mesh_to_flexible_dual_grid_cuda_batch(verts, fcs, origins, vsizes, granges, float(face_weight),
                                                        float(boundary_weight), float(regularization_weight),
-                                                       int(max_group_records), _order_code(order))
+                                                       int(max_group_records), _order_code(order),
+                                                       _precision_code(precision), float(route_tolerance))
     return [_download(o) if h else o for o, h in zip(out, host)]
 
 

@@ -34,6 +34,7 @@ PROTOTYPES = [
     ("ovx_fdg_last_counts", ctypes.c_int, [_P, ctypes.POINTER(_I64), ctypes.c_int]),
     ("ovx_fdg_set_output_order", ctypes.c_int, [_P, ctypes.c_int]),
     ("ovx_fdg_set_tuning", ctypes.c_int, [_P, _P]),
+    ("ovx_fdg_set_precision", ctypes.c_int, [_P, ctypes.c_int, _F]),
     ("ovx_fdg_get_tuning", ctypes.c_int, [_P, _P]),
     ("ovx_z_order_encode", ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
     ("ovx_z_order_decode", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
@@ -174,13 +175,20 @@ class Context:
         """0: brick order (default), 1: ascending z-order code."""
         self._check(self._lib.ovx_fdg_set_output_order(self.handle, int(order)), "ovx_fdg_set_output_order")
 
+    def set_precision(self, precision: int = 0, route_tolerance: float = 1e-3):
+        """0: exact (default), 1: compensated sums with FP64 routing of voxels
+        whose FP32 solve error estimate exceeds route_tolerance voxel edges."""
+        self._check(self._lib.ovx_fdg_set_precision(self.handle, int(precision), float(route_tolerance)),
+                    "ovx_fdg_set_precision")
+
     def last_counts(self) -> dict:
-        """Sizes of the last conversion (voxels, occupied bricks, records, boundary edges, grid bricks)."""
-        buf = (_I64 * 5)()
-        n = self._lib.ovx_fdg_last_counts(self.handle, buf, 5)
+        """Sizes of the last conversion (voxels, occupied bricks, records, boundary edges, grid bricks, and the
+        voxels the compensated mode solved in FP64)."""
+        buf = (_I64 * 6)()
+        n = self._lib.ovx_fdg_last_counts(self.handle, buf, 6)
         if n < 0:
             raise FdgError(-n, "ovx_fdg_last_counts")
-        names = ("voxels", "bricks_occupied", "records", "boundary_edges", "bricks_grid")
+        names = ("voxels", "bricks_occupied", "records", "boundary_edges", "bricks_grid", "routed_fp64")
         return {names[i]: int(buf[i]) for i in range(n)}
 
     def mesh_to_fdg(self, vertices, faces, origin, voxel_size, grid_range, fw, bw, rw, stream=None, check=True):

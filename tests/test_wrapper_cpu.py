@@ -55,12 +55,22 @@ def test_signature_matches_reference():
     import inspect
 
     sig = inspect.signature(o_voxel.convert.mesh_to_flexible_dual_grid)
-    # the reference's parameters, in order, then this implementation's optional `order`
+    # the reference's parameters, in order, then this implementation's optional ones
     assert list(sig.parameters) == ["vertices", "faces", "voxel_size", "grid_size", "aabb", "face_weight",
-                                    "boundary_weight", "regularization_weight", "timing", "order"]
+                                    "boundary_weight", "regularization_weight", "timing", "order", "precision",
+                                    "route_tolerance"]
     d = {k: p.default for k, p in sig.parameters.items()}
     assert d["face_weight"] == 1.0 and d["boundary_weight"] == 1.0 and d["regularization_weight"] == 0.1
-    assert d["order"] is None
+    assert d["order"] is None and d["precision"] is None
+
+
+def test_precision_argument_checks():
+    import torch
+
+    v = torch.zeros((3, 3))
+    f = torch.tensor([[0, 1, 2]])
+    with pytest.raises(ValueError, match="precision"):
+        o_voxel.convert.mesh_to_flexible_dual_grid(v, f, grid_size=8, aabb=[[0, 0, 0], [1, 1, 1]], precision="fp16")
 
 
 def test_order_and_serialize_argument_checks():
