@@ -351,7 +351,13 @@ def mesh_to_flexible_dual_grid_batch(
     vs_list = per_mesh_list(voxel_size, (3,)) if not isinstance(voxel_size, float) else False
     gs_list = per_mesh_list(grid_size, (3,)) if not isinstance(grid_size, int) else False
     ab_list = per_mesh_list(aabb, (2, 3))
-    verts, fcs, origins, vsizes, granges, host = [], [], [], [], [], []
+    fast = _batch_fast_args(meshes, grid_size, aabb, voxel_size, gs_list, ab_list)
+    if fast is not None:
+        verts, fcs, origins, vsizes, granges = fast
+        host = [False] * n
+        meshes = ()
+    else:
+        verts, fcs, origins, vsizes, granges, host = [], [], [], [], [], []
     for i, (v, f) in enumerate(meshes):
         v, f, ab, ab_cpu, vs_arg, gr_arg = _grid_setup(v, f, per_mesh(voxel_size, i, vs_list),
                                                       per_mesh(grid_size, i, gs_list), per_mesh(aabb, i, ab_list))
@@ -374,6 +380,46 @@ def mesh_to_flexible_dual_grid_batch(
                                                        int(max_group_records), _order_code(order),
                                                        _precision_code(precision), float(route_tolerance))
     return [_download(o) if h else o for o, h in zip(out, host)]
+
+
+def _batch_fast_args(meshes, grid_size, aabb, voxel_size, gs_list, ab_list):
+    """The batch's per-mesh arguments in one pass, for the common form: CUDA
+    float32 vertices [V,3] and int32/int64 faces [F,3] on one device, grid_size
+    and aabb given (one each, or one per mesh), no voxel_size.  The values are
+    those of the per-mesh derivation (float32 voxel size (aabb1 - aabb0) /
+    grid, grid_range [0, 0, 0, g...], origin aabb0).  None when the arguments
+    are of another form; the per-mesh derivation, with its checks, then runs."""
+    if voxel_size is not None or grid_size is None or aabb is None or not meshes:
+        return None
+    dev = None
+    for v, f in meshes:
+        if not (isinstance(v, torch.Tensor) and isinstance(f, torch.Tensor) and v.is_cuda and f.is_cuda
+                and v.dtype == torch.float32 and f.dtype in (torch.int32, torch.int64) and v.dim() == 2
+                and v.size(1) == 3 and f.dim() == 2 and f.size(1) == 3 and v.is_contiguous() and f.is_contiguous()):
+            return None
+        if dev is None:
+            dev = v.device
+        if v.device != dev or f.device != dev:
+            return None
+    n = len(meshes)
+    try:
+        if isinstance(grid_size, torch.Tensor) or isinstance(aabb, torch.Tensor):
+            return None
+        g = np.asarray(grid_size if gs_list else [grid_size] * n, dtype=np.int64)
+        if g.ndim == 1:
+            g = np.repeat(g[:, None], 3, axis=1)
+        ab = np.asarray(aabb if ab_list else [aabb] * n, dtype=np.float32)
+    except (TypeError, ValueError):
+        return None
+    if g.shape != (n, 3) or ab.shape != (n, 2, 3) or (g <= 0).any():
+        return None
+    vs = ((ab[:, 1] - ab[:, 0]) / g.astype(np.int32).astype(np.float32)).astype(np.float32)
+    verts = [v for v, _ in meshes]
+    fcs = [f for _, f in meshes]
+    origins = ab[:, 0].astype(np.float64).tolist()
+    vsizes = vs.astype(np.float64).tolist()
+    granges = [[0, 0, 0] + [int(x) for x in row] for row in g.tolist()]
+    return verts, fcs, origins, vsizes, granges
 
 
 @torch.no_grad()
