@@ -19,13 +19,13 @@
 //             face     {t, 1<<30 | local voxel, 0}
 //             boundary {e, 2<<30 | local voxel, 0}, e = index in the
 //                      boundary edge list, which is sorted by (v_min, v_max)
-//   qtab    plane quadric per triangle (10 floats)
+//   qtab    plane quadric per triangle (10 floats in a 12-float row, read as 16-byte loads)
 //   contrib per-voxel contribution lists, 16 B entries; brick b owns entries
 //           [4*roff[b], 4*roff[b+1]) (a record yields at most 4 contributions)
 //   vlist   per output row: first entry (40 bits) | entry count << 40 | sorted << 63
 //   estage, fstage  event and face records staged by the count pass (16 B,
 //           {brick, t, code, z} and {brick, t, code, rank in the brick})
-//   btab    line quadric per boundary edge (10 floats)
+//   btab    line quadric per boundary edge (10 floats in a 12-float row)
 //
 // begin (ends with the one host synchronisation of a conversion):
 //   tri_events<COUNT>   one (triangle, axis) per lane: scanline events (FP64,
@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
                 tri_quadric(v, q);
 #pragma unroll
                 for (int i = 0; i < 10; ++i)
-                    A.qtab[t * 10 + i] = q[i];
+                    A.qtab[t * 12 + i] = q[i];
             }
             AxisScan s;
             axis_setup(v, ax2, g, s);
@@ -1376,7 +1376,7 @@ __global__ void __launch_bounds__(kThreads) boundary_records(GenArgs A)
         vertex_load(Ms, ia - Ms.vert0, v0);
         vertex_load(Ms, ib - Ms.vert0, v1);
         Dda d;
-        if (!boundary_setup(v0, v1, g, d, M == FILL ? A.btab + (size_t)i * 10 : nullptr))
+        if (!boundary_setup(v0, v1, g, d, M == FILL ? A.btab + (size_t)i * 12 : nullptr))
             continue;
         if (d.guard > A.tune.long_walk)
         {
@@ -1827,6 +1827,16 @@ struct Contrib
     unsigned stage;
 };
 
+// A quadric of a 12-float (48-byte) table row: three 16-byte loads.
+__device__ __forceinline__ void load_q12(const float *p, float q[10])
+{
+    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    const float2 c = reinterpret_cast<const float2 *>(p)[4];
+    q[0] = a.x; q[1] = a.y; q[2] = a.z; q[3] = a.w;
+    q[4] = b.x; q[5] = b.y; q[6] = b.z; q[7] = b.w;
+    q[8] = c.x; q[9] = c.y;
+}
+
 __device__ __forceinline__ void contrib_load(const SolveArgs &A, const Grid &g, const int vc[3], unsigned long long key, uint32_t pay,
                                              Contrib &c)
 {
@@ -1850,23 +1860,20 @@ __device__ __forceinline__ void contrib_load(const SolveArgs &A, const Grid &g, 
         c.p[0] = ax2 == 0 ? pw : (ax2 == 1 ? pv : pu);
         c.p[1] = ax2 == 0 ? pu : (ax2 == 1 ? pw : pv);
         c.p[2] = ax2 == 0 ? pv : (ax2 == 1 ? pu : pw);
-#pragma unroll
-        for (int i = 0; i < 10; ++i)
-            c.q[i] = A.qtab[t * 10 + i];
+        load_q12(A.qtab + t * 12, c.q);
         if (dx == 0 && dy == 0)
             c.flag = 1u << ax2;
     }
     else if (c.stage == 1)
     {
         const long long t = (long long)(key & ((1ull << 62) - 1ull));
-#pragma unroll
-        for (int i = 0; i < 10; ++i)
-            c.q[i] = A.qtab[t * 10 + i];
+        load_q12(A.qtab + t * 12, c.q);
     }
     else
     {
         // line quadric of boundary edge e (computed once by the boundary pass), weighted
-        const float *bq = A.btab + (size_t)(key & 0xffffffffull) * 10;
+        float bq[10];
+        load_q12(A.btab + (size_t)(key & 0xffffffffull) * 12, bq);
 #pragma unroll
         for (int i = 0; i < 10; ++i)
             c.q[i] = A.bw * bq[i];
@@ -3470,7 +3477,7 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(ensure(st, ctx, ctx->rcnt, (size_t)(nb + 1) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
-        OVX_CUDA(ensure(st, ctx, ctx->qtab, (size_t)(nf + 1) * 40));
+        OVX_CUDA(ensure(st, ctx, ctx->qtab, (size_t)(nf + 1) * 48));
     if (full)
     {
         // staging room for the event records: the most seen so far, else a guess
@@ -4135,7 +4142,7 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     OVX_CUDA(scope.status);
     const long long nb = ctx->g.nbricks;
     OVX_CUDA(ensure(st, ctx, ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
-    OVX_CUDA(ensure(st, ctx, ctx->btab, (size_t)(ctx->n_boundary + 1) * 40));
+    OVX_CUDA(ensure(st, ctx, ctx->btab, (size_t)(ctx->n_boundary + 1) * 48));
     OVX_CUDA(ensure(st, ctx, ctx->clist, (size_t)(n + 1) * 16 * 4));
     OVX_CUDA(ensure(st, ctx, ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
     OVX_CUDA(ensure(st, ctx, ctx->vlist, (size_t)n * 8));

@@ -2,7 +2,8 @@
 
 For each grid-size bucket (64, 128, 256, 512, 1024) it builds seeded meshes
 like the mixed-batch workload (primitive soups, face counts log-uniform in
-1k-500k, per-mesh aabb) at that grid, and times their conversions through the
+1k-500k, per-mesh aabb) at that grid, plus the 282k-face primitives mesh on
+the unit box (counted twice), and times their conversions through the
 C ABI (CUDA events, device-resident inputs) while it searches the five shape
 values by coordinate descent from the library defaults: each value in turn is
 set to each of its candidates, and the fastest setting is kept when it beats
@@ -58,6 +59,10 @@ class Bucket:
 
         self.grid = grid
         self.ws = W.batch(seed=100 + grid, n_meshes=n_meshes, f_lo=1_000, f_hi=500_000, grids=(grid,))
+        # and the 282k-face primitives mesh on the unit box at this grid, twice (it is the single-mesh headline case)
+        p = W.primitives(1)
+        p.grid_size = grid
+        self.ws += [p, p]
         self.args = []
         for w in self.ws:
             origin, vs, gr = grid_args(w)
