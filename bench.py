@@ -558,7 +558,7 @@ def run_ours(args, rank, world):
         "cold_ms": cold_ms,
         "memory": {"workspace_bytes": workspace, "torch_max_allocated_bytes": int(torch.cuda.max_memory_allocated(dev)),
                    "note": "workspace: the conversion context's buffers (grown to the largest conversion); torch: outputs, inputs, "
-                           "the 256 MB L2 flush buffer, the reference's CUDA path and the batched leg"},
+                           "the 256 MB L2 flush buffer and the batched leg"},
         "workloads": {HEADLINE: head, **workloads},
         "reference_gpu": reference_gpu,
         "cpu_baseline": cpu,

@@ -1,7 +1,8 @@
 """Work shapes (ovx_fdg_tuning) change speed only: conversions under extreme
 shapes -- every pair cut into units, every face box on the large-triangle
 pass, every item tested by the whole warp, every boundary edge walked by a
-warp, and the opposite extremes -- equal the defaults' results bit for bit."""
+warp, and the opposite extremes -- and the tuned table's shapes equal the
+defaults' results bit for bit."""
 import numpy as np
 import pytest
 
@@ -37,7 +38,10 @@ def test_shapes_do_not_change_results(cuda, name):
     ctx = abi.Context(cuda.index or 0)
     try:
         want = [t.clone() for t in ctx.mesh_to_fdg(*a)]
-        for shapes in EXTREMES:
+        from o_voxel.convert import _tuning
+
+        table = [dict(zip(_tuning.FIELDS, values)) for _, values in _tuning.table()]
+        for shapes in EXTREMES + table:
             ctx.set_tuning(shapes)
             assert ctx.get_tuning() == shapes
             got = ctx.mesh_to_fdg(*a)
