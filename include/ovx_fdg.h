@@ -52,7 +52,7 @@ enum ovx_fdg_status
     OVX_FDG_BAD_FACE_INDEX = 2,   /* a face index outside [0, num_vertices) */
     OVX_FDG_CUDA_ERROR = 3,       /* a CUDA runtime call or launch failed */
     OVX_FDG_OUT_OF_MEMORY = 4,    /* workspace allocation failed */
-    OVX_FDG_CAPACITY = 5,         /* result larger than the 32-bit row / 64-bit entry indexing supports */
+    OVX_FDG_CAPACITY = 5,         /* input or result beyond the indexing limits (2^28-1 faces, 2^31-2 vertices, 2^31-1 voxels) */
     OVX_FDG_INTERNAL = 6          /* a device-side bound (walk length) was hit; results not produced */
 };
 
@@ -241,7 +241,7 @@ int ovx_fdg_sync_status(ovx_fdg_context *ctx, void *stream);
  * sum.  finish_batch: output buffers with room for total_voxels rows; mesh
  * i's rows start at num_voxels[0] + ... + num_voxels[i-1].  Same semantics,
  * order options and errors as the single-mesh calls (an error names the
- * mesh).  Limits over the whole batch: 2^30 faces, 2^31-1 vertices, 2^31
+ * mesh).  Limits over the whole batch: 2^28-1 faces, 2^31-2 vertices, 2^31
  * bricks of the grids.
  */
 typedef struct ovx_fdg_mesh

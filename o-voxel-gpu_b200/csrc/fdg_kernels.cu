@@ -20,11 +20,17 @@
 //             boundary {e, 2<<30 | local voxel, 0}, e = index in the
 //                      boundary edge list, which is sorted by (v_min, v_max)
 //   qtab    plane quadric per triangle (10 floats in a 12-float row, read as 16-byte loads)
-//   contrib per-voxel contribution lists, 16 B entries; brick b owns entries
-//           [4*roff[b], 4*roff[b+1]) (a record yields at most 4 contributions)
+//   contrib per-voxel contribution lists, 8 B entries {order key, payload};
+//           each brick reserves its lists' exact room with one atomic (the
+//           total is known after begin: 4 per scanline event, 1 per face or
+//           boundary record)
 //   vlist   per output row: first entry (40 bits) | entry count << 40 | sorted << 63
 //   estage, fstage  event and face records staged by the count pass (16 B,
-//           {brick, t, code, z} and {brick, t, code, rank in the brick})
+//           {brick, t, code, z} and {brick, t, code, rank in the brick}); both
+//           live in one arena that the contribution lists reuse once the
+//           staged records are in their buckets
+//   clist   voxels left to the constrained search, in the record buffer (dead
+//           once the lists are built); when it is full the search runs inline
 //   btab    line quadric per boundary edge (10 floats in a 12-float row)
 //
 // begin (ends with the one host synchronisation of a conversion):
@@ -58,11 +64,13 @@
 //   constrained_solve   box-constrained search for the few voxels whose
 //                       unconstrained solution leaves the voxel
 //
-// Contribution order keys (64 bit, unique per voxel; ascending = reference CPU
-// order, flexible_dual_grid.cpp:173-283, :298-414, :741-757):
-//   intersection  (0<<62) | ((t*3 + axis)*4 + (1-dy)*2 + (1-dx))
-//   face          (1<<62) | t
-//   boundary      (2<<62) | e   (edge list index; the list is in (v_min, v_max) order)
+// Contribution order keys (32 bit, unique per voxel; ascending = reference CPU
+// order, flexible_dual_grid.cpp:173-283, :298-414, :741-757), F = triangles of
+// the conversion (all meshes of a batch; F < 2^28, so every key < 16F < 2^32):
+//   intersection  (t*3 + axis)*4 + (1-dy)*2 + (1-dx)     in [0, 12F)
+//   face          12F + t                                in [12F, 13F)
+//   boundary      13F + e   (edge list index; the list is in (v_min, v_max)
+//                           order, and there are at most 3F boundary edges)
 #include "ovx_fdg.h"
 #include "fdg_device.cuh"
 
@@ -73,6 +81,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -88,7 +97,7 @@ constexpr int kInlineFaceBricks = 8; // triangles whose face box spans more bric
 constexpr int kUnitCells = 64;        // cells per unit of work of a large (triangle, axis) pair
 constexpr int kThreads = 256;
 constexpr int kConsumeThreads = 128;
-constexpr int kListStage = 768; // contributions of a brick that brick_lists stages (and sorts) in shared memory
+constexpr int kListStage = 1024; // contributions of a brick that brick_lists stages (and sorts) in shared memory
 // vlist word: first entry (bits 0-39) | count (bits 40-62) | sorted flag (bit 63)
 constexpr uint32_t kListCountMax = (1u << 23) - 1u;
 constexpr unsigned long long kListSorted = 1ull << 63;
@@ -108,13 +117,16 @@ enum
     C_FSTAGED = 5,
     C_LONG = 6,
     C_HUGE = 7,
-    C_ESTAGED = 8,
-    C_LUNITS = 9,  // units of work of the large (triangle, axis) pairs
-    C_FUNITS = 10, // units of work of the large triangles' face boxes
-    C_BLONG = 11,  // boundary edges walked by a whole warp
-    C_ROUTED = 12, // compensated precision: voxels solved in FP64
-    C_WORDS = 13
+    C_LUNITS = 8,  // units of work of the large (triangle, axis) pairs
+    C_FUNITS = 9,  // units of work of the large triangles' face boxes
+    C_BLONG = 10,  // boundary edges walked by a whole warp
+    C_ROUTED = 11, // compensated precision: voxels solved in FP64
+    C_CONTRIB = 12, // 64-bit word (12, 13): contribution entries reserved by brick_lists
+    C_ESTAGED = 14, // 64-bit pair (14, 15), added to as one word: scanline event records staged,
+    C_EVENTS = 15,  // and scanline events (each yields four contributions)
+    C_WORDS = 16
 };
+static_assert(C_CONTRIB % 2 == 0 && C_ESTAGED % 2 == 0 && C_EVENTS == C_ESTAGED + 1, "64-bit counters are 8-byte aligned words");
 enum
 {
     ST_BAD_INDEX = 1,
@@ -131,8 +143,7 @@ enum Mode
 
 constexpr uint32_t kRecFace = 1u << 30;
 constexpr uint32_t kRecBoundary = 2u << 30;
-constexpr unsigned long long kKeyFace = 1ull << 62;
-constexpr unsigned long long kKeyBoundary = 2ull << 62;
+constexpr long long kMaxTriangles = (1ll << 28) - 1; // 32-bit order keys: 16F < 2^32
 
 struct Rec
 {
@@ -611,12 +622,15 @@ __device__ __forceinline__ void event_rows(const GenArgs &A, EventWarp &E, const
             }
             if (M == COUNT && A.estage)
             {
-                // stage this round's records: one reservation for the warp
+                // stage this round's records: one reservation for the warp; the
+                // round's events are counted (four contributions each)
                 uint32_t tot;
                 const uint32_t off = warp_exclusive_scan(es.n, tot);
+                const uint32_t nev = (uint32_t)__popc(__ballot_sync(0xffffffffu, es.n > 0u));
                 uint32_t base = 0;
                 if (lane == 0 && tot)
-                    base = atomicAdd(&A.counters[C_ESTAGED], tot);
+                    base = (uint32_t)atomicAdd((unsigned long long *)&A.counters[C_ESTAGED],
+                                               ((unsigned long long)nev << 32) | (unsigned long long)tot);
                 base = __shfl_sync(0xffffffffu, base, 0);
 #pragma unroll
                 for (int k = 0; k < 4; ++k)
@@ -1705,13 +1719,15 @@ struct SolveArgs
     float *dual;
     uint8_t *flags;
     uint32_t *counters;
-    uint4 *contrib;             // per-voxel contribution lists {key lo, key hi, payload, 0}
+    uint2 *contrib;             // per-voxel contribution lists {order key, payload}
+    unsigned long long contrib_cap; // entries contrib holds
+    uint32_t key_face, key_boundary; // first face and boundary order keys: 12F and 13F
     bool zorder;                // output rows in z-order (bbase then holds z-order row bases)
     uint32_t *longv;            // rows whose lists are too long for voxel_accumulate: up to kLongMidMax
                                 // entries from the front (counter C_LONG), longer ones from the back (C_HUGE)
     uint32_t longv_cap;
     unsigned long long *vlist;  // per output row: first contribution (low 40 bits) | count << 40 | sorted << 63
-    float *clist; // deferred constrained searches, 16 words each
+    float *clist; // deferred constrained searches, 16 words each (full: searched inline)
     uint32_t clist_cap;
     float route_tol; // compensated precision: FP32 solve error (voxel edges) above which a voxel is solved in FP64
 };
@@ -1770,16 +1786,17 @@ __device__ __forceinline__ void load_brick_ranks(SS &S, const uint32_t *__restri
     __syncthreads();
 }
 
-// Expand one record of the brick into (dense voxel index, order key, payload) contributions.
+// Expand one record of the brick into (dense voxel index, order key, payload)
+// contributions; key_face and key_boundary are 12F and 13F.
 template <typename SS, typename Sink>
-__device__ __forceinline__ void expand(const SS &S, const Rec &r, Sink &sink)
+__device__ __forceinline__ void expand(const SS &S, const Rec &r, uint32_t key_face, uint32_t key_boundary, Sink &sink)
 {
     const uint32_t kind = r.b >> 30;
     if (kind == 0)
     {
         const int ax2 = (int)(r.b & 3u);
         const int u = (int)((r.b >> 2) & 15u) - 1, v = (int)((r.b >> 6) & 15u) - 1, w = (int)((r.b >> 10) & 15u);
-        const unsigned long long kb = ((unsigned long long)r.a * 3ull + (unsigned long long)ax2) * 4ull;
+        const uint32_t kb = (r.a * 3u + (uint32_t)ax2) * 4u;
 #pragma unroll
         for (int k = 0; k < 4; ++k)
         {
@@ -1789,13 +1806,13 @@ __device__ __forceinline__ void expand(const SS &S, const Rec &r, Sink &sink)
                 continue;
             int lx, ly, lz;
             place(ax2, lu, lv, w, lx, ly, lz);
-            sink(dense_index(S, lx + 8 * ly + 64 * lz), kb + (unsigned long long)((1 - dy) * 2 + (1 - dx)), r.c);
+            sink(dense_index(S, lx + 8 * ly + 64 * lz), kb + (uint32_t)((1 - dy) * 2 + (1 - dx)), r.c);
         }
     }
     else if (kind == 1)
-        sink(dense_index(S, (int)(r.b & 511u)), kKeyFace | (unsigned long long)r.a, 0u);
+        sink(dense_index(S, (int)(r.b & 511u)), key_face + r.a, 0u);
     else
-        sink(dense_index(S, (int)(r.b & 511u)), kKeyBoundary | (unsigned long long)r.a, 0u);
+        sink(dense_index(S, (int)(r.b & 511u)), key_boundary + r.a, 0u);
 }
 
 struct Acc
@@ -1837,18 +1854,18 @@ __device__ __forceinline__ void load_q12(const float *p, float q[10])
     q[8] = c.x; q[9] = c.y;
 }
 
-__device__ __forceinline__ void contrib_load(const SolveArgs &A, const Grid &g, const int vc[3], unsigned long long key, uint32_t pay,
+__device__ __forceinline__ void contrib_load(const SolveArgs &A, const Grid &g, const int vc[3], uint32_t key, uint32_t pay,
                                              Contrib &c)
 {
-    c.stage = (unsigned)(key >> 62);
+    c.stage = key < A.key_face ? 0u : (key < A.key_boundary ? 1u : 2u);
     c.flag = 0u;
     c.p[0] = c.p[1] = c.p[2] = 0.0f;
     if (c.stage == 0)
     {
-        const unsigned long long ta = key >> 2;
-        const long long t = (long long)(ta / 3ull);
-        const int ax2 = (int)(ta - (unsigned long long)t * 3ull);
-        const int dx = 1 - (int)(key & 1ull), dy = 1 - (int)((key >> 1) & 1ull);
+        const uint32_t ta = key >> 2;
+        const uint32_t t = ta / 3u;
+        const int ax2 = (int)(ta - t * 3u);
+        const int dx = 1 - (int)(key & 1u), dy = 1 - (int)((key >> 1) & 1u);
         const int ax0 = (ax2 + 1) % 3, ax1 = (ax2 + 2) % 3;
         const int c0 = ax0 == 0 ? vc[0] : (ax0 == 1 ? vc[1] : vc[2]);
         const int c1 = ax1 == 0 ? vc[0] : (ax1 == 1 ? vc[1] : vc[2]);
@@ -1860,20 +1877,17 @@ __device__ __forceinline__ void contrib_load(const SolveArgs &A, const Grid &g, 
         c.p[0] = ax2 == 0 ? pw : (ax2 == 1 ? pv : pu);
         c.p[1] = ax2 == 0 ? pu : (ax2 == 1 ? pw : pv);
         c.p[2] = ax2 == 0 ? pv : (ax2 == 1 ? pu : pw);
-        load_q12(A.qtab + t * 12, c.q);
+        load_q12(A.qtab + (size_t)t * 12, c.q);
         if (dx == 0 && dy == 0)
             c.flag = 1u << ax2;
     }
     else if (c.stage == 1)
-    {
-        const long long t = (long long)(key & ((1ull << 62) - 1ull));
-        load_q12(A.qtab + t * 12, c.q);
-    }
+        load_q12(A.qtab + (size_t)(key - A.key_face) * 12, c.q);
     else
     {
         // line quadric of boundary edge e (computed once by the boundary pass), weighted
         float bq[10];
-        load_q12(A.btab + (size_t)(key & 0xffffffffull) * 12, bq);
+        load_q12(A.btab + (size_t)(key - A.key_boundary) * 12, bq);
 #pragma unroll
         for (int i = 0; i < 10; ++i)
             c.q[i] = A.bw * bq[i];
@@ -1923,10 +1937,10 @@ __device__ __forceinline__ void contrib_apply(const Contrib &c, Acc &a)
 // contributions); then one thread per voxel orders its list by key, sums it in
 // that order (the reference CPU order) and solves.
 // ---------------------------------------------------------------------------
-// Order key of a contribution list entry {key lo, key hi, payload, 0}.
-__device__ __forceinline__ unsigned long long entry_key(const uint4 &e)
+// Order key of a contribution list entry {key, payload}.
+__device__ __forceinline__ uint32_t entry_key(const uint2 &e)
 {
-    return (unsigned long long)e.x | ((unsigned long long)e.y << 32);
+    return e.x;
 }
 
 struct ListShared
@@ -1940,16 +1954,17 @@ struct ListShared
     uint32_t scan_tmp[kConsumeThreads / 32 + 1]; // per-warp offsets, then the brick's total
     int nvox;
     uint32_t status;
-    // the brick's lists, when they fit (keys and payloads apart: 12 bytes an
-    // entry): filled, short lists sorted, copied out
-    unsigned long long skey[kListStage];
+    unsigned long long first; // the brick's first contribution entry (reserved by one atomic)
+    // the brick's lists, when they fit (keys and payloads apart): filled,
+    // short lists sorted, copied out
+    uint32_t skey[kListStage];
     uint32_t spay[kListStage];
 };
 
 struct ListCount
 {
     ListShared &S;
-    __device__ __forceinline__ void operator()(int i, unsigned long long, uint32_t) const
+    __device__ __forceinline__ void operator()(int i, uint32_t, uint32_t) const
     {
         atomicAdd(&S.cnt[i], 1u);
     }
@@ -1958,19 +1973,19 @@ struct ListCount
 struct ListFill
 {
     ListShared &S;
-    uint4 *out;              // the brick's first entry
-    unsigned long long room; // entries the brick owns
-    __device__ __forceinline__ void operator()(int i, unsigned long long key, uint32_t pay) const
+    uint2 *out;    // the brick's first entry
+    uint32_t room; // entries the brick reserved
+    __device__ __forceinline__ void operator()(int i, uint32_t key, uint32_t pay) const
     {
         // off[i] counts up from the start of voxel i's list: records are taken
         // in bucket order, which is close to key order, so lists come out nearly sorted
         const uint32_t k = atomicAdd(&S.off[i], 1u);
-        if ((unsigned long long)k >= room)
+        if (k >= room)
         {
             atomicOr(&S.status, (uint32_t)ST_REPLAY);
             return;
         }
-        out[k] = make_uint4((uint32_t)key, (uint32_t)(key >> 32), pay, 0u);
+        out[k] = make_uint2(key, pay);
     }
 };
 
@@ -1978,7 +1993,7 @@ struct ListFill
 struct ListStageFill
 {
     ListShared &S;
-    __device__ __forceinline__ void operator()(int i, unsigned long long key, uint32_t pay) const
+    __device__ __forceinline__ void operator()(int i, uint32_t key, uint32_t pay) const
     {
         const uint32_t k = atomicAdd(&S.off[i], 1u);
         if (k >= (uint32_t)kListStage)
@@ -2025,7 +2040,7 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     {
         ListCount cs{S};
         for (unsigned long long r = tid; r < nrec; r += blockDim.x)
-            expand(S, rec[r], cs);
+            expand(S, rec[r], A.key_face, A.key_boundary, cs);
     }
     __syncthreads();
     // exclusive scan of the counts: off[i] = start of voxel i's list
@@ -2061,11 +2076,25 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
                 r += x;
             }
             S.scan_tmp[kConsumeThreads / 32] = r;
+            // the brick's room in contrib: exactly its entries
+            unsigned long long f = atomicAdd((unsigned long long *)&A.counters[C_CONTRIB], (unsigned long long)r);
+            if (f + r > A.contrib_cap)
+            {
+                atomicOr(&S.status, (uint32_t)ST_LIST_OVERFLOW);
+                f = ~0ull;
+            }
+            S.first = f;
         }
         __syncthreads();
+        if (S.first == ~0ull)
+        {
+            if (tid == 0)
+                atomicOr(&A.counters[C_STATUS], S.status);
+            return;
+        }
         const bool staged = S.scan_tmp[kConsumeThreads / 32] <= (uint32_t)kListStage;
         uint32_t run = S.scan_tmp[warp] + incl - sum;
-        const unsigned long long first = 4ull * A.roff[b];
+        const unsigned long long first = S.first;
 #pragma unroll
         for (int k = 0; k < per; ++k)
         {
@@ -2083,7 +2112,7 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
     }
     __syncthreads();
     const uint32_t total = S.scan_tmp[kConsumeThreads / 32];
-    uint4 *out = A.contrib + 4ull * A.roff[b];
+    uint2 *out = A.contrib + S.first;
     if (total <= (uint32_t)kListStage)
     {
         // the lists fit in shared memory: fill them there, sort the short ones
@@ -2091,7 +2120,7 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
         {
             ListStageFill fs{S};
             for (unsigned long long r = tid; r < nrec; r += blockDim.x)
-                expand(S, rec[r], fs);
+                expand(S, rec[r], A.key_face, A.key_boundary, fs);
         }
         __syncthreads();
         for (int j = tid; j < nvox; j += blockDim.x)
@@ -2099,11 +2128,11 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
             const uint32_t c = S.cnt[j];
             if (c < 2u || c >= (uint32_t)kWarpSortMin)
                 continue;
-            unsigned long long *K = S.skey + (S.off[j] - c);
+            uint32_t *K = S.skey + (S.off[j] - c);
             uint32_t *P = S.spay + (S.off[j] - c);
             for (uint32_t x = 1; x < c; ++x)
             {
-                const unsigned long long k = K[x];
+                const uint32_t k = K[x];
                 const uint32_t pv = P[x];
                 uint32_t y = x;
                 while (y > 0 && K[y - 1] > k)
@@ -2118,16 +2147,13 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
         }
         __syncthreads();
         for (uint32_t i = tid; i < total; i += blockDim.x)
-        {
-            const unsigned long long k = S.skey[i];
-            out[i] = make_uint4((uint32_t)k, (uint32_t)(k >> 32), S.spay[i], 0u);
-        }
+            out[i] = make_uint2(S.skey[i], S.spay[i]);
     }
     else
     {
-        ListFill fs{S, out, 4ull * nrec};
+        ListFill fs{S, out, total};
         for (unsigned long long r = tid; r < nrec; r += blockDim.x)
-            expand(S, rec[r], fs);
+            expand(S, rec[r], A.key_face, A.key_boundary, fs);
     }
     __syncthreads();
     if (tid == 0 && S.status)
@@ -2137,13 +2163,6 @@ __global__ void __launch_bounds__(kConsumeThreads) brick_lists(SolveArgs A)
 // One thread per voxel row: order the voxel's contributions by key, sum them in
 // that order, regularise and solve (flexible_dual_grid.cpp:763-797); voxels
 // whose unconstrained solution leaves the box go to the constrained-search list.
-
-__device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int src)
-{
-    const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src);
-    const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src);
-    return (unsigned long long)lo | ((unsigned long long)hi << 32);
-}
 
 // Regularise and solve one voxel (flexible_dual_grid.cpp:763-797); a voxel whose
 // unconstrained solution leaves its box goes to the constrained-search list.
@@ -2189,6 +2208,30 @@ __device__ __forceinline__ void contrib_apply(const Contrib &c, AccC &a)
 }
 
 __device__ __forceinline__ void voxel_finish(const SolveArgs &A, const Grid &g, long long row, const int vc[3], const Acc &a);
+
+// The constrained search for a voxel the full deferred list could not take:
+// a call of its own, so that its registers stay out of the accumulate loop.
+// Everything is passed by value (taking the address of the kernel's
+// parameters would move them to local memory); the search uses only the
+// grid's voxel size.
+struct Q10
+{
+    float v[10];
+};
+
+__device__ __noinline__ void constrained_here(float *dual, long long row, int x, int y, int z, float vx, float vy, float vz, Q10 q)
+{
+    Grid g{};
+    g.vs[0] = vx;
+    g.vs[1] = vy;
+    g.vs[2] = vz;
+    const int vc[3] = {x, y, z};
+    float w[3];
+    solve_constrained(vc, g, q.v, w);
+    dual[row * 3 + 0] = w[0];
+    dual[row * 3 + 1] = w[1];
+    dual[row * 3 + 2] = w[2];
+}
 
 // Compensated precision: sums merged and regularised in double; the FP32
 // solve of the rounded quadric is kept unless its error estimate -- the
@@ -2243,7 +2286,12 @@ __device__ __forceinline__ void voxel_finish(const SolveArgs &A, const Grid &g, 
     const uint32_t slot = atomicAdd(&A.counters[C_CONSTRAINED], 1u);
     if (slot >= A.clist_cap)
     {
-        atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+        // the deferred list is full: search here (same routine, same result)
+        Q10 qv;
+#pragma unroll
+        for (int i = 0; i < 10; ++i)
+            qv.v[i] = qf[i];
+        constrained_here(A.dual, row, vc[0], vc[1], vc[2], g.vs[0], g.vs[1], g.vs[2], qv);
         return;
     }
     float *c = A.clist + (size_t)slot * 16;
@@ -2275,7 +2323,12 @@ __device__ __forceinline__ void voxel_finish(const SolveArgs &A, const Grid &g, 
     const uint32_t slot = atomicAdd(&A.counters[C_CONSTRAINED], 1u);
     if (slot >= A.clist_cap)
     {
-        atomicOr(&A.counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+        // the deferred list is full: search here (same routine, same result)
+        Q10 qv;
+#pragma unroll
+        for (int i = 0; i < 10; ++i)
+            qv.v[i] = q[i];
+        constrained_here(A.dual, row, vc[0], vc[1], vc[2], g.vs[0], g.vs[1], g.vs[2], qv);
         return;
     }
     float *c = A.clist + (size_t)slot * 16;
@@ -2316,10 +2369,10 @@ __global__ void __launch_bounds__(128, P == 0 ? 12 : 4) voxel_accumulate(SolveAr
         const int v = __ffs(m) - 1;
         const uint32_t nv = __shfl_sync(0xffffffffu, n, v);
         const unsigned long long fv = __shfl_sync(0xffffffffu, first, v);
-        uint4 *L = A.contrib + fv;
-        const uint4 pad = make_uint4(0xffffffffu, 0xffffffffu, 0u, 0u);
-        uint4 e[kWarpSortPer];
-        unsigned long long k[kWarpSortPer];
+        uint2 *L = A.contrib + fv;
+        const uint2 pad = make_uint2(0xffffffffu, 0u);
+        uint2 e[kWarpSortPer];
+        uint32_t k[kWarpSortPer];
         uint32_t r[kWarpSortPer];
 #pragma unroll
         for (int q = 0; q < kWarpSortPer; ++q)
@@ -2339,7 +2392,7 @@ __global__ void __launch_bounds__(128, P == 0 ? 12 : 4) voxel_accumulate(SolveAr
             const uint32_t jn = nv - 32u * sq < 32u ? nv - 32u * sq : 32u;
             for (uint32_t j = 0; j < jn; ++j)
             {
-                const unsigned long long kj = shfl_u64(k[sq], (int)j);
+                const uint32_t kj = __shfl_sync(0xffffffffu, k[sq], (int)j);
                 const uint32_t jj = 32u * sq + j;
 #pragma unroll
                 for (int q = 0; q < kWarpSortPer; ++q)
@@ -2370,19 +2423,19 @@ __global__ void __launch_bounds__(128, P == 0 ? 12 : 4) voxel_accumulate(SolveAr
     }
     const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
     const Grid &g = mesh_of<B>(A, seg_of_row<B>(A, row)).g;
-    uint4 *lst = A.contrib + first;
+    uint2 *lst = A.contrib + first;
     if (n < (uint32_t)kWarpSortMin && !sorted)
     {
         // short lists that brick_lists could not sort in shared memory:
         // insertion sort in place
         for (uint32_t x = 1; x < n; ++x)
         {
-            const uint4 e = lst[x];
-            const unsigned long long k = entry_key(e);
+            const uint2 e = lst[x];
+            const uint32_t k = entry_key(e);
             uint32_t j = x;
             while (j > 0)
             {
-                const uint4 pe = lst[j - 1];
+                const uint2 pe = lst[j - 1];
                 if (entry_key(pe) <= k)
                     break;
                 lst[j] = pe;
@@ -2396,9 +2449,9 @@ __global__ void __launch_bounds__(128, P == 0 ? 12 : 4) voxel_accumulate(SolveAr
     acc_init(a);
     for (uint32_t x = 0; x < n; ++x)
     {
-        const uint4 e = lst[x];
+        const uint2 e = lst[x];
         Contrib c;
-        contrib_load(A, g, vc, entry_key(e), e.z, c);
+        contrib_load(A, g, vc, entry_key(e), e.y, c);
         contrib_apply(c, a);
     }
     voxel_finish(A, g, row, vc, a);
@@ -2408,7 +2461,7 @@ constexpr int kLongChunk = 256; // contributions staged per step of the sequenti
 template <int kMax>
 constexpr size_t long_smem()
 {
-    return (size_t)kMax * 12 + (size_t)kLongChunk * sizeof(Contrib);
+    return (size_t)kMax * 8 + (size_t)kLongChunk * sizeof(Contrib);
 }
 
 // One CTA per voxel with a long contribution list (coarse grids over dense
@@ -2420,9 +2473,9 @@ constexpr size_t long_smem()
 template <int kMax, int kThreadsT, bool kHuge, bool B, int P>
 __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
 {
-    extern __shared__ unsigned long long lsm[];
-    unsigned long long *key = lsm;
-    uint32_t *pay = reinterpret_cast<uint32_t *>(key + kMax);
+    extern __shared__ uint4 lsm[];
+    uint32_t *key = reinterpret_cast<uint32_t *>(lsm);
+    uint32_t *pay = key + kMax;
     Contrib *cb = reinterpret_cast<Contrib *>(pay + kMax);
     const int tid = threadIdx.x;
     const uint32_t nlong = min(A.counters[kHuge ? C_HUGE : C_LONG], A.longv_cap);
@@ -2434,7 +2487,7 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
         const uint32_t n = (uint32_t)(d >> 40) & kListCountMax;
         const int vc[3] = {A.vox[row * 3 + 0], A.vox[row * 3 + 1], A.vox[row * 3 + 2]};
         const Grid &g = mesh_of<B>(A, seg_of_row<B>(A, row)).g;
-        uint4 *lst = A.contrib + first;
+        uint2 *lst = A.contrib + first;
         std::conditional_t<P == 0, Acc, AccC> a;
         acc_init(a);
         if (n <= (uint32_t)kMax)
@@ -2446,13 +2499,13 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
             {
                 if (i < n)
                 {
-                    const uint4 e = lst[i];
+                    const uint2 e = lst[i];
                     key[i] = entry_key(e);
-                    pay[i] = e.z;
+                    pay[i] = e.y;
                 }
                 else
                 {
-                    key[i] = ~0ull;
+                    key[i] = ~0u;
                     pay[i] = 0u;
                 }
             }
@@ -2466,7 +2519,7 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
                         if (l > i)
                         {
                             const bool up = (i & k) == 0;
-                            const unsigned long long ki = key[i], kl = key[l];
+                            const uint32_t ki = key[i], kl = key[l];
                             if ((ki > kl) == up)
                             {
                                 key[i] = kl;
@@ -2495,12 +2548,12 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
         {
             for (uint32_t x = 1; x < n; ++x)
             {
-                const uint4 e = lst[x];
-                const unsigned long long k = entry_key(e);
+                const uint2 e = lst[x];
+                const uint32_t k = entry_key(e);
                 uint32_t j = x;
                 while (j > 0)
                 {
-                    const uint4 pe = lst[j - 1];
+                    const uint2 pe = lst[j - 1];
                     if (entry_key(pe) <= k)
                         break;
                     lst[j] = pe;
@@ -2511,9 +2564,9 @@ __global__ void __launch_bounds__(kThreadsT) voxel_accumulate_long(SolveArgs A)
             }
             for (uint32_t x = 0; x < n; ++x)
             {
-                const uint4 e = lst[x];
+                const uint2 e = lst[x];
                 Contrib c;
-                contrib_load(A, g, vc, entry_key(e), e.z, c);
+                contrib_load(A, g, vc, entry_key(e), e.y, c);
                 contrib_apply(c, a);
             }
         }
@@ -2913,7 +2966,8 @@ struct ovx_fdg_context
     int sms = 148;
     Buf bits, bcount, bbase, aflag, aslot, active, counters, scan_large, scan_units, face_large, face_units, qtab;
     Buf vcnt, voff, emax, bkeys, blong, boff, btab;
-    Buf rcnt, roff, rec, clist, cub_tmp, cub_tmp_side, contrib, vlist, fstage, estage, longv, face_end;
+    Buf rcnt, roff, rec, cub_tmp, cub_tmp_side, vlist, longv, face_end;
+    Buf arena; // staged event records, then staged face records; after the fills, the contribution lists
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
     Buf segs_d;                             // batched conversion: the meshes (device copy of segs)
     std::vector<Mesh> segs;                 // batched conversion: the meshes, with their global offsets
@@ -2945,6 +2999,8 @@ struct ovx_fdg_context
     bool face_staged = false;                         // all of them fitted: the fill pass need not redo the tests
     unsigned long long n_estaged = 0, estage_want = 0; // the same for the scanline event records
     bool event_staged = false;
+    unsigned long long estage_n = 0, fstage_n = 0; // staging room in the arena: event records, then face records
+    unsigned long long n_events = 0, n_contrib = 0; // scanline events; contribution entries (4 per event, 1 per other record)
     int order = 0;                                    // output row order: 0 brick-linear, 1 z-order
     int finished = 0;
     long long launches = 0; // kernels this library launched (its own, not CUB's)
@@ -2957,6 +3013,9 @@ struct ovx_fdg_context
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool done_valid = false;
+    bool grew = false; // a buffer grew during this conversion: the pool gives back what it no longer backs
+    long long clist_limit = -1; // entries of the deferred constrained list (-1: as many as fit; tests set
+                                // OVX_FDG_CLIST_LIMIT to send voxels down the inline path)
 };
 
 namespace
@@ -2967,7 +3026,7 @@ int buffer_list(Ctx *c, Buf **out)
 {
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large, &c->scan_units,
                 &c->face_large, &c->face_units, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->blong, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
-                &c->clist, &c->cub_tmp, &c->cub_tmp_side, &c->contrib, &c->vlist, &c->fstage, &c->estage, &c->longv, &c->face_end,
+                &c->cub_tmp, &c->cub_tmp_side, &c->vlist, &c->arena, &c->longv, &c->face_end,
                 &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase, &c->segs_d};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
@@ -3062,7 +3121,8 @@ cudaError_t ensure(cudaStream_t st, ovx_fdg_context *ctx, Buf &b, size_t bytes)
         b.p = nullptr;
         b.cap = 0;
     }
-    const size_t want = bytes + bytes / 4 + 256;
+    const size_t want = bytes + bytes / 8 + 256;
+    ctx->grew = true;
     cudaError_t e = cudaMallocFromPoolAsync(&b.p, want, ctx->pool, st);
     if (e != cudaSuccess)
     {
@@ -3313,10 +3373,11 @@ GenArgs make_gen(ovx_fdg_context *ctx)
     A.rec = (Rec *)ctx->rec.p;
     A.qtab = (float *)ctx->qtab.p;
     A.btab = (float *)ctx->btab.p;
-    A.fstage = (uint4 *)ctx->fstage.p;
-    A.fstage_cap = cap_u32(ctx->fstage, sizeof(uint4));
-    A.estage = (uint4 *)ctx->estage.p;
-    A.estage_cap = cap_u32(ctx->estage, sizeof(uint4));
+    // staging: event records, then face records, in the arena
+    A.estage = ctx->estage_n ? (uint4 *)ctx->arena.p : nullptr;
+    A.estage_cap = (uint32_t)ctx->estage_n;
+    A.fstage = ctx->fstage_n ? (uint4 *)ctx->arena.p + ctx->estage_n : nullptr;
+    A.fstage_cap = (uint32_t)ctx->fstage_n;
     A.counters = (uint32_t *)ctx->counters.p;
     A.scan_large = (uint32_t *)ctx->scan_large.p;
     A.scan_units = (uint32_t *)ctx->scan_units.p;
@@ -3478,20 +3539,19 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(ensure(st, ctx, ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
         OVX_CUDA(ensure(st, ctx, ctx->qtab, (size_t)(nf + 1) * 48));
+    ctx->estage_n = ctx->fstage_n = 0;
     if (full)
     {
-        // staging room for the event records: the most seen so far, else a guess
+        // staging room for the event records and then the face records, one
+        // arena: for each, the most seen so far, else a guess
         const unsigned long long guess = std::min(24ull * (unsigned long long)nf, 4ull * (unsigned long long)nf + (16ull << 20));
-        const unsigned long long want = std::max(ctx->estage_want, guess);
-        OVX_CUDA(ensure(st, ctx, ctx->estage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
-    }
-    if (full && ctx->fw > 0.0f)
-    {
-        // staging room for the face records: the most seen so far, else a guess
-        const unsigned long long guess = std::min(24ull * (unsigned long long)nf, 4ull * (unsigned long long)nf + (16ull << 20));
-        const unsigned long long want = std::max(ctx->fstage_want, guess);
-        OVX_CUDA(ensure(st, ctx, ctx->fstage, (size_t)std::min(want, 0xffffffffull) * sizeof(uint4)));
-        OVX_CUDA(ensure(st, ctx, ctx->face_end, (size_t)(nb + 1) * 4));
+        ctx->estage_n = std::min(std::max(ctx->estage_want, guess), 0xffffffffull);
+        if (ctx->fw > 0.0f)
+        {
+            ctx->fstage_n = std::min(std::max(ctx->fstage_want, guess), 0xffffffffull);
+            OVX_CUDA(ensure(st, ctx, ctx->face_end, (size_t)(nb + 1) * 4));
+        }
+        OVX_CUDA(ensure(st, ctx, ctx->arena, (size_t)(ctx->estage_n + ctx->fstage_n) * sizeof(uint4)));
     }
     if (boundary)
     {
@@ -3609,6 +3669,14 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     }
     OVX_CUDA(cudaGetLastError());
     OVX_CUDA(cudaStreamSynchronize(st));
+    if (ctx->grew)
+    {
+        // the blocks freed by growth (this conversion's and the last one's) are
+        // no longer in use: give them back instead of holding them
+        ctx->grew = false;
+        if (cudaMemPoolTrimTo(ctx->pool, 0) != cudaSuccess)
+            cudaGetLastError();
+    }
     const uint32_t *hc = (const uint32_t *)&ctx->host[kHostCounters];
     const int rc = status_to_error(ctx, hc[C_STATUS]);
     if (rc != OVX_FDG_OK)
@@ -3624,11 +3692,14 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     ctx->n_funits = hc[C_FUNITS];
     ctx->n_blong = hc[C_BLONG];
     ctx->n_estaged = full ? hc[C_ESTAGED] : 0u;
-    ctx->event_staged = full && ctx->n_estaged <= (unsigned long long)cap_u32(ctx->estage, sizeof(uint4));
+    ctx->event_staged = full && ctx->n_estaged <= ctx->estage_n;
     ctx->estage_want = std::max(ctx->estage_want, ctx->n_estaged);
     ctx->n_fstaged = full ? hc[C_FSTAGED] : 0u;
-    ctx->face_staged = full && ctx->n_fstaged <= (unsigned long long)cap_u32(ctx->fstage, sizeof(uint4));
+    ctx->face_staged = full && ctx->n_fstaged <= ctx->fstage_n;
     ctx->fstage_want = std::max(ctx->fstage_want, ctx->n_fstaged);
+    // contribution entries: four per scanline event, one per face or boundary record
+    ctx->n_events = full ? hc[C_EVENTS] : 0u;
+    ctx->n_contrib = full ? 4ull * ctx->n_events + ((unsigned long long)ctx->n_rec - ctx->n_estaged) : 0ull;
     *num_voxels = (int64_t)n;
     return OVX_FDG_OK;
 }
@@ -3655,7 +3726,7 @@ int launch_consume(ovx_fdg_context *ctx, const SolveArgs &SA, cudaStream_t st, l
     ctx->launches += 3;
     stage(ctx, EV_SOLVE, st);
     constrained_solve<B><<<(unsigned)std::min<long long>(ctx->sms * 8, blocks_for(n, 128)), 128, 0, st>>>(
-        (const float *)ctx->clist.p, (const uint32_t *)ctx->counters.p, SA.clist_cap, ctx->g, SA.segs, SA.nseg, SA.dual);
+        SA.clist, (const uint32_t *)ctx->counters.p, SA.clist_cap, ctx->g, SA.segs, SA.nseg, SA.dual);
     ++ctx->launches;
     OVX_CUDA(cudaGetLastError());
     return OVX_FDG_OK;
@@ -3681,6 +3752,8 @@ int ovx_fdg_context_create(int device, ovx_fdg_context **out)
     }
     ovx_fdg_context *ctx = new ovx_fdg_context();
     ctx->device = device;
+    if (const char *lim = std::getenv("OVX_FDG_CLIST_LIMIT"))
+        ctx->clist_limit = std::max(0ll, std::atoll(lim));
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
@@ -3960,6 +4033,12 @@ int64_t ovx_fdg_workspace_bytes(const ovx_fdg_context *ctx)
     int64_t s = 0;
     for (int i = 0; i < n; ++i)
         s += (int64_t)list[i]->cap;
+    // what the pool holds on the device, freed blocks it kept included
+    unsigned long long reserved = 0;
+    if (ctx->pool && cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess)
+        s = std::max(s, (int64_t)reserved);
+    else
+        cudaGetLastError();
     return s;
 }
 
@@ -3982,8 +4061,8 @@ int ovx_fdg_begin(ovx_fdg_context *ctx, void *stream, const float *vertices, int
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "NULL vertices or faces");
     if (face_index_bytes != 4 && face_index_bytes != 8)
         return fail(ctx, OVX_FDG_INVALID_ARGUMENT, "face_index_bytes must be 4 or 8");
-    if (num_faces >= (1ll << 30) || num_vertices >= (1ll << 31) - 1)
-        return fail(ctx, OVX_FDG_CAPACITY, "more than 2^30 faces or 2^31-1 vertices");
+    if (num_faces > kMaxTriangles || num_vertices >= (1ll << 31) - 1)
+        return fail(ctx, OVX_FDG_CAPACITY, "more than 2^28-1 faces or 2^31-2 vertices");
     Grid g{};
     int rc = check_grid(ctx, grid, g);
     if (rc != OVX_FDG_OK)
@@ -4060,8 +4139,8 @@ int ovx_fdg_begin_batch(ovx_fdg_context *ctx, void *stream, const ovx_fdg_mesh *
         brick += g.nbricks;
         vert += m.num_vertices;
     }
-    if (tri >= (1ll << 30) || vert >= (1ll << 31) - 1)
-        return fail(ctx, OVX_FDG_CAPACITY, "batch: more than 2^30 faces or 2^31-1 vertices in all");
+    if (tri > kMaxTriangles || vert >= (1ll << 31) - 1)
+        return fail(ctx, OVX_FDG_CAPACITY, "batch: more than 2^28-1 faces or 2^31-2 vertices in all");
     if (brick >= (1ll << 31) || brick * kWordsPerBrick * 4ll > (64ll << 30))
         return fail(ctx, OVX_FDG_CAPACITY, "batch: grids too large for the dense brick bitmap (64 GiB limit)");
     const DeviceScope scope(ctx->device);
@@ -4141,10 +4220,9 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     const DeviceScope scope(ctx->device);
     OVX_CUDA(scope.status);
     const long long nb = ctx->g.nbricks;
-    OVX_CUDA(ensure(st, ctx, ctx->rec, (size_t)ctx->n_rec * sizeof(Rec)));
+    // the record buffer holds the constrained-search list once the lists are built
+    OVX_CUDA(ensure(st, ctx, ctx->rec, std::max((size_t)ctx->n_rec * sizeof(Rec), (size_t)64 * 1024)));
     OVX_CUDA(ensure(st, ctx, ctx->btab, (size_t)(ctx->n_boundary + 1) * 48));
-    OVX_CUDA(ensure(st, ctx, ctx->clist, (size_t)(n + 1) * 16 * 4));
-    OVX_CUDA(ensure(st, ctx, ctx->contrib, (size_t)(4 * ctx->n_rec + 1) * 16));
     OVX_CUDA(ensure(st, ctx, ctx->vlist, (size_t)n * 8));
     OVX_CUDA(ensure(st, ctx, ctx->longv, (size_t)(n + 1) * 4));
     OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_LONG, 0, 4, st));
@@ -4160,6 +4238,10 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     launch_faces_boundary_any<FILL>(ctx, A, st);
     OVX_CUDA(cudaGetLastError());
     stage(ctx, EV_RECORD_FILL, st);
+    // the staged records are in their buckets: the arena now takes the
+    // contribution lists (a growth frees the old block behind the fills)
+    OVX_CUDA(ensure(st, ctx, ctx->arena, (size_t)(ctx->n_contrib + 1) * sizeof(uint2)));
+    OVX_CUDA(cudaMemsetAsync((uint32_t *)ctx->counters.p + C_CONTRIB, 0, 8, st));
 
     SolveArgs SA{};
     SA.m = make_mesh(ctx);
@@ -4186,12 +4268,17 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     SA.dual = dual_vertices;
     SA.flags = intersected;
     SA.counters = (uint32_t *)ctx->counters.p;
-    SA.clist = (float *)ctx->clist.p;
-    SA.contrib = (uint4 *)ctx->contrib.p;
+    SA.clist = (float *)ctx->rec.p;
+    SA.contrib = (uint2 *)ctx->arena.p;
+    SA.contrib_cap = ctx->arena.cap / sizeof(uint2);
+    SA.key_face = (uint32_t)(12 * ctx->nf);
+    SA.key_boundary = (uint32_t)(13 * ctx->nf);
     SA.vlist = (unsigned long long *)ctx->vlist.p;
     SA.longv = (uint32_t *)ctx->longv.p;
     SA.longv_cap = (uint32_t)(n + 1);
-    SA.clist_cap = (uint32_t)(n + 1);
+    SA.clist_cap = (uint32_t)std::min<size_t>(ctx->rec.cap / 64, (size_t)n + 1);
+    if (ctx->clist_limit >= 0)
+        SA.clist_cap = (uint32_t)std::min<long long>(SA.clist_cap, ctx->clist_limit);
     SA.route_tol = ctx->route_tol;
     const int cr = ctx->batch ? (ctx->precision ? launch_consume<true, 1>(ctx, SA, st, n) : launch_consume<true, 0>(ctx, SA, st, n))
                               : (ctx->precision ? launch_consume<false, 1>(ctx, SA, st, n) : launch_consume<false, 0>(ctx, SA, st, n));

@@ -228,3 +228,31 @@ def test_host_tensors(cuda):
     assert batch[0][0].device.type == "cpu" and batch[1][0].is_cuda
     for a, b, c in zip(batch[0], batch[1], host):
         assert torch.equal(a, b.cpu()) and torch.equal(a, c)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("limit", [0, 7])
+def test_constrained_list_full(cuda, limit, monkeypatch):
+    """Voxels that the deferred constrained-search list cannot take (its room
+    capped by OVX_FDG_CLIST_LIMIT at context creation) are searched inline by
+    the accumulate kernels: the results stay bit-exact, for the short-list
+    kernel and (a 40k-face mesh on a 24^3 grid, whose lists run long) the
+    long-list kernels."""
+    import torch
+    import ovx_fdg_abi as abi
+
+    monkeypatch.setenv("OVX_FDG_CLIST_LIMIT", str(limit))
+    coarse = W.primitives(3, faces_total=40_000)
+    coarse.grid_size = 24
+    for w in (W.ico_cap(1), W.primitives(3, faces_total=40_000), coarse):
+        _, _, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
+        ab = np.asarray(w.aabb, np.float32).reshape(2, 3)
+        ctx = abi.Context(cuda.index or 0)
+        try:
+            vt = torch.from_numpy(w.vertices).to(cuda)
+            ft = torch.from_numpy(w.faces).to(cuda)
+            out = ctx.mesh_to_fdg(vt, ft, ab[0], vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+            torch.cuda.synchronize()
+            assert_fdg_equal(tuple(t.cpu().numpy() for t in out), _oracle(w), f"{w.name} clist limit {limit}")
+        finally:
+            ctx.close()
