@@ -438,6 +438,48 @@ __device__ __forceinline__ bool face_test_c(const Coef &C, const Grid &g, int x,
     return ok;
 }
 
+// True when no voxel of the index box [lo, hi) (absolute voxel indices, each
+// range non-empty) can pass face_test_c.  Exact, not an estimate: every test
+// is a sum of products of a fixed coefficient and a coordinate vs * i, and
+// IEEE rounding is monotone, so each computed test value is monotone in every
+// coordinate; evaluated with the same operations at the box corner that
+// maximises (or minimises) it, it bounds the computed value of every voxel of
+// the box.  A test that fails at its best corner fails for the whole box.
+// NaN coefficients reject nothing (every comparison is false).
+template <typename Coef>
+__device__ __forceinline__ bool face_box_rejects(const Coef &C, const Grid &g, const int lo[3], const int hi[3])
+{
+    // coordinate of axis a at the corner maximising (want_max) or minimising c * p
+    auto pick = [&](float c, int a, bool want_max) -> float {
+        const int i = ((c >= 0.0f) == want_max) ? hi[a] - 1 : lo[a];
+        return g.vs[a] * (float)i;
+    };
+    // plane slab: fails where (nd + d1) and (nd + d2) are both positive (or
+    // both negative) with a positive product; nd is smallest (largest) at one corner
+    const float nlo = dot3f(C(0), C(1), C(2), pick(C(0), 0, false), pick(C(1), 1, false), pick(C(2), 2, false));
+    const float ul = nlo + C(3), wl = nlo + C(4);
+    if (ul > 0.0f && wl > 0.0f && ul * wl > 0.0f)
+        return true;
+    const float nhi = dot3f(C(0), C(1), C(2), pick(C(0), 0, true), pick(C(1), 1, true), pick(C(2), 2, true));
+    const float uh = nhi + C(3), wh = nhi + C(4);
+    if (uh < 0.0f && wh < 0.0f && uh * wh > 0.0f)
+        return true;
+    // the 9 edge half-planes: fail where the value is negative; largest at one corner
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (dot2f(C(5 + 2 * k), C(6 + 2 * k), pick(C(5 + 2 * k), 0, true), pick(C(6 + 2 * k), 1, true)) + C(11 + k) < 0.0f)
+            return true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (dot2f(C(14 + 2 * k), C(15 + 2 * k), pick(C(14 + 2 * k), 1, true), pick(C(15 + 2 * k), 2, true)) + C(20 + k) < 0.0f)
+            return true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        if (dot2f(C(23 + 2 * k), C(24 + 2 * k), pick(C(23 + 2 * k), 2, true), pick(C(24 + 2 * k), 0, true)) + C(29 + k) < 0.0f)
+            return true;
+    return false;
+}
+
 struct FaceCoefRegs
 {
     const FaceSetup &fs;

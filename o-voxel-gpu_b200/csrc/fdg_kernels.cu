@@ -895,6 +895,7 @@ __device__ __forceinline__ uint32_t box_word(uint32_t word, int w, const int lo[
 }
 
 constexpr int kFaceThreads = 128; // face pass: one triangle per lane
+constexpr int kRejectMin = 4;     // (triangle, brick) items with more candidates first test the whole box
 constexpr int kFaceWindow = 512; // candidates listed per step of a warp
 static_assert(kFaceWindow >= kBrick * kBrick * kBrick, "a dense item's candidates (up to a whole brick) fit the list");
 static_assert(kFaceWindow >= kWordsPerBrick * 4, "the slot list holds a dense item's words");
@@ -1055,6 +1056,19 @@ __device__ __forceinline__ void face_item(const GenArgs &A, FaceWarp &W, const i
             {
                 cw[q4 * 4 + k] = any ? box_word(words[k], q4 * 4 + k, lo, hi) : 0u;
                 cnt += __popc(cw[q4 * 4 + k]);
+            }
+        }
+        if (cnt > (uint32_t)kRejectMin)
+        {
+            // the triangle misses the item's whole box: no candidate can pass
+            const int alo[3] = {o[0] + lo[0], o[1] + lo[1], o[2] + lo[2]};
+            const int ahi[3] = {o[0] + hi[0], o[1] + hi[1], o[2] + hi[2]};
+            if (face_box_rejects(FaceCoefSmem{&W.coef[0][ol]}, g, alo, ahi))
+            {
+                cnt = 0;
+#pragma unroll
+                for (int w = 0; w < kWordsPerBrick; ++w)
+                    cw[w] = 0u;
             }
         }
 #pragma unroll
@@ -1306,13 +1320,24 @@ __global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
     for (long long ub = ((long long)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; ub < (long long)total; ub += stride)
     {
         const long long u = ub + lane;
-        bool valid = false;
+        const bool inside = u < (long long)total;
         int r = 0;
-        if (u < (long long)total)
+        uint32_t i = 0xffffffffu;
+        if (inside)
         {
-            const uint32_t i = unit_owner(A.face_units, n, (uint32_t)u);
-            const uint32_t t = A.face_large[i];
+            i = unit_owner(A.face_units, n, (uint32_t)u);
             r = (int)((uint32_t)u - A.face_units[i]);
+        }
+        // a triangle's items are consecutive: the first lane of each run sets
+        // the triangle up once, the run's other lanes use that lane's column
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, i, 1);
+        const bool first = inside && (lane == 0 || prev != i);
+        const uint32_t firsts = __ballot_sync(0xffffffffu, first);
+        const int ol = 31 - __clz(firsts & (0xffffffffu >> (31 - lane)));
+        bool ok = false;
+        if (first)
+        {
+            const uint32_t t = A.face_large[i];
             const int sg = seg_of_tri<B>(A, t);
             const Mesh &Ms = mesh_of<B>(A, sg);
             const Grid &g = Ms.g;
@@ -1329,11 +1354,13 @@ __global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
                     b1[a] = (bmax[a] - 1 - g.gmin[a]) >> 3;
                 }
                 face_lane_setup(W, lane, v, g, bmin, bmax, b0, b1[0] - b0[0] + 1, b1[1] - b0[1] + 1, t, sg);
-                valid = true;
+                ok = true;
             }
         }
+        const uint32_t oks = __ballot_sync(0xffffffffu, ok);
+        const bool valid = inside && ((oks >> ol) & 1u);
         __syncwarp();
-        face_item<M, B>(A, W, lane, valid, lane, r);
+        face_item<M, B>(A, W, lane, valid, inside ? ol : lane, r);
         __syncwarp();
     }
 }
