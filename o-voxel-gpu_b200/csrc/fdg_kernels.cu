@@ -1706,7 +1706,8 @@ __global__ void edge_sort_count(const unsigned long long *__restrict__ voff, uin
 // Per vertex a: its boundary edges at their rank in (a, b) order, so the
 // boundary list is sorted like the reference's std::map.
 __global__ void edge_emit(const unsigned long long *__restrict__ voff, const uint32_t *__restrict__ emax, long long nv,
-                          const unsigned long long *__restrict__ boff, unsigned long long *__restrict__ bkeys)
+                          const unsigned long long *__restrict__ boff, unsigned long long *__restrict__ bkeys,
+                          unsigned long long bkeys_cap, uint32_t *__restrict__ counters)
 {
     const long long a = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= nv)
@@ -1721,7 +1722,13 @@ __global__ void edge_emit(const unsigned long long *__restrict__ voff, const uin
         while (j < n && l[j] == l[i])
             ++j;
         if (j - i == 1)
-            bkeys[k++] = ((unsigned long long)a << 32) | l[i];
+        {
+            if (k < bkeys_cap)
+                bkeys[k] = ((unsigned long long)a << 32) | l[i];
+            else
+                atomicOr(&counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
+            ++k;
+        }
         i = j;
     }
 }
@@ -3041,6 +3048,11 @@ struct ovx_fdg_context
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     bool done_valid = false;
     bool grew = false; // a buffer grew during this conversion: the pool gives back what it no longer backs
+    // work lists of begin (large pairs, large triangles, long boundary edges,
+    // boundary edges): sized from the most entries seen, else a guess; a
+    // conversion whose lists overflow runs its begin once more with exact sizes
+    unsigned long long want_scan = 0, want_face = 0, want_blong = 0, want_bkeys = 0;
+    unsigned long long list_guess = 65536; // floor of the guess (tests set OVX_FDG_LIST_GUESS)
     long long clist_limit = -1; // entries of the deferred constrained list (-1: as many as fit; tests set
                                 // OVX_FDG_CLIST_LIMIT to send voxels down the inline path)
 };
@@ -3546,8 +3558,9 @@ void launch_faces_boundary_any(ovx_fdg_context *ctx, const GenArgs &A, cudaStrea
 
 // Occupancy stage shared by the full conversion and intersect_occ; ends with
 // the one host synchronisation of a conversion.
-int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *num_voxels)
+int occupancy_pass(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *num_voxels, bool *retry)
 {
+    *retry = false;
     const Grid &g = ctx->g;
     const long long nf = ctx->nf, nb = g.nbricks;
     const bool boundary = full && ctx->bw > 0.0f;
@@ -3558,10 +3571,15 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     OVX_CUDA(ensure(st, ctx, ctx->aslot, (size_t)(nb + 1) * 8));
     OVX_CUDA(ensure(st, ctx, ctx->active, (size_t)(nb + 1) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->counters, C_WORDS * 4));
-    OVX_CUDA(ensure(st, ctx, ctx->scan_large, (size_t)(3 * nf + 1) * 4));
-    OVX_CUDA(ensure(st, ctx, ctx->scan_units, (size_t)(3 * nf + 2) * 4));
-    OVX_CUDA(ensure(st, ctx, ctx->face_large, (size_t)(nf + 1) * 4));
-    OVX_CUDA(ensure(st, ctx, ctx->face_units, (size_t)(nf + 2) * 4));
+    // work lists: the most entries seen, else a guess, never above the worst case
+    auto list_room = [&](unsigned long long worst, unsigned long long want) {
+        return std::min(worst, std::max(want, worst / 16 + ctx->list_guess));
+    };
+    const unsigned long long n_scan = list_room(3ull * nf, ctx->want_scan), n_face = list_room((unsigned long long)nf, ctx->want_face);
+    OVX_CUDA(ensure(st, ctx, ctx->scan_large, (size_t)(n_scan + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->scan_units, (size_t)(n_scan + 2) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->face_large, (size_t)(n_face + 1) * 4));
+    OVX_CUDA(ensure(st, ctx, ctx->face_units, (size_t)(n_face + 2) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->rcnt, (size_t)(nb + 1) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
@@ -3585,8 +3603,8 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         OVX_CUDA(ensure(st, ctx, ctx->vcnt, (size_t)(ctx->nv + 1) * 4));
         OVX_CUDA(ensure(st, ctx, ctx->voff, (size_t)(ctx->nv + 1) * 8));
         OVX_CUDA(ensure(st, ctx, ctx->emax, (size_t)(3 * nf + 1) * 4));
-        OVX_CUDA(ensure(st, ctx, ctx->bkeys, (size_t)(3 * nf + 1) * 8));
-        OVX_CUDA(ensure(st, ctx, ctx->blong, (size_t)(3 * nf + 1) * 4));
+        OVX_CUDA(ensure(st, ctx, ctx->bkeys, (size_t)(list_room(3ull * nf, ctx->want_bkeys) + 1) * 8));
+        OVX_CUDA(ensure(st, ctx, ctx->blong, (size_t)(list_room(3ull * nf, ctx->want_blong) + 1) * 4));
         OVX_CUDA(ensure(st, ctx, ctx->boff, (size_t)(ctx->nv + 1) * 8));
     }
     OVX_CUDA(cudaMemsetAsync(ctx->bits.p, 0, (size_t)nb * kWordsPerBrick * 4, st));
@@ -3631,7 +3649,8 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
         unsigned long long *boff = (unsigned long long *)ctx->boff.p;
         OVX_CUDA(exclusive_scan(ctx, (const uint32_t *)vcnt, boff, ctx->nv + 1, es, &ctx->cub_tmp_side));
         edge_emit<<<blocks_for(ctx->nv, kThreads), kThreads, 0, es>>>(voff, (const uint32_t *)ctx->emax.p, ctx->nv, boff,
-                                                                     (unsigned long long *)ctx->bkeys.p);
+                                                                     (unsigned long long *)ctx->bkeys.p,
+                                                                     ctx->bkeys.cap / 8, (uint32_t *)ctx->counters.p);
         // boundary edge count -> counters[C_BOUNDARY] (low word of the u64 total; at most 3F < 2^32), by a
         // kernel rather than a copy, which could queue behind another stream's large copy
         copy_word<<<1, 1, 0, es>>>((const uint32_t *)(boff + ctx->nv), (uint32_t *)ctx->counters.p + C_BOUNDARY);
@@ -3705,6 +3724,25 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
             cudaGetLastError();
     }
     const uint32_t *hc = (const uint32_t *)&ctx->host[kHostCounters];
+    if (hc[C_STATUS] == (uint32_t)ST_LIST_OVERFLOW)
+    {
+        // a work list was too small: the counters hold the exact entry counts
+        const GenArgs caps = make_gen(ctx); // the capacities the kernels used
+        const bool over = hc[C_SCAN_LARGE] > caps.scan_large_cap || hc[C_FACE_LARGE] > caps.face_large_cap ||
+                          (boundary && (hc[C_BLONG] > caps.blong_cap || hc[C_BOUNDARY] > caps.bkeys_cap));
+        if (over)
+        {
+            ctx->want_scan = std::max(ctx->want_scan, (unsigned long long)hc[C_SCAN_LARGE]);
+            ctx->want_face = std::max(ctx->want_face, (unsigned long long)hc[C_FACE_LARGE]);
+            if (boundary)
+            {
+                ctx->want_blong = std::max(ctx->want_blong, (unsigned long long)hc[C_BLONG]);
+                ctx->want_bkeys = std::max(ctx->want_bkeys, (unsigned long long)hc[C_BOUNDARY]);
+            }
+            *retry = true;
+            return OVX_FDG_OK;
+        }
+    }
     const int rc = status_to_error(ctx, hc[C_STATUS]);
     if (rc != OVX_FDG_OK)
         return rc;
@@ -3729,6 +3767,23 @@ int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *n
     ctx->n_contrib = full ? 4ull * ctx->n_events + ((unsigned long long)ctx->n_rec - ctx->n_estaged) : 0ull;
     *num_voxels = (int64_t)n;
     return OVX_FDG_OK;
+}
+
+// The occupancy pass, run again with larger work lists when one overflowed.
+// A pass counts every list's entries in full except the long boundary edges
+// when the boundary list itself overflowed (only the edges that fitted were
+// walked), so a second replay may be needed; each replay only grows a list.
+int occupancy_stage(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *num_voxels)
+{
+    for (int attempt = 0;; ++attempt)
+    {
+        bool retry = false;
+        const int rc = occupancy_pass(ctx, st, full, num_voxels, &retry);
+        if (rc != OVX_FDG_OK || !retry)
+            return rc;
+        if (attempt >= 3)
+            return fail(ctx, OVX_FDG_INTERNAL, "work list overflow");
+    }
 }
 
 // The per-brick lists, the per-voxel sums and solves, and the constrained
@@ -3781,6 +3836,8 @@ int ovx_fdg_context_create(int device, ovx_fdg_context **out)
     ctx->device = device;
     if (const char *lim = std::getenv("OVX_FDG_CLIST_LIMIT"))
         ctx->clist_limit = std::max(0ll, std::atoll(lim));
+    if (const char *gs = std::getenv("OVX_FDG_LIST_GUESS"))
+        ctx->list_guess = (unsigned long long)std::max(1ll, std::atoll(gs));
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device);

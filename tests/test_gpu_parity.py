@@ -256,3 +256,34 @@ def test_constrained_list_full(cuda, limit, monkeypatch):
             assert_fdg_equal(tuple(t.cpu().numpy() for t in out), _oracle(w), f"{w.name} clist limit {limit}")
         finally:
             ctx.close()
+
+
+@pytest.mark.gpu
+def test_work_list_replay(cuda, monkeypatch):
+    """Work lists sized from a tiny guess (OVX_FDG_LIST_GUESS=1) overflow on
+    the first conversion -- the large pairs and large triangles of a low-poly
+    mesh, the long and the plain boundary edges of an open mesh -- and begin
+    runs once more with exact sizes; results stay bit-exact, and the next
+    conversion on the context fits the first time."""
+    import torch
+    import ovx_fdg_abi as abi
+
+    monkeypatch.setenv("OVX_FDG_LIST_GUESS", "1")
+    lp = W.lowpoly(5, faces_total=600, grid_size=256)
+    # the same triangles with no vertex shared: every edge is a boundary edge, most of them long
+    soup = W.Workload("lowpoly_soup", lp.vertices[lp.faces].reshape(-1, 3).copy(),
+                      np.arange(3 * lp.faces.shape[0], dtype=np.int64).reshape(-1, 3), lp.grid_size, lp.aabb)
+    for w in (lp, soup, W.ico_cap(2)):
+        _, _, vs, gr = O.grid_args(w.vertices, w.faces, w.grid_size, w.aabb)
+        ab = np.asarray(w.aabb, np.float32).reshape(2, 3)
+        want = _oracle(w)
+        ctx = abi.Context(cuda.index or 0)
+        try:
+            vt = torch.from_numpy(w.vertices).to(cuda)
+            ft = torch.from_numpy(w.faces).to(cuda)
+            for step in ("replayed", "sized"):
+                out = ctx.mesh_to_fdg(vt, ft, ab[0], vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
+                torch.cuda.synchronize()
+                assert_fdg_equal(tuple(t.cpu().numpy() for t in out), want, f"{w.name} ({step})")
+        finally:
+            ctx.close()
