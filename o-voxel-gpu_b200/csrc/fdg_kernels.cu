@@ -1690,6 +1690,35 @@ __global__ void edge_sort_count(const unsigned long long *__restrict__ voff, uin
     const unsigned long long s = voff[a], e = voff[a + 1];
     const long long n = (long long)(e - s);
     uint32_t *l = emax + s;
+    if (n <= 8)
+    {
+        // the usual case: the list in registers, Batcher's 19-comparator
+        // network for 8 (padding sorts last: vertex indices are below 2^31)
+        uint32_t r[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            r[i] = i < n ? l[i] : 0xffffffffu;
+        constexpr int net[19][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {1, 2}, {5, 6},
+                                    {0, 4}, {1, 5}, {2, 6}, {3, 7}, {2, 4}, {3, 5}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+        for (int k = 0; k < 19; ++k)
+        {
+            const uint32_t x = r[net[k][0]], y = r[net[k][1]];
+            r[net[k][0]] = min(x, y);
+            r[net[k][1]] = max(x, y);
+        }
+        uint32_t c = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (i < n)
+            {
+                l[i] = r[i];
+                const bool dup = (i > 0 && r[i - 1] == r[i]) || (i + 1 < n && r[i + 1] == r[i]);
+                c += dup ? 0u : 1u;
+            }
+        bcnt[a] = c;
+        return;
+    }
     sort_list(l, n);
     uint32_t c = 0;
     for (long long i = 0; i < n;)
