@@ -3508,10 +3508,14 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
                 ++ctx->launches;
             }
             // the boundary records follow the face records: the bucket cursors
-            // as the count pass left them after the faces
-            copy_words<<<blocks_for(ctx->g.nbricks + 1, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->face_end.p, A.rcnt,
-                                                                                    ctx->g.nbricks + 1);
-            ++ctx->launches;
+            // as the count pass left them after the faces (a fill that runs
+            // beside the event buckets uses that snapshot as its cursor)
+            if (A.rcnt != (uint32_t *)ctx->face_end.p)
+            {
+                copy_words<<<blocks_for(ctx->g.nbricks + 1, kThreads), kThreads, 0, st>>>((const uint32_t *)ctx->face_end.p,
+                                                                                        A.rcnt, ctx->g.nbricks + 1);
+                ++ctx->launches;
+            }
         }
         else
         {
@@ -4346,9 +4350,29 @@ int ovx_fdg_finish(ovx_fdg_context *ctx, void *stream, int32_t *voxel_indices, f
     stage(ctx, EV_FINISH, st);
     GenArgs A = make_gen(ctx);
     A.qtab = nullptr;
-    launch_events_any<FILL>(ctx, A, st);
-    stage(ctx, EV_EVENTS_FILL, st);
-    launch_faces_boundary_any<FILL>(ctx, A, st);
+    if (ctx->event_staged && ctx->face_staged && ctx->fw > 0.0f && ctx->bw > 0.0f && ctx->nf > 0 && ctx->side)
+    {
+        // every record was staged: the event buckets (cursor rcnt), the face
+        // records (at their staged ranks) and the boundary records (cursor:
+        // the per-brick counts after the faces, face_end) write disjoint
+        // places, so the face and boundary fills run on the side stream
+        // beside the event buckets
+        OVX_CUDA(cudaEventRecord(ctx->fork_ev, st));
+        OVX_CUDA(cudaStreamWaitEvent(ctx->side, ctx->fork_ev, 0));
+        GenArgs Af = A;
+        Af.rcnt = (uint32_t *)ctx->face_end.p;
+        launch_faces_boundary_any<FILL>(ctx, Af, ctx->side);
+        OVX_CUDA(cudaEventRecord(ctx->join_ev, ctx->side));
+        launch_events_any<FILL>(ctx, A, st);
+        stage(ctx, EV_EVENTS_FILL, st);
+        OVX_CUDA(cudaStreamWaitEvent(st, ctx->join_ev, 0));
+    }
+    else
+    {
+        launch_events_any<FILL>(ctx, A, st);
+        stage(ctx, EV_EVENTS_FILL, st);
+        launch_faces_boundary_any<FILL>(ctx, A, st);
+    }
     OVX_CUDA(cudaGetLastError());
     stage(ctx, EV_RECORD_FILL, st);
     // the staged records are in their buckets: the arena now takes the
