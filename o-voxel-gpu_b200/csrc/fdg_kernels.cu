@@ -726,21 +726,20 @@ __global__ void __launch_bounds__(kEventThreads) tri_events(GenArgs A)
     event_rows<M, B>(A, E, lane, nrows);
 }
 
-// In-place exclusive scan of the unit counts of a work list (one CTA): entry i
-// of `units` becomes the first unit of list entry i, entry n the total, which
-// also goes to counters[total_word].  n is read from counters[count_word].
-__global__ void __launch_bounds__(1024) unit_offsets(uint32_t *__restrict__ units, uint32_t cap, uint32_t *__restrict__ counters,
-                                                      int count_word, int total_word)
+// In-place exclusive scan of the unit counts of a work list: entry i of
+// `units` becomes the first unit of list entry i, entry n the total, which
+// also goes to counters[total_word].  n = min(counters[count_word], cap) is
+// known only on the device, so the scan covers the capacity in tiles of
+// kUnitTile entries (entries from n on count as 0) in three passes: tile
+// sums, one CTA scanning the tile sums, then each tile scanning its entries
+// from its offset.  A total of 2^32 units or more sets the list-overflow status.
+constexpr int kUnitTile = 1024;
+
+__device__ __forceinline__ unsigned long long block_exclusive_u64(unsigned long long v, unsigned long long *wsum,
+                                                                  unsigned long long &total)
 {
-    __shared__ unsigned long long wsum[32];
-    const uint32_t n = min(counters[count_word], cap);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
-    const uint32_t b0 = min(n, (uint32_t)tid * per), b1 = min(n, b0 + per);
-    unsigned long long sum = 0;
-    for (uint32_t i = b0; i < b1; ++i)
-        sum += units[i];
-    unsigned long long incl = sum;
+    unsigned long long incl = v;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1)
     {
@@ -766,23 +765,69 @@ __global__ void __launch_bounds__(1024) unit_offsets(uint32_t *__restrict__ unit
             wsum[lane] = w;
     }
     __syncthreads();
-    unsigned long long run = (warp > 0 ? wsum[warp - 1] : 0ull) + incl - sum;
+    total = wsum[(blockDim.x >> 5) - 1];
+    const unsigned long long ex = (warp > 0 ? wsum[warp - 1] : 0ull) + incl - v;
+    __syncthreads();
+    return ex;
+}
+
+__global__ void __launch_bounds__(kUnitTile) unit_tile_sums(const uint32_t *__restrict__ units, uint32_t cap,
+                                                            const uint32_t *__restrict__ counters, int count_word,
+                                                            unsigned long long *__restrict__ tile_sum)
+{
+    __shared__ unsigned long long wsum[32];
+    const uint32_t n = min(counters[count_word], cap);
+    const uint32_t i = blockIdx.x * kUnitTile + threadIdx.x;
+    unsigned long long total;
+    block_exclusive_u64(i < n ? units[i] : 0u, wsum, total);
+    if (threadIdx.x == 0)
+        tile_sum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) unit_tile_offsets(unsigned long long *__restrict__ tile_sum, uint32_t ntiles,
+                                                           uint32_t *__restrict__ units, uint32_t cap, uint32_t *__restrict__ counters,
+                                                           int count_word, int total_word)
+{
+    __shared__ unsigned long long wsum[32];
+    const int tid = threadIdx.x;
+    const uint32_t per = (ntiles + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = min(ntiles, (uint32_t)tid * per), b1 = min(ntiles, b0 + per);
+    unsigned long long sum = 0;
+    for (uint32_t i = b0; i < b1; ++i)
+        sum += tile_sum[i];
+    unsigned long long total;
+    unsigned long long run = block_exclusive_u64(sum, wsum, total);
     for (uint32_t i = b0; i < b1; ++i)
     {
-        const uint32_t u = units[i];
-        units[i] = (uint32_t)run;
-        run += u;
+        const unsigned long long t = tile_sum[i];
+        tile_sum[i] = run;
+        run += t;
     }
-    if (tid == (int)blockDim.x - 1)
+    if (tid == 0)
     {
-        if (run >= (1ull << 32))
+        const uint32_t n = min(counters[count_word], cap);
+        if (total >= (1ull << 32))
         {
             atomicOr(&counters[C_STATUS], (uint32_t)ST_LIST_OVERFLOW);
-            run = 0;
+            total = 0;
         }
-        units[n] = (uint32_t)run;
-        counters[total_word] = (uint32_t)run;
+        units[n] = (uint32_t)total;
+        counters[total_word] = (uint32_t)total;
     }
+}
+
+__global__ void __launch_bounds__(kUnitTile) unit_tile_scan(uint32_t *__restrict__ units, uint32_t cap,
+                                                            const uint32_t *__restrict__ counters, int count_word,
+                                                            const unsigned long long *__restrict__ tile_sum)
+{
+    __shared__ unsigned long long wsum[32];
+    const uint32_t n = min(counters[count_word], cap);
+    const uint32_t i = blockIdx.x * kUnitTile + threadIdx.x;
+    const uint32_t u = i < n ? units[i] : 0u;
+    unsigned long long total;
+    const unsigned long long ex = block_exclusive_u64(u, wsum, total);
+    if (i < n)
+        units[i] = (uint32_t)(tile_sum[blockIdx.x] + ex);
 }
 
 // Entry i of a scanned unit list with units[i] <= u < units[i + 1] (u below units[n]).
@@ -3032,6 +3077,7 @@ struct ovx_fdg_context
     Buf rcnt, roff, rec, cub_tmp, cub_tmp_side, vlist, longv, face_end;
     Buf arena; // staged event records, then staged face records; after the fills, the contribution lists
     Buf zkeys, zslots, zcnt, zsbase, zbase; // z-order row bases
+    Buf unit_tiles;                         // tile sums of the unit-list scans
     Buf segs_d;                             // batched conversion: the meshes (device copy of segs)
     std::vector<Mesh> segs;                 // batched conversion: the meshes, with their global offsets
     Mesh *segs_pinned = nullptr;            // staging of the mesh table for its upload (pinned)
@@ -3095,7 +3141,7 @@ int buffer_list(Ctx *c, Buf **out)
     Buf *b[] = {&c->bits, &c->bcount, &c->bbase, &c->aflag, &c->aslot, &c->active, &c->counters, &c->scan_large, &c->scan_units,
                 &c->face_large, &c->face_units, &c->qtab, &c->vcnt, &c->voff, &c->emax, &c->bkeys, &c->blong, &c->boff, &c->btab, &c->rcnt, &c->roff, &c->rec,
                 &c->cub_tmp, &c->cub_tmp_side, &c->vlist, &c->arena, &c->longv, &c->face_end,
-                &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase, &c->segs_d};
+                &c->zkeys, &c->zslots, &c->zcnt, &c->zsbase, &c->zbase, &c->segs_d, &c->unit_tiles};
     const int n = (int)(sizeof(b) / sizeof(b[0]));
     for (int i = 0; i < n; ++i)
         out[i] = b[i];
@@ -3461,6 +3507,22 @@ GenArgs make_gen(ovx_fdg_context *ctx)
     return A;
 }
 
+// The in-place scan of a unit list (unit_tile_sums, unit_tile_offsets,
+// unit_tile_scan); the occupancy pass sized unit_tiles for both lists.
+cudaError_t unit_scan(ovx_fdg_context *ctx, uint32_t *units, uint32_t cap, uint32_t *counters, int count_word, int total_word,
+                      cudaStream_t st)
+{
+    const uint32_t ntiles = cap / kUnitTile + 1;
+    if ((size_t)ntiles * 8 > ctx->unit_tiles.cap)
+        return cudaErrorInvalidValue;
+    unsigned long long *tiles = (unsigned long long *)ctx->unit_tiles.p;
+    unit_tile_sums<<<ntiles, kUnitTile, 0, st>>>(units, cap, counters, count_word, tiles);
+    unit_tile_offsets<<<1, 1024, 0, st>>>(tiles, ntiles, units, cap, counters, count_word, total_word);
+    unit_tile_scan<<<ntiles, kUnitTile, 0, st>>>(units, cap, counters, count_word, tiles);
+    ctx->launches += 3;
+    return cudaSuccess; // launch errors stay pending for the caller's check
+}
+
 template <int M, typename IdxT, bool B>
 void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
 {
@@ -3480,8 +3542,7 @@ void launch_events(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t st)
         ++ctx->launches;
         if (M == COUNT)
         {
-            unit_offsets<<<1, 1024, 0, st>>>(A.scan_units, A.scan_large_cap, A.counters, C_SCAN_LARGE, C_LUNITS);
-            ++ctx->launches;
+            unit_scan(ctx, A.scan_units, A.scan_large_cap, A.counters, C_SCAN_LARGE, C_LUNITS, st);
         }
         // the fill pass knows the units (32 a warp); the count pass does not yet
         const long long rows_grid = M == FILL ? std::min<long long>(ctx->sms * 8, blocks_for((long long)ctx->n_lunits, kEventThreads))
@@ -3526,8 +3587,7 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
         {
             if (M == COUNT)
             {
-                unit_offsets<<<1, 1024, 0, st>>>(A.face_units, A.face_large_cap, A.counters, C_FACE_LARGE, C_FUNITS);
-                ++ctx->launches;
+                unit_scan(ctx, A.face_units, A.face_large_cap, A.counters, C_FACE_LARGE, C_FUNITS, st);
             }
             const long long faces_grid =
                 M == FILL ? std::min<long long>(ctx->sms * 7, blocks_for((long long)ctx->n_funits, kFaceThreads)) : ctx->sms * 7;
@@ -3613,6 +3673,11 @@ int occupancy_pass(ovx_fdg_context *ctx, cudaStream_t st, bool full, int64_t *nu
     OVX_CUDA(ensure(st, ctx, ctx->scan_units, (size_t)(n_scan + 2) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->face_large, (size_t)(n_face + 1) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->face_units, (size_t)(n_face + 2) * 4));
+    {
+        // tile sums of the unit-list scans, for the lists as allocated
+        const size_t tiles = std::max(cap_u32(ctx->scan_large, 4), cap_u32(ctx->face_large, 4)) / kUnitTile + 2;
+        OVX_CUDA(ensure(st, ctx, ctx->unit_tiles, tiles * 8));
+    }
     OVX_CUDA(ensure(st, ctx, ctx->rcnt, (size_t)(nb + 1) * 4));
     OVX_CUDA(ensure(st, ctx, ctx->roff, (size_t)(nb + 1) * 8));
     if (full)
