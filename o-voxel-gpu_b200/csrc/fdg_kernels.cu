@@ -3589,8 +3589,21 @@ void launch_faces_boundary(ovx_fdg_context *ctx, const GenArgs &A, cudaStream_t 
             {
                 unit_scan(ctx, A.face_units, A.face_large_cap, A.counters, C_FACE_LARGE, C_FUNITS, st);
             }
+            // one resident wave: the kernel loops over the units, and a second,
+            // partial wave of CTAs only lengthens the tail
+            static int per_sm = 0;
+            if (per_sm < 1)
+            {
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, large_faces<M, IdxT, B>, kFaceThreads, 0) != cudaSuccess ||
+                    per_sm < 1)
+                {
+                    cudaGetLastError();
+                    per_sm = 4;
+                }
+            }
+            const long long wave = (long long)ctx->sms * per_sm;
             const long long faces_grid =
-                M == FILL ? std::min<long long>(ctx->sms * 7, blocks_for((long long)ctx->n_funits, kFaceThreads)) : ctx->sms * 7;
+                M == FILL ? std::min<long long>(wave, blocks_for((long long)ctx->n_funits, kFaceThreads)) : wave;
             if (faces_grid > 0)
             {
                 large_faces<M, IdxT, B><<<(unsigned)faces_grid, kFaceThreads, 0, st>>>(A);
