@@ -1350,8 +1350,9 @@ __global__ void __launch_bounds__(kThreads) bucket_records(const uint4 *__restri
 
 // Triangles whose face box spans more than tune.inline_face_bricks bricks: their
 // (triangle, brick) items, all listed triangles' items one after another, 32
-// per warp and round, one per lane; each lane sets up its own item's triangle
-// and the round runs as in face_records.
+// per warp and round, one per lane; the first lane of each run of a triangle's
+// items sets the triangle up for the run, and the round runs as in
+// face_records.  The grid is one resident wave; the warps loop over the units.
 template <int M, typename IdxT, bool B>
 __global__ void __launch_bounds__(kFaceThreads) large_faces(GenArgs A)
 {
