@@ -2041,10 +2041,11 @@ __device__ __forceinline__ void contrib_apply(const Contrib &c, Acc &a)
 
 // ---------------------------------------------------------------------------
 // Contribution lists: one CTA per active brick expands the brick's records
-// and counting-sorts the contributions by voxel into global memory (brick b
-// owns entries [4*roff[b], 4*roff[b+1]): a record expands to at most four
-// contributions); then one thread per voxel orders its list by key, sums it in
-// that order (the reference CPU order) and solves.
+// and counting-sorts the contributions by voxel into global memory (the
+// brick reserves exactly its entries with one atomic on counters[C_CONTRIB];
+// the total, four per scanline event and one per other record, sized the
+// buffer); then one thread per voxel orders its list by key, sums it in that
+// order (the reference CPU order) and solves.
 // ---------------------------------------------------------------------------
 // Order key of a contribution list entry {key, payload}.
 __device__ __forceinline__ uint32_t entry_key(const uint2 &e)
