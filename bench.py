@@ -105,6 +105,15 @@ def algorithmic_bytes(V, F, N, face_bytes=8):
     return 12 * V + face_bytes * 3 * F + 27 * N
 
 
+def headline_config(w, voxels: int, world: int) -> dict:
+    """The workload description both arms report, key for key."""
+    return {"workload": HEADLINE, "faces": int(w.num_faces), "vertices": int(w.vertices.shape[0]), "voxels": int(voxels),
+            "grid": 512, "weights": [w.face_weight, w.boundary_weight, w.regularization_weight], "faces_dtype": "int64",
+            "l2": "GPU arm: flushed between steps by a 256 MB write outside the timed events; CPU arm: host code, "
+                  "no GPU cache involved",
+            "parallelism": f"replicas x{world}"}
+
+
 # ----------------------------------------------------------------------------- CPU baseline
 def _ref_worker(args):
     """Runs in a spawned process: one conversion of the mesh by the reference CPU code."""
@@ -114,10 +123,10 @@ def _ref_worker(args):
 
     t0 = time.perf_counter()
     if kind == "reference":
-        O.ref_mesh_to_fdg(v, f, vs, gr, fw, bw, rw)
+        vox = O.ref_mesh_to_fdg(v, f, vs, gr, fw, bw, rw)[0]
     else:
-        O.mesh_to_fdg(v, f, vs, gr, fw, bw, rw)
-    return time.perf_counter() - t0
+        vox = O.mesh_to_fdg(v, f, vs, gr, fw, bw, rw).voxels
+    return time.perf_counter() - t0, int(vox.shape[0])
 
 
 REF_PROCESS_BYTES = 2 << 30  # one full-mesh reference conversion peaks at about 1.6 GB of host memory
@@ -153,12 +162,14 @@ class CpuBaseline:
         self.job = (self.kind, v, f, vs, gr, w.face_weight, w.boundary_weight, w.regularization_weight)
         self.pool = mp.get_context("spawn").Pool(self.cores)
         self.latencies = []
+        self.voxels = 0
 
     def step(self):
         t0 = time.perf_counter()
-        lat = self.pool.map(_ref_worker, [self.job] * self.cores)
+        res = self.pool.map(_ref_worker, [self.job] * self.cores)
         wall = time.perf_counter() - t0
-        self.latencies.extend(lat)
+        self.latencies.extend(r[0] for r in res)
+        self.voxels = res[0][1]
         return wall
 
     def close(self):
@@ -250,7 +261,7 @@ def run_reference(args, rank):
                           f"(at least two) and one warm-up step is run, so that the run ends within minutes",
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64,f32",
             "data": "synthetic: seeded 48-primitive mesh (no dataset on the box)",
-            "config": {"workload": HEADLINE, "faces": int(w.num_faces), "vertices": int(w.vertices.shape[0]), "grid": 512},
+            "config": headline_config(w, cb.voxels, args.gpus),
             "cpu_baseline": cb.describe(value),
             "e2e": {"value": value, "unit": "Mfaces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -542,9 +553,7 @@ def run_ours(args, rank, world):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED_MFACES, "dtype": "f64,f32",
         "data": "synthetic: seeded 48-primitive mesh (no dataset on the box)",
-        "config": {"workload": HEADLINE, "faces": F, "vertices": V, "voxels": N, "grid": 512,
-                   "weights": [w.face_weight, w.boundary_weight, w.regularization_weight], "faces_dtype": "int64",
-                   "l2": "flushed between steps (256 MB write outside the timed events)", "parallelism": f"replicas x{world}"},
+        "config": headline_config(w, N, world),
         "meshes_per_s": world / (ms_per_step / 1e3),
         "batched": batched,
         "e2e": {"value": e2e_value, "unit": "Mfaces/s", "ms_per_step": e2e_ms, "h2d_bytes_per_step": 12 * V + 8 * 3 * F,
